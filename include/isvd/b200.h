@@ -1,0 +1,90 @@
+/*
+ * B200 extensions of the iSVD API.  None of these has a counterpart in the reference
+ * library; they add what the reference cannot express: status codes, a precision mode,
+ * a caller-supplied Gaussian test matrix, and status-returning drivers.
+ */
+#ifndef ISVD_B200_H_
+#define ISVD_B200_H_
+
+#include <isvd/def.h>
+#include <isvd/core/param.h>
+
+#if defined(__cplusplus)
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define ISVD_GPU_SUCCESS            0
+#define ISVD_GPU_ERROR_ARGUMENT     1  /* invalid argument (selector, layout char, size, leading dim) */
+#define ISVD_GPU_ERROR_CUDA         2  /* a CUDA runtime call failed */
+#define ISVD_GPU_ERROR_MEMORY       3  /* device or pinned allocation failed */
+#define ISVD_GPU_ERROR_TIMEOUT      4  /* a bounded device-side wait expired */
+#define ISVD_GPU_ERROR_NUMERICAL    5  /* non-finite values or a matrix iteration that did not converge */
+#define ISVD_GPU_ERROR_UNSUPPORTED  6  /* configuration not implemented (e.g. MPI size > 1) */
+
+/* Status of the most recent failing call on this thread (0 if none since the last clear).
+ * The void entry points of the reference API report failures here and print the message
+ * to stderr, mirroring the reference's print-and-return behaviour for bad arguments. */
+int  isvd_gpu_get_last_error( void );
+const char *isvd_gpu_get_error_string( void );
+void isvd_gpu_clear_error( void );
+
+/* ---------------------------------------------------------------- precision */
+#define ISVD_GPU_PRECISION_NATIVE   0  /* products in the routine's own type (FP64 for isvd_d*, FP32 for isvd_s*) */
+#define ISVD_GPU_PRECISION_MIXED    1  /* BF16x3 split products on tcgen05 tensor cores, FP32 accumulation;
+                                          l x l steps (eigensolves, inverse square roots, small SVDs) in FP64 */
+
+/* Process-wide default precision.  Initial value: ISVD_GPU_PRECISION_NATIVE, or the value
+ * of the environment variable ISVD_GPU_PRECISION ("native" / "mixed") at first use. */
+void isvd_gpu_set_precision( int mode );
+int  isvd_gpu_get_precision( void );
+
+/* ---------------------------------------------------------------- Omega passed in
+ * Gaussian projection sketching with a caller-supplied test matrix Omega (n x Nl,
+ * row-major, leading dimension ldomega >= Nl; the rows of this rank's column block for
+ * dista = 'C').  This is how the reference's own Omega (MKL/LAPACK stream, drawn as
+ * r[j*Nl + c] = Omega(j, c), la/vsl/@x@_rng_gaussian_driver.c:16-41) is replayed. */
+void isvd_sSketchGaussianProjectionOmega(
+    const isvd_Param param, const isvd_s_val_t *argv, const isvd_int_t argc, isvd_s_val_t *retv,
+    const isvd_int_t retc, const char dista, const char ordera, const isvd_s_val_t *a, const isvd_int_t lda,
+    const isvd_s_val_t *omega, const isvd_int_t ldomega, isvd_s_val_t *yst, const isvd_int_t ldyst
+);
+void isvd_dSketchGaussianProjectionOmega(
+    const isvd_Param param, const isvd_d_val_t *argv, const isvd_int_t argc, isvd_d_val_t *retv,
+    const isvd_int_t retc, const char dista, const char ordera, const isvd_d_val_t *a, const isvd_int_t lda,
+    const isvd_d_val_t *omega, const isvd_int_t ldomega, isvd_d_val_t *yst, const isvd_int_t ldyst
+);
+
+/* ---------------------------------------------------------------- status-returning drivers
+ * Same arguments as isvd_?Isvd plus an optional Omega (NULL: drawn on the GPU from seed)
+ * and an explicit precision (-1: the process default).  Returns an ISVD_GPU_* status. */
+int isvd_sIsvd_ex(
+    const isvd_Param param,
+    const char *alg_s, const char *alg_o, const char *alg_i, const char *alg_p,
+    const isvd_s_val_t *argv[4], const isvd_int_t argc[4], isvd_s_val_t *retv[4], const isvd_int_t retc[4],
+    double time[4], FILE *stream,
+    const char dista, const char ordera, const isvd_s_val_t *a, const isvd_int_t lda,
+    isvd_s_val_t *s, isvd_s_val_t *ut, const isvd_int_t ldut, isvd_s_val_t *vt, const isvd_int_t ldvt,
+    const isvd_int_t seed, const mpi_int_t ut_root, const mpi_int_t vt_root,
+    const isvd_s_val_t *omega, const isvd_int_t ldomega, const int precision
+);
+int isvd_dIsvd_ex(
+    const isvd_Param param,
+    const char *alg_s, const char *alg_o, const char *alg_i, const char *alg_p,
+    const isvd_d_val_t *argv[4], const isvd_int_t argc[4], isvd_d_val_t *retv[4], const isvd_int_t retc[4],
+    double time[4], FILE *stream,
+    const char dista, const char ordera, const isvd_d_val_t *a, const isvd_int_t lda,
+    isvd_d_val_t *s, isvd_d_val_t *ut, const isvd_int_t ldut, isvd_d_val_t *vt, const isvd_int_t ldvt,
+    const isvd_int_t seed, const mpi_int_t ut_root, const mpi_int_t vt_root,
+    const isvd_d_val_t *omega, const isvd_int_t ldomega, const int precision
+);
+
+/* Number of kernels this library has launched since the process started (all devices).
+ * Used by benchmarks to report how much of a timed region ran in this library's kernels. */
+unsigned long long isvd_gpu_kernel_launch_count( void );
+
+#if defined(__cplusplus)
+}
+#endif
+
+#endif  /* ISVD_B200_H_ */

@@ -1,0 +1,194 @@
+"""ctypes binding of the iSVD C ABI (``include/isvd.h``).
+
+The same binding loads any library that exports the iSVD C ABI: the B200 library
+(``isvd_b200/libisvd_gpu_b200.so``) or another build of the same interface.  It
+is the Python mirror of the reference's C entry points
+(``src/include/c/isvd/core/@x@_driver.h:21``, ``core/@x@_stage.h:21-77``,
+``gpu/@x@_stage.h:28-90``, ``core/param.h:100``): same names, same argument
+meaning, same layouts (``yst``/``qt``/``ut``/``vt`` row-major, ``a`` per
+``dista``/``ordera``).  Arrays are passed as raw pointers: NumPy arrays give host
+pointers, and anything with ``data_ptr()`` (a CUDA tensor) gives a device pointer.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+c_int_t = ctypes.c_int32          # isvd_int_t (LP64 build, include/isvd/def.h)
+c_mpi_int = ctypes.c_int          # mpi_int_t
+MPI_COMM_WORLD = 0x44000000       # include/mpi_shim/mpi.h
+
+_PARAM_INT_FIELDS = ["nrow", "ncol", "nrow_proc", "ncol_proc", "nrow_each", "ncol_each", "nrow_total",
+                     "ncol_total", "rowidxbegin", "rowidxend", "colidxbegin", "colidxend", "rank", "over_rank",
+                     "dim_sketch", "dim_sketch_total", "num_sketch"]
+
+
+class Param(ctypes.Structure):
+    """isvd_Param (include/isvd/core/param.h; reference core/param.h:27-92)."""
+    _fields_ = [("mpi_comm", ctypes.c_int), ("mpi_size", c_mpi_int), ("mpi_root", c_mpi_int),
+                ("mpi_rank", c_mpi_int)] + [(f, c_int_t) for f in _PARAM_INT_FIELDS]
+
+
+_VP = ctypes.c_void_p
+_CH = ctypes.c_char
+
+
+def ptr(x):
+    """Raw address of a NumPy array / CUDA tensor / int / None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    raise TypeError("cannot take the address of %r" % type(x))
+
+
+def _dt(x):
+    return np.float32 if x == "s" else np.float64
+
+
+class IsvdLib:
+    """Thin wrapper over one shared library exporting the iSVD C ABI."""
+
+    STAGE_HEAD = [Param, _VP, c_int_t, _VP, c_int_t]   # param, argv, argc, retv, retc
+
+    def __init__(self, path, mode=ctypes.RTLD_LOCAL):
+        self.path = os.path.abspath(path)
+        self.lib = ctypes.CDLL(self.path, mode=mode)
+        L = self.lib
+        L.isvd_createParam.restype = Param
+        L.isvd_createParam.argtypes = [c_int_t] * 5 + [c_mpi_int, ctypes.c_int]
+        H = self.STAGE_HEAD
+        for x in "sd":
+            self._decl("isvd_%sSketchGaussianProjection" % x,
+                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, c_int_t, c_mpi_int])
+            self._decl("isvd_%sSketchGaussianProjection_gpu" % x,
+                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, c_int_t, c_mpi_int])
+            for name in ("OrthogonalizeTallSkinnyQr", "OrthogonalizeGramian"):
+                self._decl("isvd_%s%s" % (x, name), H + [_VP, c_int_t])
+            for name in ("IntegrateKolmogorovNagumo", "IntegrateWenYin", "IntegrateHierarchicalReduction"):
+                self._decl("isvd_%s%s" % (x, name), H + [_VP, c_int_t, _VP, c_int_t])
+            post = H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t, c_mpi_int, c_mpi_int]
+            for name in ("PostprocessTallSkinnyQr", "PostprocessGramian", "PostprocessSymmetric"):
+                self._decl("isvd_%s%s" % (x, name), post)
+                self._decl("isvd_%s%s_gpu" % (x, name), post)
+            self._decl("isvd_%sIsvd" % x,
+                       [Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t,
+                        c_int_t, c_mpi_int, c_mpi_int])
+
+        # B200 extensions (include/isvd/b200.h)
+        self._decl("isvd_gpu_get_last_error", [], ctypes.c_int)
+        self._decl("isvd_gpu_get_error_string", [], ctypes.c_char_p)
+        self._decl("isvd_gpu_clear_error", [])
+        self._decl("isvd_gpu_set_precision", [ctypes.c_int])
+        self._decl("isvd_gpu_get_precision", [], ctypes.c_int)
+        self._decl("isvd_gpu_kernel_launch_count", [], ctypes.c_ulonglong)
+        for x in "sd":
+            self._decl("isvd_%sSketchGaussianProjectionOmega" % x,
+                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, _VP, c_int_t])
+            self._decl("isvd_%sIsvd_ex" % x,
+                       [Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t,
+                        c_int_t, c_mpi_int, c_mpi_int, _VP, c_int_t, ctypes.c_int], ctypes.c_int)
+
+    def _decl(self, name, argtypes, restype=None):
+        fn = getattr(self.lib, name, None)
+        if fn is None:
+            return
+        fn.argtypes = argtypes
+        fn.restype = restype
+
+    def has(self, name):
+        return hasattr(self.lib, name)
+
+    # ------------------------------------------------------------------ parameters
+    def create_param(self, m, n, k, p, N, root=0, comm=MPI_COMM_WORLD):
+        return self.lib.isvd_createParam(m, n, k, p, N, root, comm)
+
+    @staticmethod
+    def _args(x, argv, retc):
+        av = None if argv is None else np.ascontiguousarray(argv, dtype=_dt(x))
+        rv = np.zeros(max(retc, 1), dtype=_dt(x))
+        return av, (0 if av is None else len(av)), rv
+
+    # ------------------------------------------------------------------ stages
+    def sketch(self, x, param, a, lda, yst, ldyst, seed, dista=b"R", ordera=b"R", gpu=False, root=0):
+        fn = getattr(self.lib, "isvd_%sSketchGaussianProjection%s" % (x, "_gpu" if gpu else ""))
+        fn(param, None, 0, None, 0, dista, ordera, ptr(a), lda, ptr(yst), ldyst, seed, root)
+
+    def orthogonalize(self, x, alg, param, yst, ldyst):
+        name = {"GR": "OrthogonalizeGramian", "TS": "OrthogonalizeTallSkinnyQr"}[alg]
+        getattr(self.lib, "isvd_%s%s" % (x, name))(param, None, 0, None, 0, ptr(yst), ldyst)
+
+    def integrate(self, x, alg, param, yst, ldyst, qt, ldqt, argv=None, retc=2):
+        name = {"KN": "IntegrateKolmogorovNagumo", "WY": "IntegrateWenYin",
+                "HR": "IntegrateHierarchicalReduction"}[alg]
+        av, ac, rv = self._args(x, argv, retc)
+        getattr(self.lib, "isvd_%s%s" % (x, name))(param, ptr(av), ac, ptr(rv), retc, ptr(yst), ldyst, ptr(qt), ldqt)
+        return rv[:retc]
+
+    def query(self, x, alg, retc):
+        """Default-argument query protocol (argc < 0)."""
+        name = {"KN": "IntegrateKolmogorovNagumo", "WY": "IntegrateWenYin",
+                "HR": "IntegrateHierarchicalReduction"}[alg]
+        rv = np.zeros(max(retc, 1), dtype=_dt(x))
+        p = self.create_param(4, 4, 1, 0, 1)
+        getattr(self.lib, "isvd_%s%s" % (x, name))(p, None, -1, ptr(rv), retc, None, 1, None, 1)
+        return rv[:retc]
+
+    def postprocess(self, x, alg, param, a, lda, qt, ldqt, s, ut, ldut, vt, ldvt, dista=b"R", ordera=b"R",
+                    ut_root=-1, vt_root=-1, gpu=False):
+        name = {"GR": "PostprocessGramian", "TS": "PostprocessTallSkinnyQr", "SY": "PostprocessSymmetric"}[alg]
+        fn = getattr(self.lib, "isvd_%s%s%s" % (x, name, "_gpu" if gpu else ""))
+        fn(param, None, 0, None, 0, dista, ordera, ptr(a), lda, ptr(qt), ldqt, ptr(s), ptr(ut), ldut, ptr(vt),
+           ldvt, ut_root, vt_root)
+
+    # ------------------------------------------------------------------ extensions
+    def last_error(self):
+        return self.lib.isvd_gpu_get_last_error(), (self.lib.isvd_gpu_get_error_string() or b"").decode()
+
+    def clear_error(self):
+        self.lib.isvd_gpu_clear_error()
+
+    def sketch_omega(self, x, param, a, lda, omega, ldomega, yst, ldyst, dista=b"R", ordera=b"R"):
+        fn = getattr(self.lib, "isvd_%sSketchGaussianProjectionOmega" % x)
+        fn(param, None, 0, None, 0, dista, ordera, ptr(a), lda, ptr(omega), ldomega, ptr(yst), ldyst)
+
+    def isvd(self, x, param, algs, a, lda, s, ut, ldut, vt, ldvt, seed=0, dista=b"R", ordera=b"R",
+             argv=None, retc=(0, 0, 2, 0), ut_root=-1, vt_root=-1, omega=None, ldomega=0, precision=None):
+        """isvd_?Isvd driver (isvd_?Isvd_ex when omega / precision is given).
+
+        Returns (retv list, time[4], status)."""
+        dt = _dt(x)
+        keep = []
+        argv_arr = (ctypes.c_void_p * 4)()
+        argc_arr = (c_int_t * 4)()
+        for i in range(4):
+            av = None if argv is None or argv[i] is None else np.ascontiguousarray(argv[i], dtype=dt)
+            keep.append(av)
+            argv_arr[i] = ptr(av)
+            argc_arr[i] = 0 if av is None else len(av)
+        retv_arr = (ctypes.c_void_p * 4)()
+        retc_arr = (c_int_t * 4)()
+        rvs = []
+        for i in range(4):
+            rv = np.zeros(max(retc[i], 1), dtype=dt)
+            rvs.append(rv)
+            retv_arr[i] = ptr(rv)
+            retc_arr[i] = retc[i]
+        times = (ctypes.c_double * 4)()
+        common = (param, algs[0].encode(), algs[1].encode(), algs[2].encode(), algs[3].encode(),
+                  ctypes.cast(argv_arr, _VP) if argv is not None else None, ctypes.cast(argc_arr, _VP),
+                  ctypes.cast(retv_arr, _VP), ctypes.cast(retc_arr, _VP), ctypes.cast(times, _VP), None,
+                  dista, ordera, ptr(a), lda, ptr(s), ptr(ut), ldut, ptr(vt), ldvt, seed, ut_root, vt_root)
+        status = 0
+        if omega is None and precision is None:
+            getattr(self.lib, "isvd_%sIsvd" % x)(*common)
+        else:
+            prec = -1 if precision is None else int(precision)
+            status = getattr(self.lib, "isvd_%sIsvd_ex" % x)(*common, ptr(omega), ldomega, prec)
+        return [rv[:retc[i]] for i, rv in enumerate(rvs)], list(times), status

@@ -1,0 +1,754 @@
+// C ABI of libisvd_gpu_b200: the iSVD entry points of emfomy/isvd v1.3.2 (include/isvd.h) plus
+// the B200 extensions (include/isvd/b200.h).  This file is host code only: argument checking
+// with the reference's semantics, host <-> device marshalling, stage dispatch and the driver.
+#include <cuda_runtime.h>
+
+#include <cctype>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "kernels.h"
+#include "runtime.h"
+#include "stages.h"
+
+// The library is built with -fvisibility=hidden; only the C ABI is exported.
+#pragma GCC visibility push(default)
+extern "C" {
+#include <isvd.h>
+}
+#pragma GCC visibility pop
+
+using namespace isvdb;
+
+// ============================================================================ error state
+namespace {
+
+thread_local int t_last_error = 0;
+thread_local std::string t_last_msg;
+std::recursive_mutex g_api_mu;  // the API is not re-entrant (as the reference); calls are serialised
+
+void record_error(int code, const std::string &msg) {
+  t_last_error = code;
+  t_last_msg = msg;
+  fprintf(stderr, "isvd: %s\n", msg.c_str());
+}
+
+// Print-and-return argument failure (reference util/arg.h:40-48 prints and returns 0).
+struct ArgFail {};
+
+template <class F>
+int api_call(F &&f) {
+  std::lock_guard<std::recursive_mutex> lk(g_api_mu);
+  try {
+    f();
+    return kSuccess;
+  } catch (const ArgFail &) {
+    return t_last_error;
+  } catch (const Error &e) {
+    record_error(e.code, e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    record_error(kErrCuda, e.what());
+    return kErrCuda;
+  }
+}
+
+[[noreturn]] void arg_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_last_error = kErrArgument;
+  t_last_msg = buf;
+  fputs(buf, stderr);
+  throw ArgFail();
+}
+
+// Reference isvd_assert_* failures abort; here they become an argument error.
+#define REQUIRE(cond)                                                                        \
+  do {                                                                                       \
+    if (!(cond)) ::isvdb::fail(kErrArgument, "argument check failed: %s", #cond);            \
+  } while (0)
+
+// Case-insensitive single-character option (reference util/arg.h:22-49).
+char arg2char(const char *name, char arg, const char *opts) {
+  for (const char *o = opts; *o; ++o)
+    if (toupper((unsigned char)arg) == toupper((unsigned char)*o)) return *o;
+  std::string msg = std::string(name) + " ('" + arg + "') must be one of the following characters: ";
+  for (const char *o = opts; *o; ++o) {
+    if (o != opts) msg += ", ";
+    msg += "'";
+    msg += *o;
+    msg += "'";
+  }
+  arg_error("%s.\n", msg.c_str());
+}
+
+// Case-insensitive selector (reference util/arg.h:51-79).
+const char *arg2str(const char *name, const char *arg, const char *const *opts, int nopts) {
+  if (arg) {
+    const size_t la = strlen(arg);
+    for (int i = 0; i < nopts; ++i) {
+      if (strlen(opts[i]) != la) continue;
+      bool eq = true;
+      for (size_t c = 0; c < la && eq; ++c) eq = toupper((unsigned char)arg[c]) == toupper((unsigned char)opts[i][c]);
+      if (eq) return opts[i];
+    }
+  }
+  std::string msg = std::string(name) + " ('" + (arg ? arg : "(null)") + "') must be one of the following strings: ";
+  for (int i = 0; i < nopts; ++i) {
+    if (i) msg += ", ";
+    msg += "\"";
+    msg += opts[i];
+    msg += "\"";
+  }
+  arg_error("%s.\n", msg.c_str());
+}
+
+void require_single_rank(const isvd_Param &p) {
+  if (p.mpi_size != 1)
+    fail(kErrUnsupported, "MPI size %d: this build runs one MPI rank per GPU (P = 1)", (int)p.mpi_size);
+}
+
+template <class T>
+struct TypeName;
+template <>
+struct TypeName<float> { static constexpr const char *name = "Real Single"; };
+template <>
+struct TypeName<double> { static constexpr const char *name = "Real Double"; };
+
+// ============================================================================ marshalling
+// A caller matrix region: `outer` lines of `inner` contiguous elements, line stride `ld`.
+template <class T>
+struct View {
+  T *d = nullptr;
+  DBuf<T> own;
+  T *host = nullptr;
+  long long inner = 0, outer = 0, ld = 0;
+
+  void bind(const T *p, long long inner_, long long outer_, long long ld_, bool copy_in, cudaStream_t st) {
+    inner = inner_; outer = outer_; ld = ld_;
+    if (p == nullptr || inner <= 0 || outer <= 0) { d = const_cast<T *>(p); return; }
+    if (is_device_pointer(p)) { d = const_cast<T *>(p); return; }
+    host = const_cast<T *>(p);
+    own.alloc((size_t)((outer - 1) * ld + inner));
+    d = own.p;
+    if (copy_in)
+      CK(cudaMemcpy2DAsync(d, ld * sizeof(T), p, ld * sizeof(T), inner * sizeof(T), outer, cudaMemcpyHostToDevice,
+                           st));
+  }
+  // Copy `cols` leading elements of each line back to the host buffer.
+  void back(cudaStream_t st, long long cols = -1) {
+    if (!host) return;
+    if (cols < 0) cols = inner;
+    CK(cudaMemcpy2DAsync(host, ld * sizeof(T), d, ld * sizeof(T), cols * sizeof(T), outer, cudaMemcpyDeviceToHost,
+                         st));
+  }
+};
+
+struct Ctx {
+  StageCtx sc;
+  explicit Ctx(int precision) {
+    Runtime &rt = Runtime::get();
+    sc.st = rt.stream;
+    sc.precision = precision < 0 ? default_precision() : precision;
+    sc.status = reinterpret_cast<int *>(rt.ctl + 16);
+    CK(cudaMemsetAsync(sc.status, 0, sizeof(int), sc.st));
+  }
+};
+
+// ============================================================================ stages
+// Sketching (reference core/stage/@x@_sketch_gaussian_projection.c:46-84, @x@_sketch.h).
+template <class T>
+void sketch_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd_int_t retc, char dista,
+                char ordera, const T *a, isvd_int_t lda, const T *omega, isvd_int_t ldomega, T *yst,
+                isvd_int_t ldyst, isvd_int_t seed, int precision) {
+  if (argc > 0) REQUIRE(argv != nullptr);
+  if (retc > 0) REQUIRE(retv != nullptr);
+  if (argc < 0) return;
+  const char dista_ = arg2char("DISTA", dista, "CR");
+  const char ordera_ = arg2char("ORDERA", ordera, "CR");
+  require_single_rank(p);
+  const int m = p.nrow, n = p.ncol, Nl = p.dim_sketch_total;
+  if (dista_ == 'C') {
+    REQUIRE(ordera_ == 'C' ? lda >= m : lda >= p.ncol_proc);
+    REQUIRE(ldyst == Nl);
+  } else {
+    REQUIRE(ordera_ == 'C' ? lda >= p.nrow_proc : lda >= n);
+    REQUIRE(ldyst >= Nl);
+  }
+  if (omega) REQUIRE(ldomega >= Nl);
+  Ctx c(precision);
+  View<T> A, Om, Y;
+  if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
+  else A.bind(a, m, n, lda, true, c.sc.st);
+  if (omega) Om.bind(omega, Nl, n, ldomega, true, c.sc.st);
+  Y.bind(yst, Nl, m, ldyst, false, c.sc.st);
+  sketch_dev<T>(c.sc, m, n, Nl, ordera_, A.d, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.d,
+                ldyst);
+  Y.back(c.sc.st);
+  sync();
+}
+
+template <class T>
+void orth_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd_int_t retc, T *yst,
+              isvd_int_t ldyst, bool tsqr) {
+  if (argc > 0) REQUIRE(argv != nullptr);
+  if (retc > 0) REQUIRE(retv != nullptr);
+  if (argc < 0) return;
+  require_single_rank(p);
+  const int m = p.nrow_proc, l = p.dim_sketch, N = p.num_sketch, Nl = p.dim_sketch_total;
+  REQUIRE(ldyst >= Nl);
+  if (tsqr) REQUIRE(m >= l);
+  Ctx c(-1);
+  View<T> Y;
+  Y.bind(yst, Nl, m, ldyst, true, c.sc.st);
+  if (tsqr) orth_tsqr_dev<T>(c.sc, m, l, N, Y.d, ldyst);
+  else orth_gramian_dev<T>(c.sc, m, l, N, Y.d, ldyst);
+  Y.back(c.sc.st);
+  sync();
+}
+
+template <class T>
+void query_kn(T *retv, isvd_int_t retc) {
+  int i = -1;
+  if (retc > ++i) retv[i] = (T)256;
+  if (retc > ++i) retv[i] = (T)1e-4;
+}
+
+template <class T>
+void query_wy(T *retv, isvd_int_t retc) {
+  const double d[9] = {256, 1e-3, 1.0, 1e14, 1e-14, 20, 0.5, 1e-4, 0.85};
+  for (int i = 0; i < 9 && i < retc; ++i) retv[i] = (T)d[i];
+}
+
+template <class T>
+void integrate_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd_int_t retc, T *yst,
+                   isvd_int_t ldyst, T *qt, isvd_int_t ldqt, int alg) {
+  if (argc > 0) REQUIRE(argv != nullptr);
+  if (retc > 0) REQUIRE(retv != nullptr);
+  if (argc < 0) {
+    if (alg == 0) query_kn(retv, retc);
+    if (alg == 1) query_wy(retv, retc);
+    return;
+  }
+  require_single_rank(p);
+  const int m = p.nrow_proc, l = p.dim_sketch, N = p.num_sketch, Nl = p.dim_sketch_total;
+  REQUIRE(ldyst >= Nl);
+  REQUIRE(ldqt >= l);
+  Ctx c(-1);
+  View<T> Y, Q;
+  Y.bind(yst, Nl, m, ldyst, true, c.sc.st);
+  Q.bind(qt, l, m, ldqt, false, c.sc.st);
+  IterResult r;
+  if (alg == 0) {
+    int ai = -1;
+    const int maxit = (argc > ++ai) ? (int)argv[ai] : 256;
+    const double tol = (argc > ++ai) ? (double)argv[ai] : 1e-4;
+    REQUIRE(maxit >= 0);
+    REQUIRE(tol >= 0);
+    r = integrate_kn_dev<T>(c.sc, m, l, N, Y.d, ldyst, Q.d, ldqt, maxit, tol);
+  } else if (alg == 1) {
+    WyArgs w;
+    int ai = -1;
+    if (argc > ++ai) w.maxit = (int)argv[ai];
+    if (argc > ++ai) w.tol = argv[ai];
+    if (argc > ++ai) w.tau0 = argv[ai];
+    if (argc > ++ai) w.taumax = argv[ai];
+    if (argc > ++ai) w.taumin = argv[ai];
+    if (argc > ++ai) w.taumaxit = (int)argv[ai];
+    if (argc > ++ai) w.beta = argv[ai];
+    if (argc > ++ai) w.sigma = argv[ai];
+    if (argc > ++ai) w.eta = argv[ai];
+    REQUIRE(w.maxit >= 0 && w.tol >= 0 && w.tau0 >= 0 && w.taumax >= 0 && w.taumin >= 0 && w.taumaxit >= 0);
+    REQUIRE(w.beta > 0 && w.beta < 1 && w.sigma > 0 && w.sigma < 1 && w.eta > 0 && w.eta < 1);
+    r = integrate_wy_dev<T>(c.sc, m, l, N, Y.d, ldyst, Q.d, ldqt, w);
+  } else {
+    integrate_hr_dev<T>(c.sc, m, l, N, Y.d, ldyst, Q.d, ldqt);
+    Y.back(c.sc.st);  // the reference overwrites yst
+  }
+  Q.back(c.sc.st);
+  sync();
+  if (alg != 2) {
+    int ri = -1;
+    if (retc > ++ri) retv[ri] = (T)r.iterations;
+    if (retc > ++ri) retv[ri] = (T)r.error;
+  }
+}
+
+// Postprocessing (reference @x@_postprocess_{gramian,tall_skinny_qr,symmetric}.c).  alg 0 GR, 1 TS, 2 SY.
+template <class T>
+void post_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd_int_t retc, char dista,
+              char ordera, const T *a, isvd_int_t lda, const T *qt, isvd_int_t ldqt, T *s, T *ut, isvd_int_t ldut,
+              T *vt, isvd_int_t ldvt, mpi_int_t ut_root, mpi_int_t vt_root, int alg, int precision) {
+  if (argc > 0) REQUIRE(argv != nullptr);
+  if (retc > 0) REQUIRE(retv != nullptr);
+  if (argc < 0) return;
+  const char dista_ = arg2char("DISTA", dista, "CR");
+  const char ordera_ = arg2char("ORDERA", ordera, "CR");
+  require_single_rank(p);
+  const int m = p.nrow, n = p.ncol, k = p.rank, l = p.dim_sketch;
+  if (alg == 2) {
+    // symmetric: U and V are the same matrix; the first requested one is computed (:101-104)
+    REQUIRE(p.nrow_proc == p.ncol_proc);
+    const mpi_int_t r = (ut_root >= -1) ? ut_root : vt_root;
+    const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
+    if (r >= 0) REQUIRE(ld == l);
+    else if (r == -1) REQUIRE(ld >= l);
+  } else {
+    if (ut_root >= 0) REQUIRE(ldut == l);
+    else if (ut_root == -1) REQUIRE(ldut >= l);
+    if (vt_root >= 0) REQUIRE(ldvt == l);
+    else if (vt_root == -1) REQUIRE(ldvt >= l);
+  }
+  if (dista_ == 'C') {
+    REQUIRE(ordera_ == 'C' ? lda >= m : lda >= p.ncol_proc);
+    REQUIRE(ldqt == l);
+  } else {
+    REQUIRE(ordera_ == 'C' ? lda >= p.nrow_proc : lda >= n);
+    REQUIRE(ldqt >= l);
+  }
+  if (alg == 1) REQUIRE(n >= l);
+  Ctx c(precision);
+  View<T> A, Q, S, U, V;
+  if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
+  else A.bind(a, m, n, lda, true, c.sc.st);
+  Q.bind(qt, l, m, ldqt, true, c.sc.st);
+  S.bind(s, l, 1, l, false, c.sc.st);
+  if (alg == 2) {
+    const bool wu = ut_root >= -1 || vt_root >= -1;
+    T *u = (ut_root >= -1) ? ut : vt;
+    const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
+    U.bind(u, k, m, ld, false, c.sc.st);
+    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ld, wu);
+    S.back(c.sc.st);
+    if (wu) U.back(c.sc.st, k);
+    if (ut_root >= -1 && vt_root >= -1) {
+      // the reference copies U into V as well (:162-164)
+      View<T> V2;
+      V2.bind(vt, k, m, ldvt, false, c.sc.st);
+      CK(cudaMemcpy2DAsync(V2.d, ldvt * sizeof(T), U.d, ld * sizeof(T), k * sizeof(T), m, cudaMemcpyDeviceToDevice,
+                           c.sc.st));
+      V2.back(c.sc.st, k);
+      sync();
+    }
+    sync();
+    return;
+  }
+  const bool wu = ut_root >= -1, wv = vt_root >= -1;
+  const int vcols = (alg == 1) ? l : k;
+  if (wu) U.bind(ut, k, m, ldut, false, c.sc.st);
+  if (wv) V.bind(vt, vcols, n, ldvt, false, c.sc.st);
+  if (alg == 0)
+    post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+  else
+    post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+  S.back(c.sc.st);
+  if (wu) U.back(c.sc.st, k);
+  if (wv) V.back(c.sc.st, vcols);
+  sync();
+}
+
+// ============================================================================ driver
+const char *const kOptsS[] = {"GP", "GP_gpu"};
+const char *const kOptsO[] = {"TS", "GR", "TS_gpu", "GR_gpu"};
+const char *const kOptsI[] = {"KN", "WY", "HR", "KN_gpu", "WY_gpu", "HR_gpu"};
+const char *const kOptsP[] = {"TS", "GR", "SY", "TS_gpu", "GR_gpu", "SY_gpu"};
+
+std::string base(const char *sel) {
+  std::string s(sel);
+  const size_t u = s.find('_');
+  return u == std::string::npos ? s : s.substr(0, u);
+}
+
+const char *alg_name(char stage, const std::string &b, bool gpu) {
+  static thread_local std::string out;
+  const char *what = "";
+  if (stage == 'S') what = "Gaussian Projection Sketching";
+  if (stage == 'O') what = (b == "TS") ? "Tall-Skinny QR Orthogonalization" : "Gramian Orthogonalization";
+  if (stage == 'I')
+    what = (b == "KN") ? "Kolmogorov-Nagumo Integration"
+                       : (b == "WY") ? "Wen-Yin Integration" : "Hierarchical Reduction Integration";
+  if (stage == 'P')
+    what = (b == "TS") ? "Tall-Skinny QR Postprocessing"
+                       : (b == "GR") ? "Gramian Postprocessing" : "Symmetric Postprocessing";
+  out = std::string(gpu ? "GPU " : "") + what;
+  return out.c_str();
+}
+
+struct StageTimer {
+  cudaEvent_t ev[5];
+  StageTimer() { for (auto &e : ev) CK(cudaEventCreate(&e)); }
+  ~StageTimer() { for (auto &e : ev) cudaEventDestroy(e); }
+  void mark(int i, cudaStream_t st) { CK(cudaEventRecord(ev[i], st)); }
+  double sec(int i) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+    return ms * 1e-3;
+  }
+};
+
+template <class T>
+void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const char *alg_i, const char *alg_p,
+            const T *argv[4], const isvd_int_t argc[4], T *retv[4], const isvd_int_t retc[4], double time[4],
+            FILE *stream, char dista, char ordera, const T *a, isvd_int_t lda, T *s, T *ut, isvd_int_t ldut, T *vt,
+            isvd_int_t ldvt, isvd_int_t seed, mpi_int_t ut_root, mpi_int_t vt_root, const T *omega,
+            isvd_int_t ldomega, int precision) {
+  // Selectors (reference core/driver/@x@_isvd.c:135-149)
+  const std::string bs = base(arg2str("ALG_S", alg_s, kOptsS, 2));
+  const std::string bo = base(arg2str("ALG_O", alg_o, kOptsO, 4));
+  const std::string bi = base(arg2str("ALG_I", alg_i, kOptsI, 6));
+  const std::string bp = base(arg2str("ALG_P", alg_p, kOptsP, 6));
+  (void)bs;
+  const T *av[4] = {nullptr, nullptr, nullptr, nullptr};
+  isvd_int_t ac[4] = {0, 0, 0, 0};
+  T *rv[4] = {nullptr, nullptr, nullptr, nullptr};
+  isvd_int_t rc[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; ++i) {
+    if (argv) { av[i] = argv[i]; ac[i] = argc[i]; }
+    if (retv) { rv[i] = retv[i]; rc[i] = retc[i]; }
+    if (ac[i] > 0) REQUIRE(av[i] != nullptr);
+    if (rc[i] > 0) REQUIRE(rv[i] != nullptr);
+  }
+  // Default-argument query (:199-218): only the integration stages have defaults.
+  bool query = false;
+  for (int i = 0; i < 4; ++i) query |= ac[i] < 0;
+  if (query) {
+    if (ac[2] < 0) {
+      if (bi == "KN") query_kn(rv[2], rc[2]);
+      if (bi == "WY") query_wy(rv[2], rc[2]);
+    }
+    return;
+  }
+  const char dista_ = arg2char("DISTA", dista, "CR");
+  const char ordera_ = arg2char("ORDERA", ordera, "CR");
+  require_single_rank(p);
+  const int m = p.nrow, n = p.ncol, k = p.rank, l = p.dim_sketch, N = p.num_sketch, Nl = p.dim_sketch_total;
+  const bool root = p.mpi_rank == p.mpi_root;
+  if (stream && root) {
+    const char *tn = TypeName<T>::name;
+    fprintf(stream, "Using %s Precision %s.\n", tn, alg_name('S', "GP", true));
+    fprintf(stream, "Using %s Precision %s.\n", tn, alg_name('O', bo, true));
+    fprintf(stream, "Using %s Precision %s.\n", tn, alg_name('I', bi, true));
+    fprintf(stream, "Using %s Precision %s.\n", tn, alg_name('P', bp, true));
+    fprintf(stream, "\n");
+  }
+  // Argument checks of the stages (sketch / postprocess), done up front
+  if (dista_ == 'C') REQUIRE(ordera_ == 'C' ? lda >= m : lda >= p.ncol_proc);
+  else REQUIRE(ordera_ == 'C' ? lda >= p.nrow_proc : lda >= n);
+  if (ut_root >= 0) REQUIRE(ldut == l); else if (ut_root == -1) REQUIRE(ldut >= l);
+  if (vt_root >= 0) REQUIRE(ldvt == l); else if (vt_root == -1) REQUIRE(ldvt >= l);
+  if (bo == "TS") REQUIRE(m >= l);
+  if (bp == "TS") REQUIRE(n >= l);
+  if (bp == "SY") REQUIRE(m == n);
+  if (omega) REQUIRE(ldomega >= Nl);
+
+  Ctx c(precision);
+  cudaStream_t st = c.sc.st;
+  StageTimer tm;
+  auto progress = [&](const char *what) {
+    if (stream && root) { fprintf(stream, "%s", what); fflush(stream); }
+  };
+  auto done = [&]() {
+    if (stream && root) { fprintf(stream, "done.\n"); fflush(stream); }
+  };
+
+  // ---- sketch (includes moving A to the device when it is on the host)
+  progress("Sketching ..................... ");
+  tm.mark(0, st);
+  View<T> A, Om;
+  if (ordera_ == 'R') A.bind(a, n, m, lda, true, st);
+  else A.bind(a, m, n, lda, true, st);
+  if (omega) Om.bind(omega, Nl, n, ldomega, true, st);
+  DBuf<T> Y((size_t)m * Nl), Q((size_t)m * l);
+  sketch_dev<T>(c.sc, m, n, Nl, ordera_, A.d, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
+                Nl);
+  tm.mark(1, st);
+  sync();
+  done();
+  // ---- orthogonalize
+  progress("Orthogonalizing ............... ");
+  if (bo == "TS") orth_tsqr_dev<T>(c.sc, m, l, N, Y.p, Nl);
+  else orth_gramian_dev<T>(c.sc, m, l, N, Y.p, Nl);
+  tm.mark(2, st);
+  sync();
+  done();
+  // ---- integrate
+  progress("Integrating ................... ");
+  IterResult ir;
+  if (bi == "KN") {
+    int ai = -1;
+    const int maxit = (ac[2] > ++ai) ? (int)av[2][ai] : 256;
+    const double tol = (ac[2] > ++ai) ? (double)av[2][ai] : 1e-4;
+    REQUIRE(maxit >= 0 && tol >= 0);
+    ir = integrate_kn_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l, maxit, tol);
+  } else if (bi == "WY") {
+    WyArgs w;
+    int ai = -1;
+    const T *x = av[2];
+    if (ac[2] > ++ai) w.maxit = (int)x[ai];
+    if (ac[2] > ++ai) w.tol = x[ai];
+    if (ac[2] > ++ai) w.tau0 = x[ai];
+    if (ac[2] > ++ai) w.taumax = x[ai];
+    if (ac[2] > ++ai) w.taumin = x[ai];
+    if (ac[2] > ++ai) w.taumaxit = (int)x[ai];
+    if (ac[2] > ++ai) w.beta = x[ai];
+    if (ac[2] > ++ai) w.sigma = x[ai];
+    if (ac[2] > ++ai) w.eta = x[ai];
+    ir = integrate_wy_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l, w);
+  } else {
+    integrate_hr_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l);
+  }
+  tm.mark(3, st);
+  sync();
+  done();
+  if (bi != "HR") {
+    int ri = -1;
+    if (rc[2] > ++ri) rv[2][ri] = (T)ir.iterations;
+    if (rc[2] > ++ri) rv[2][ri] = (T)ir.error;
+  }
+  // ---- postprocess
+  progress("Postprocessing ................ ");
+  View<T> S, U, V;
+  S.bind(s, l, 1, l, false, st);
+  if (bp == "SY") {
+    const bool wu = ut_root >= -1 || vt_root >= -1;
+    T *u = (ut_root >= -1) ? ut : vt;
+    const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
+    U.bind(u, k, m, ld, false, st);
+    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ld, wu);
+    tm.mark(4, st);
+    S.back(st);
+    if (wu) U.back(st, k);
+    if (ut_root >= -1 && vt_root >= -1) {
+      View<T> V2;
+      V2.bind(vt, k, m, ldvt, false, st);
+      CK(cudaMemcpy2DAsync(V2.d, ldvt * sizeof(T), U.d, ld * sizeof(T), k * sizeof(T), m, cudaMemcpyDeviceToDevice,
+                           st));
+      V2.back(st, k);
+      sync();
+    }
+  } else {
+    const bool wu = ut_root >= -1, wv = vt_root >= -1;
+    const int vcols = (bp == "TS") ? l : k;
+    if (wu) U.bind(ut, k, m, ldut, false, st);
+    if (wv) V.bind(vt, vcols, n, ldvt, false, st);
+    if (bp == "GR")
+      post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+    else
+      post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+    tm.mark(4, st);
+    S.back(st);
+    if (wu) U.back(st, k);
+    if (wv) V.back(st, vcols);
+  }
+  sync();
+  done();
+  if (time) for (int i = 0; i < 4; ++i) time[i] = tm.sec(i);
+}
+
+}  // namespace
+
+// ============================================================================ exported C ABI
+#pragma GCC visibility push(default)
+extern "C" {
+
+size_t isvd_gpu_memory_limit = 0;
+
+int isvd_gpu_get_last_error(void) { return t_last_error; }
+const char *isvd_gpu_get_error_string(void) { return t_last_msg.c_str(); }
+void isvd_gpu_clear_error(void) { t_last_error = 0; t_last_msg.clear(); }
+void isvd_gpu_set_precision(int mode) { set_default_precision(mode == ISVD_GPU_PRECISION_MIXED ? kMixed : kNative); }
+int isvd_gpu_get_precision(void) { return default_precision(); }
+unsigned long long isvd_gpu_kernel_launch_count(void) { return g_launches.load(); }
+
+// ---------------------------------------------------------------- utilities
+mpi_int_t isvd_getMpiSize(const isvd_MpiComm comm) {
+  int s = 0;
+  MPI_Comm_size(comm, &s);
+  return s;
+}
+mpi_int_t isvd_getMpiRank(const isvd_MpiComm comm) {
+  int r = 0;
+  MPI_Comm_rank(comm, &r);
+  return r;
+}
+
+static void *aligned64(size_t bytes) {
+  void *p = nullptr;
+  if (bytes == 0) bytes = 64;
+  if (posix_memalign(&p, 64, bytes) != 0) return nullptr;
+  return p;
+}
+isvd_int_t *isvd_iMalloc(const size_t num) { return (isvd_int_t *)aligned64(num * sizeof(isvd_int_t)); }
+isvd_s_val_t *isvd_sMalloc(const size_t num) { return (isvd_s_val_t *)aligned64(num * sizeof(isvd_s_val_t)); }
+isvd_d_val_t *isvd_dMalloc(const size_t num) { return (isvd_d_val_t *)aligned64(num * sizeof(isvd_d_val_t)); }
+void isvd_Free(void *ptr) { free(ptr); }
+void isvd_iMemset0(isvd_int_t *ptr, const size_t num) { memset(ptr, 0, num * sizeof(*ptr)); }
+void isvd_sMemset0(isvd_s_val_t *ptr, const size_t num) { memset(ptr, 0, num * sizeof(*ptr)); }
+void isvd_dMemset0(isvd_d_val_t *ptr, const size_t num) { memset(ptr, 0, num * sizeof(*ptr)); }
+void isvd_iMemcpy(isvd_int_t *d, const isvd_int_t *s, const size_t num) { memcpy(d, s, num * sizeof(*d)); }
+void isvd_sMemcpy(isvd_s_val_t *d, const isvd_s_val_t *s, const size_t num) { memcpy(d, s, num * sizeof(*d)); }
+void isvd_dMemcpy(isvd_d_val_t *d, const isvd_d_val_t *s, const size_t num) { memcpy(d, s, num * sizeof(*d)); }
+
+// ---------------------------------------------------------------- environment
+void isvd_Init_cpu(int *argcp, char ***argvp, const isvd_MpiComm mpi_comm) {
+  (void)mpi_comm;
+  MPI_Init(argcp, argvp);
+}
+void isvd_Finalize_cpu(void) { MPI_Finalize(); }
+void isvd_PrintEnvironment_cpu(const isvd_MpiComm comm) {
+  printf("iSVD %s (B200 implementation %s), %d MPI process(es)\n", ISVD_VERSION, ISVD_B200_VERSION,
+         (int)isvd_getMpiSize(comm));
+}
+void isvd_Init_gpu(int *argcp, char ***argvp, const isvd_MpiComm mpi_comm) {
+  (void)argcp; (void)argvp;
+  api_call([&] {
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    if (count == 0) fail(kErrCuda, "no CUDA device");
+    CK(cudaSetDevice(isvd_getMpiRank(mpi_comm) % count));
+    Runtime::get();
+  });
+}
+void isvd_Finalize_gpu(void) {
+  api_call([] { Runtime::reset(); });
+}
+void isvd_PrintEnvironment_gpu(const isvd_MpiComm comm) {
+  (void)comm;
+  api_call([] {
+    Runtime &rt = Runtime::get();
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, rt.device));
+    printf("GPU %d: %s, sm_%d%d, %d SMs, %.1f GiB\n\n", rt.device, prop.name, prop.major, prop.minor,
+           prop.multiProcessorCount, prop.totalGlobalMem / 1073741824.0);
+  });
+}
+
+// ---------------------------------------------------------------- parameters
+isvd_Param isvd_createParam(const isvd_int_t nrow, const isvd_int_t ncol, const isvd_int_t rank,
+                            const isvd_int_t over_rank, const isvd_int_t num_sketch, const mpi_int_t mpi_root,
+                            const isvd_MpiComm mpi_comm) {
+  const mpi_int_t P = isvd_getMpiSize(mpi_comm), j = isvd_getMpiRank(mpi_comm);
+  if (!(nrow > 0 && ncol > 0 && rank > 0 && over_rank >= 0 && num_sketch > 0))
+    record_error(kErrArgument, "isvd_createParam: sizes must be positive (nrow, ncol, rank, num_sketch > 0, "
+                               "over_rank >= 0)");
+  const isvd_int_t mb = (nrow - 1) / P + 1, nb = (ncol - 1) / P + 1;
+  isvd_int_t rb = j * mb, re = rb + mb, cb = j * nb, ce = cb + nb;
+  if (rb > nrow) rb = nrow;
+  if (re > nrow) re = nrow;
+  if (cb > ncol) cb = ncol;
+  if (ce > ncol) ce = ncol;
+  isvd_Param p = {mpi_comm, P, mpi_root, j, nrow, ncol, re - rb, ce - cb, mb, nb, mb * P, nb * P, rb, re, cb, ce,
+                  rank, over_rank, rank + over_rank, (rank + over_rank) * num_sketch, num_sketch};
+  return p;
+}
+
+// ---------------------------------------------------------------- stages
+#define ISVD_STAGES(x, T)                                                                                          \
+  void isvd_##x##SketchGaussianProjection(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,    \
+                                          const isvd_int_t retc, const char dista, const char ordera, const T *a,    \
+                                          const isvd_int_t lda, T *yst, const isvd_int_t ldyst,                      \
+                                          const isvd_int_t seed, const mpi_int_t mpi_root) {                         \
+    (void)mpi_root;                                                                                                \
+    api_call([&] {                                                                                                 \
+      sketch_api<T>(param, argv, argc, retv, retc, dista, ordera, a, lda, nullptr, 0, yst, ldyst, seed, -1);      \
+    });                                                                                                            \
+  }                                                                                                                \
+  void isvd_##x##SketchGaussianProjection_gpu(const isvd_Param param, const T *argv, const isvd_int_t argc,         \
+                                              T *retv, const isvd_int_t retc, const char dista, const char ordera, \
+                                              const T *a, const isvd_int_t lda, T *yst, const isvd_int_t ldyst,    \
+                                              const isvd_int_t seed, const mpi_int_t mpi_root) {                   \
+    isvd_##x##SketchGaussianProjection(param, argv, argc, retv, retc, dista, ordera, a, lda, yst, ldyst, seed,     \
+                                       mpi_root);                                                                  \
+  }                                                                                                                \
+  void isvd_##x##SketchGaussianProjectionOmega(const isvd_Param param, const T *argv, const isvd_int_t argc,        \
+                                               T *retv, const isvd_int_t retc, const char dista,                   \
+                                               const char ordera, const T *a, const isvd_int_t lda,                \
+                                               const T *omega, const isvd_int_t ldomega, T *yst,                   \
+                                               const isvd_int_t ldyst) {                                           \
+    api_call([&] {                                                                                                 \
+      if (!omega) fail(kErrArgument, "isvd_" #x "SketchGaussianProjectionOmega: omega is NULL");                   \
+      sketch_api<T>(param, argv, argc, retv, retc, dista, ordera, a, lda, omega, ldomega, yst, ldyst, 0, -1);     \
+    });                                                                                                            \
+  }                                                                                                                \
+  void isvd_##x##OrthogonalizeTallSkinnyQr(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,   \
+                                           const isvd_int_t retc, T *yst, const isvd_int_t ldyst) {                \
+    api_call([&] { orth_api<T>(param, argv, argc, retv, retc, yst, ldyst, true); });                                \
+  }                                                                                                                \
+  void isvd_##x##OrthogonalizeGramian(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,        \
+                                      const isvd_int_t retc, T *yst, const isvd_int_t ldyst) {                     \
+    api_call([&] { orth_api<T>(param, argv, argc, retv, retc, yst, ldyst, false); });                               \
+  }                                                                                                                \
+  void isvd_##x##IntegrateKolmogorovNagumo(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,   \
+                                           const isvd_int_t retc, const T *yst, const isvd_int_t ldyst, T *qt,     \
+                                           const isvd_int_t ldqt) {                                                \
+    api_call([&] { integrate_api<T>(param, argv, argc, retv, retc, const_cast<T *>(yst), ldyst, qt, ldqt, 0); });  \
+  }                                                                                                                \
+  void isvd_##x##IntegrateWenYin(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,             \
+                                 const isvd_int_t retc, const T *yst, const isvd_int_t ldyst, T *qt,               \
+                                 const isvd_int_t ldqt) {                                                          \
+    api_call([&] { integrate_api<T>(param, argv, argc, retv, retc, const_cast<T *>(yst), ldyst, qt, ldqt, 1); });  \
+  }                                                                                                                \
+  void isvd_##x##IntegrateHierarchicalReduction(const isvd_Param param, const T *argv, const isvd_int_t argc,       \
+                                                T *retv, const isvd_int_t retc, T *yst, const isvd_int_t ldyst,    \
+                                                T *qt, const isvd_int_t ldqt) {                                    \
+    api_call([&] { integrate_api<T>(param, argv, argc, retv, retc, yst, ldyst, qt, ldqt, 2); });                    \
+  }                                                                                                                \
+  ISVD_POST(x, T, PostprocessGramian, 0)                                                                           \
+  ISVD_POST(x, T, PostprocessTallSkinnyQr, 1)                                                                      \
+  ISVD_POST(x, T, PostprocessSymmetric, 2)                                                                         \
+  void isvd_##x##Isvd(const isvd_Param param, const char *alg_s, const char *alg_o, const char *alg_i,             \
+                      const char *alg_p, const T *argv[4], const isvd_int_t argc[4], T *retv[4],                   \
+                      const isvd_int_t retc[4], double time[4], FILE *stream, const char dista, const char ordera, \
+                      const T *a, const isvd_int_t lda, T *s, T *ut, const isvd_int_t ldut, T *vt,                 \
+                      const isvd_int_t ldvt, const isvd_int_t seed, const mpi_int_t ut_root,                       \
+                      const mpi_int_t vt_root) {                                                                   \
+    api_call([&] {                                                                                                 \
+      driver<T>(param, alg_s, alg_o, alg_i, alg_p, argv, argc, retv, retc, time, stream, dista, ordera, a, lda, s, \
+                ut, ldut, vt, ldvt, seed, ut_root, vt_root, nullptr, 0, -1);                                       \
+    });                                                                                                            \
+  }                                                                                                                \
+  int isvd_##x##Isvd_ex(const isvd_Param param, const char *alg_s, const char *alg_o, const char *alg_i,           \
+                        const char *alg_p, const T *argv[4], const isvd_int_t argc[4], T *retv[4],                 \
+                        const isvd_int_t retc[4], double time[4], FILE *stream, const char dista,                  \
+                        const char ordera, const T *a, const isvd_int_t lda, T *s, T *ut, const isvd_int_t ldut,   \
+                        T *vt, const isvd_int_t ldvt, const isvd_int_t seed, const mpi_int_t ut_root,              \
+                        const mpi_int_t vt_root, const T *omega, const isvd_int_t ldomega, const int precision) {  \
+    return api_call([&] {                                                                                          \
+      driver<T>(param, alg_s, alg_o, alg_i, alg_p, argv, argc, retv, retc, time, stream, dista, ordera, a, lda, s, \
+                ut, ldut, vt, ldvt, seed, ut_root, vt_root, omega, ldomega,                                        \
+                precision == ISVD_GPU_PRECISION_MIXED ? (int)kMixed                                               \
+                : precision == ISVD_GPU_PRECISION_NATIVE ? (int)kNative : -1);                                     \
+    });                                                                                                            \
+  }
+
+#define ISVD_POST(x, T, NAME, ALG)                                                                                 \
+  void isvd_##x##NAME(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv, const isvd_int_t retc, \
+                      const char dista, const char ordera, const T *a, const isvd_int_t lda, const T *qt,          \
+                      const isvd_int_t ldqt, T *s, T *ut, const isvd_int_t ldut, T *vt, const isvd_int_t ldvt,     \
+                      const mpi_int_t ut_root, const mpi_int_t vt_root) {                                          \
+    api_call([&] {                                                                                                 \
+      post_api<T>(param, argv, argc, retv, retc, dista, ordera, a, lda, qt, ldqt, s, ut, ldut, vt, ldvt, ut_root,  \
+                  vt_root, ALG, -1);                                                                               \
+    });                                                                                                            \
+  }                                                                                                                \
+  void isvd_##x##NAME##_gpu(const isvd_Param param, const T *argv, const isvd_int_t argc, T *retv,                 \
+                            const isvd_int_t retc, const char dista, const char ordera, const T *a,                \
+                            const isvd_int_t lda, const T *qt, const isvd_int_t ldqt, T *s, T *ut,                 \
+                            const isvd_int_t ldut, T *vt, const isvd_int_t ldvt, const mpi_int_t ut_root,          \
+                            const mpi_int_t vt_root) {                                                             \
+    isvd_##x##NAME(param, argv, argc, retv, retc, dista, ordera, a, lda, qt, ldqt, s, ut, ldut, vt, ldvt, ut_root, \
+                   vt_root);                                                                                       \
+  }
+
+ISVD_STAGES(s, float)
+ISVD_STAGES(d, double)
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,211 @@
+// General strided matrix product on CUDA cores (FP64 / FP32), used by the NATIVE precision path
+// and for the small (Nl x l, l x l) products of the integration loop.
+//
+// Tiling: BM x BN output tile per 256-thread CTA, BK-deep K slices staged in shared memory
+// with register prefetch of the next slice; each thread owns a (BM/16) x (BN/16) register
+// block at rows ty + 16 i, cols tx + 16 j (conflict-free shared reads, coalesced stores).
+// Tall-skinny products (K >> M N) are split along K; partials are summed in FP64.
+#include <algorithm>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace isvdb {
+namespace {
+
+constexpr int kThreads = 256;
+
+template <class T, class Tout, int BM, int BN, int BK, bool A_KC, bool B_NC>
+__global__ void __launch_bounds__(kThreads)
+    gemm_kernel(const Gemm<T, Tout> g, const int splits, const int kchunk, T *__restrict__ partial) {
+  constexpr int TM = BM / 16, TN = BN / 16;
+  constexpr int LA = BM * BK / kThreads, LB = BK * BN / kThreads;
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
+  const int kb = sp * kchunk;
+  const int ke = min(g.K, kb + kchunk);
+  const T *__restrict__ A = g.A + (long long)b * g.a_bs;
+  const T *__restrict__ B = g.B + (long long)b * g.b_bs;
+
+  T acc[TM][TN];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+
+  T ra[LA], rb[LB];
+  auto a_idx = [](int e, int &mm, int &kk) {
+    if (A_KC) { kk = e % BK; mm = e / BK; } else { mm = e % BM; kk = e / BM; }
+  };
+  auto b_idx = [](int e, int &kk, int &nn) {
+    if (B_NC) { nn = e % BN; kk = e / BN; } else { kk = e % BK; nn = e / BK; }
+  };
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int r = 0; r < LA; ++r) {
+      int mm, kk;
+      a_idx(tid + r * kThreads, mm, kk);
+      const int gm = m0 + mm, gk = k0 + kk;
+      ra[r] = (gm < g.M && gk < ke) ? A[(long long)gm * g.a_rs + (long long)gk * g.a_cs] : T(0);
+    }
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      int kk, nn;
+      b_idx(tid + r * kThreads, kk, nn);
+      const int gn = n0 + nn, gk = k0 + kk;
+      rb[r] = (gn < g.N && gk < ke) ? B[(long long)gk * g.b_rs + (long long)gn * g.b_cs] : T(0);
+    }
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int r = 0; r < LA; ++r) {
+      int mm, kk;
+      a_idx(tid + r * kThreads, mm, kk);
+      As[kk][mm] = ra[r];
+    }
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      int kk, nn;
+      b_idx(tid + r * kThreads, kk, nn);
+      Bs[kk][nn] = rb[r];
+    }
+  };
+
+  if (kb < ke) load(kb);
+  for (int k0 = kb; k0 < ke; k0 += BK) {
+    store();
+    __syncthreads();
+    if (k0 + BK < ke) load(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T av[TM], bv[TN];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+
+  if (splits == 1) {
+    Tout *__restrict__ C = g.C + (long long)b * g.c_bs;
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gm = m0 + ty + 16 * i;
+      if (gm >= g.M) continue;
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const int gn = n0 + tx + 16 * j;
+        if (gn >= g.N) continue;
+        Tout *c = C + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+        double v = g.alpha * (double)acc[i][j];
+        if (g.beta != 0.0) v += g.beta * (double)(*c);
+        *c = (Tout)v;
+      }
+    }
+  } else {
+    T *__restrict__ P = partial + ((long long)blockIdx.z * g.M) * g.N;
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gm = m0 + ty + 16 * i;
+      if (gm >= g.M) continue;
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const int gn = n0 + tx + 16 * j;
+        if (gn < g.N) P[(long long)gm * g.N + gn] = acc[i][j];
+      }
+    }
+  }
+}
+
+template <class T, class Tout>
+__global__ void splitk_reduce_kernel(const Gemm<T, Tout> g, const int splits, const T *__restrict__ partial) {
+  const long long MN = (long long)g.M * g.N;
+  const long long total = MN * g.batch;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(e / MN);
+    const long long r = e - (long long)b * MN;
+    const int gm = (int)(r / g.N), gn = (int)(r - (long long)gm * g.N);
+    double s = 0.0;
+    const T *p = partial + ((long long)b * splits) * MN + r;
+    for (int sp = 0; sp < splits; ++sp) s += (double)p[(long long)sp * MN];
+    Tout *c = g.C + (long long)b * g.c_bs + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+    double v = g.alpha * s;
+    if (g.beta != 0.0) v += g.beta * (double)(*c);
+    *c = (Tout)v;
+  }
+}
+
+template <class T, class Tout, int BM, int BN, int BK>
+void launch(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, cudaStream_t st) {
+  Runtime &rt = Runtime::get();
+  const int gx = (g.M + BM - 1) / BM, gy = (g.N + BN - 1) / BN;
+  const long long tiles = (long long)gx * gy * g.batch;
+  int splits = g.splits;
+  if (splits <= 0) {
+    const long long target = 2LL * rt.num_sms;
+    splits = 1;
+    if (tiles < target) {
+      long long s = (target + tiles - 1) / tiles;
+      long long smax = std::max<long long>(1, g.K / (8 * BK));
+      splits = (int)std::min<long long>(s, smax);
+    }
+  }
+  int kchunk = (g.K + splits - 1) / splits;
+  kchunk = ((kchunk + BK - 1) / BK) * BK;
+  if (kchunk <= 0) kchunk = BK;
+  splits = std::max(1, (g.K + kchunk - 1) / kchunk);
+  DBuf<T> part;
+  if (splits > 1) part.alloc((size_t)g.batch * splits * g.M * g.N);
+  dim3 grid(gx, gy, g.batch * splits);
+#define ISVD_GEMM_CASE(AK, BN_)                                                                   \
+  if (a_kc == AK && b_nc == BN_) {                                                                \
+    gemm_kernel<T, Tout, BM, BN, BK, AK, BN_><<<grid, kThreads, 0, st>>>(g, splits, kchunk, part.p); \
+    KLAUNCHED();                                                                                  \
+  }
+  ISVD_GEMM_CASE(true, true)
+  ISVD_GEMM_CASE(true, false)
+  ISVD_GEMM_CASE(false, true)
+  ISVD_GEMM_CASE(false, false)
+#undef ISVD_GEMM_CASE
+  if (splits > 1) {
+    const long long total = (long long)g.M * g.N * g.batch;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * rt.num_sms);
+    splitk_reduce_kernel<T, Tout><<<blocks, 256, 0, st>>>(g, splits, part.p);
+    KLAUNCHED();
+  }
+}
+
+}  // namespace
+
+template <class T, class Tout>
+void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
+  if (g.K <= 0) {
+    if (g.beta == 1.0) return;
+    fail(kErrArgument, "gemm: empty inner dimension with beta != 1");
+  }
+  const bool a_kc = (g.a_cs == 1);
+  const bool b_nc = (g.b_cs == 1);
+  if (!a_kc && g.a_rs != 1) fail(kErrArgument, "gemm: operand A has no unit stride");
+  if (!b_nc && g.b_rs != 1) fail(kErrArgument, "gemm: operand B has no unit stride");
+  if (g.M <= 64 || g.N <= 64)
+    launch<T, Tout, 64, 64, 16>(g, a_kc, b_nc, st);
+  else
+    launch<T, Tout, 128, 128, 16>(g, a_kc, b_nc, st);
+}
+
+template void gemm<double, double>(const Gemm<double, double> &, cudaStream_t);
+template void gemm<float, float>(const Gemm<float, float> &, cudaStream_t);
+template void gemm<float, double>(const Gemm<float, double> &, cudaStream_t);
+
+}  // namespace isvdb

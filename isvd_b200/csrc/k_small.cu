@@ -1,0 +1,493 @@
+// Small dense FP64 linear algebra on l x l matrices (l <= 160), kept on chip:
+//   * batched symmetric eigendecomposition (parallel cyclic two-sided Jacobi),
+//   * batched general SVD (parallel cyclic one-sided Jacobi, Hestenes),
+//   * the Kolmogorov-Nagumo step C = (I/2 + (I/4 - Z)^(1/2))^(1/2) by coupled Newton-Schulz
+//     iterations in one cooperative multi-CTA kernel.
+// These replace LAPACK gesvd/syev (reference la/lapack/gesvd.c, syev.c) on the stages' l x l
+// matrices.  Jacobi methods are used because they are accurate to working precision in the
+// eigenvectors and map onto one CTA; rotation order is the round-robin tournament, so each
+// round applies l/2 disjoint rotations in parallel.
+#include <cmath>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace isvdb {
+namespace {
+
+constexpr int kEigThreads = 512;
+constexpr int kMaxSweeps = 60;
+
+// Round-robin tournament: player i at round r (ne even, player 0 fixed).
+__device__ __forceinline__ int rr_player(int i, int r, int ne) { return i == 0 ? 0 : 1 + (i - 1 + r) % (ne - 1); }
+
+// Rotation (c, s) annihilating the off-diagonal of [[app, apq], [apq, aqq]] with
+// R = [[c, s], [-s, c]] (Golub & Van Loan, Matrix Computations, Alg. 8.4.1 sym.schur2).
+__device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, double &c, double &s) {
+  if (apq == 0.0 || fabs(apq) <= 1e-300 || fabs(apq) <= 2.2e-16 * 0.25 * sqrt(fabs(app) * fabs(aqq))) {
+    c = 1.0;
+    s = 0.0;
+    return false;
+  }
+  const double tau = (aqq - app) / (2.0 * apq);
+  const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+  c = 1.0 / sqrt(1.0 + t * t);
+  s = t * c;
+  return true;
+}
+
+__global__ void __launch_bounds__(kEigThreads)
+    sym_eig_kernel(int n, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg, int order,
+                   bool absval, int *status) {
+  extern __shared__ double sm[];
+  const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const double *A0 = Ag + (size_t)b * n * n;
+  double *V = Vg + (size_t)b * n * n;
+  double *w = wg + (size_t)b * n;
+  const int ne = n + (n & 1), np = ne / 2;
+  double *A = sm;                       // n * n
+  double *rc = A + n * n;               // np
+  double *rs = rc + np;                 // np
+  double *key = rs + np;                // n
+  int *pp = (int *)(key + n);           // np
+  int *qq = pp + np;                    // np
+  int *flag = qq + np;                  // 1
+
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e - i * n;
+    A[e] = 0.5 * (A0[i * n + j] + A0[j * n + i]);
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+
+  int sweep = 0;
+  for (; sweep < kMaxSweeps; ++sweep) {
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int k = tid; k < np; k += nt) {
+        int p = rr_player(k, r, ne), q = rr_player(ne - 1 - k, r, ne);
+        if (p > q) { const int t = p; p = q; q = t; }
+        double c = 1.0, s = 0.0;
+        if (q < n && jacobi_rot(A[p * n + p], A[q * n + q], A[p * n + q], c, s)) *flag = 1;
+        pp[k] = p; qq[k] = q; rc[k] = c; rs[k] = s;
+      }
+      __syncthreads();
+      // A := R' A R on every 2 x 2 block of pair rows x pair columns (I <= J).
+      const int nblk = np * (np + 1) / 2;
+      for (int e = tid; e < nblk; e += nt) {
+        // decode e -> (I, J), I <= J
+        int I = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+        while ((I + 1) * (I + 2) / 2 <= e) ++I;
+        while (I * (I + 1) / 2 > e) --I;
+        int J = e - I * (I + 1) / 2;  // J <= I; swap roles so that we process (J, I)
+        const int pi = pp[J], qi = qq[J], pj = pp[I], qj = qq[I];
+        const double ci = rc[J], si = rs[J], cj = rc[I], sj = rs[I];
+        if (si == 0.0 && sj == 0.0) continue;
+        const bool qiv = qi < n, qjv = qj < n;
+        const double x11 = A[pi * n + pj];
+        const double x12 = qjv ? A[pi * n + qj] : 0.0;
+        const double x21 = qiv ? A[qi * n + pj] : 0.0;
+        const double x22 = (qiv && qjv) ? A[qi * n + qj] : 0.0;
+        // left: rows (pi, qi)
+        const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;
+        const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
+        // right: cols (pj, qj)
+        double z11 = y11 * cj - y12 * sj, z12 = y11 * sj + y12 * cj;
+        double z21 = y21 * cj - y22 * sj, z22 = y21 * sj + y22 * cj;
+        if (I == J) {
+          if (si != 0.0) { z12 = 0.0; z21 = 0.0; }
+          A[pi * n + pi] = z11;
+          if (qiv) { A[qi * n + qi] = z22; A[pi * n + qi] = z12; A[qi * n + pi] = z12; }
+        } else {
+          A[pi * n + pj] = z11; A[pj * n + pi] = z11;
+          if (qjv) { A[pi * n + qj] = z12; A[qj * n + pi] = z12; }
+          if (qiv) { A[qi * n + pj] = z21; A[pj * n + qi] = z21; }
+          if (qiv && qjv) { A[qi * n + qj] = z22; A[qj * n + qi] = z22; }
+        }
+      }
+      // V := V R (columns p, q of every row)
+      for (int e = tid; e < n * np; e += nt) {
+        const int row = e / np, k = e - row * np;
+        const double s = rs[k];
+        if (s == 0.0) continue;
+        const double c = rc[k];
+        const int p = pp[k], q = qq[k];
+        const double v1 = V[row * n + p], v2 = V[row * n + q];
+        V[row * n + p] = c * v1 - s * v2;
+        V[row * n + q] = s * v1 + c * v2;
+      }
+      __syncthreads();
+    }
+    const int f = *flag;
+    __syncthreads();
+    if (!f) break;
+  }
+  if (sweep == kMaxSweeps && tid == 0) atomicExch(status, kErrNumerical);
+
+  // Sort eigenpairs: order > 0 by |lambda| descending, order < 0 by lambda ascending.
+  for (int i = tid; i < n; i += nt) key[i] = A[i * n + i];
+  __syncthreads();
+  // reuse A as the permuted eigenvector buffer
+  for (int i = tid; i < n; i += nt) {
+    const double ki = key[i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double kj = key[j];
+      bool before;
+      if (order > 0) before = fabs(kj) > fabs(ki) || (fabs(kj) == fabs(ki) && j < i);
+      else before = kj < ki || (kj == ki && j < i);
+      rank += before;
+    }
+    w[rank] = absval ? fabs(ki) : ki;
+    pp[0] = pp[0];  // no-op keeps pp live
+    for (int r = 0; r < n; ++r) A[r * n + rank] = V[r * n + i];
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) V[e] = A[e];
+}
+
+// One-sided Jacobi SVD: B (row-major n x n) -> U diag(s) V'.
+// Columns of B are held column-major in shared memory; V in global memory (this CTA only).
+__global__ void __launch_bounds__(kEigThreads)
+    svd_jacobi_kernel(int n, const double *__restrict__ Bg, double *__restrict__ Ug, double *__restrict__ sg,
+                      double *__restrict__ Vg, int *status) {
+  extern __shared__ double sm[];
+  const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  const double *B0 = Bg + (size_t)b * n * n;
+  double *U = Ug + (size_t)b * n * n;
+  double *V = Vg + (size_t)b * n * n;
+  double *s = sg + (size_t)b * n;
+  const int ne = n + (n & 1), np = ne / 2;
+  double *X = sm;                  // column-major: X[j * n + i] = B(i, j)
+  double *nrm = X + n * n;         // n
+  int *flag = (int *)(nrm + n);
+
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e - i * n;
+    X[j * n + i] = B0[e];
+    V[e] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  int sweep = 0;
+  for (; sweep < kMaxSweeps; ++sweep) {
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    for (int r = 0; r < ne - 1; ++r) {
+      for (int k = warp; k < np; k += nwarp) {
+        int p = rr_player(k, r, ne), q = rr_player(ne - 1 - k, r, ne);
+        if (p > q) { const int t = p; p = q; q = t; }
+        if (q >= n) continue;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int i = lane; i < n; i += 32) {
+          const double xp = X[p * n + i], xq = X[q * n + i];
+          al += xp * xp; be += xq * xq; ga += xp * xq;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        if (ga == 0.0 || fabs(ga) <= 2.2e-16 * 0.25 * sqrt(al * be)) continue;
+        if (lane == 0) *flag = 1;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), sn = t * c;
+        for (int i = lane; i < n; i += 32) {
+          const double xp = X[p * n + i], xq = X[q * n + i];
+          X[p * n + i] = c * xp - sn * xq;
+          X[q * n + i] = sn * xp + c * xq;
+          const double vp = V[i * n + p], vq = V[i * n + q];
+          V[i * n + p] = c * vp - sn * vq;
+          V[i * n + q] = sn * vp + c * vq;
+        }
+      }
+      __syncthreads();
+    }
+    const int f = *flag;
+    __syncthreads();
+    if (!f) break;
+  }
+  if (sweep == kMaxSweeps && tid == 0) atomicExch(status, kErrNumerical);
+  for (int j = warp; j < n; j += nwarp) {
+    double a = 0.0;
+    for (int i = lane; i < n; i += 32) a += X[j * n + i] * X[j * n + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) nrm[j] = sqrt(a);
+  }
+  __syncthreads();
+  // sort by singular value descending; write U = X / s (row-major) and permuted V.
+  for (int j = tid; j < n; j += nt) {
+    const double sj = nrm[j];
+    int rank = 0;
+    for (int k = 0; k < n; ++k) rank += (nrm[k] > sj) || (nrm[k] == sj && k < j);
+    s[rank] = sj;
+    const double inv = sj > 0.0 ? 1.0 / sj : 0.0;
+    for (int i = 0; i < n; ++i) U[i * n + rank] = X[j * n + i] * inv;
+  }
+  __syncthreads();
+  // permute V columns through shared memory (X no longer needed)
+  for (int j = tid; j < n; j += nt) {
+    const double sj = nrm[j];
+    int rank = 0;
+    for (int k = 0; k < n; ++k) rank += (nrm[k] > sj) || (nrm[k] == sj && k < j);
+    for (int i = 0; i < n; ++i) X[i * n + rank] = V[i * n + j];
+  }
+  __syncthreads();
+  for (int e = tid; e < n * n; e += nt) V[e] = X[e];
+}
+
+// ------------------------------------------------------------------------------------------
+// Cooperative Kolmogorov-Nagumo step.
+
+constexpr int kKnThreads = 256;
+constexpr long long kSpinLimit = 1LL << 22;  // ~0.5-2 s of polling before giving up
+
+// Grid-wide barrier for a cooperative launch.  bar[0] counts arrivals, bar[1] is the generation.
+// Every wait is bounded; on expiry the status word is set and all CTAs leave the kernel.
+__device__ bool grid_barrier(unsigned int *bar, int *status) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *gen = bar + 1;
+    const unsigned int g = *gen;
+    __threadfence();
+    const unsigned int t = atomicAdd(bar, 1u);
+    if (t == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*gen == g) {
+        if (++spins > kSpinLimit) { atomicExch(status, kErrTimeout); break; }
+        if (*(volatile int *)status) break;
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok = (*(volatile int *)status == 0);
+  }
+  __syncthreads();
+  return ok;
+}
+
+// C = alpha * A * B + beta * Cin + diag * I over 16 x 16 tiles (row-major l x l, ld l).
+// All operands may have been written by other CTAs in earlier phases: loads go through L2.
+__device__ void mm_tiles(int l, int ntile_row, int tile_begin, int tile_end, double alpha, const double *A,
+                         const double *B, double beta, const double *Cin, double diag, double *C) {
+  __shared__ double As[16][161];
+  __shared__ double Bs[160][17];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int t = tile_begin + blockIdx.x; t < tile_end; t += gridDim.x) {
+    const int tt = t - tile_begin;
+    const int i0 = (tt / ntile_row) * 16, j0 = (tt % ntile_row) * 16;
+    __syncthreads();
+    for (int e = threadIdx.x; e < 16 * l; e += blockDim.x) {
+      const int r = e / l, k = e - r * l;
+      As[r][k] = (i0 + r < l) ? __ldcg(A + (size_t)(i0 + r) * l + k) : 0.0;
+    }
+    for (int e = threadIdx.x; e < 16 * l; e += blockDim.x) {
+      const int k = e / 16, c = e - k * 16;
+      Bs[k][c] = (j0 + c < l) ? __ldcg(B + (size_t)k * l + j0 + c) : 0.0;
+    }
+    __syncthreads();
+    const int i = i0 + ty, j = j0 + tx;
+    double acc = 0.0;
+    for (int k = 0; k < l; ++k) acc = fma(As[ty][k], Bs[k][tx], acc);
+    if (i < l && j < l) {
+      double v = alpha * acc;
+      if (beta != 0.0) v += beta * __ldcg(Cin + (size_t)i * l + j);
+      if (i == j) v += diag;
+      C[(size_t)i * l + j] = v;
+    }
+  }
+}
+
+// Number of coupled Newton-Schulz steps so that rho^(2^k) <= 1e-18 (rho: bound of ||I - X||_2).
+__device__ int ns_steps(double rho) {
+  if (!(rho < 0.999)) return 40;
+  if (rho < 1e-300) return 1;
+  const double need = 41.45 / -log(rho);  // ln(1e18)
+  int k = 0;
+  double p = 1.0;
+  while (p < need && k < 40) { p *= 2.0; ++k; }
+  return k + 1;
+}
+
+__global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
+  const int l = a.l;
+  const size_t ll = (size_t)l * l;
+  double *Zm = a.work, *Y0 = Zm + ll, *Y1 = Y0 + ll, *Q0 = Y1 + ll, *Q1 = Q0 + ll, *T = Q1 + ll;
+  double *scal = a.work + 8 * ll;  // [0] rho, [1] k
+  const int nr = (l + 15) / 16, nt = nr * nr;
+  __shared__ double red[kKnThreads];
+
+  // Z = Dgc - Dc Dc (reference :184-190)
+  mm_tiles(l, nr, 0, nt, -1.0, a.Dc, a.Dc, 1.0, a.Dgc, 0.0, Zm);
+  if (!grid_barrier(a.bar, a.status)) return;
+  // X = I - 4 Zsym (upper triangle of Z, as syev 'U' reads it); Y0 = X, Q0 = I.
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / l), j = (int)(e % l);
+    const double z = __ldcg(Zm + (size_t)min(i, j) * l + max(i, j));
+    Y0[e] = (i == j ? 1.0 : 0.0) - 4.0 * z;
+    Q0[e] = (i == j ? 1.0 : 0.0);
+  }
+  if (blockIdx.x == 0) {
+    // rho = min(||4Z||_F, ||4Z||_inf): deterministic (single CTA)
+    double f = 0.0;
+    for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
+      const int i = (int)(e / l), j = (int)(e % l);
+      const double z = __ldcg(Zm + (size_t)min(i, j) * l + max(i, j));
+      f += 16.0 * z * z;
+    }
+    red[threadIdx.x] = f;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    const double fro = sqrt(red[0]);
+    __syncthreads();
+    double rmax = 0.0;
+    for (int i = threadIdx.x; i < l; i += blockDim.x) {
+      double rs = 0.0;
+      for (int j = 0; j < l; ++j) rs += fabs(4.0 * __ldcg(Zm + (size_t)min(i, j) * l + max(i, j)));
+      rmax = fmax(rmax, rs);
+    }
+    red[threadIdx.x] = rmax;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      const double rho = fmin(fro, red[0]);
+      scal[0] = rho;
+      scal[1] = (double)ns_steps(rho);
+    }
+  }
+  if (!grid_barrier(a.bar, a.status)) return;
+
+  // Two coupled Newton-Schulz square roots (Higham, Functions of Matrices, eq. 6.35):
+  //   T = Q Y;  Y <- Y (3I - T)/2;  Q <- (3I - T) Q / 2   ->  Y -> X^(1/2), Q -> X^(-1/2).
+  for (int stage = 0; stage < 2; ++stage) {
+    const int k = (int)__ldcg(scal + 1);
+    double *Y = Y0, *Yn = Y1, *Q = Q0, *Qn = Q1;
+    for (int it = 0; it < k; ++it) {
+      mm_tiles(l, nr, 0, nt, 1.0, Q, Y, 0.0, nullptr, 0.0, T);
+      if (!grid_barrier(a.bar, a.status)) return;
+      mm_tiles(l, nr, 0, nt, -0.5, Y, T, 1.5, Y, 0.0, Yn);
+      mm_tiles(l, nr, nt, 2 * nt, -0.5, T, Q, 1.5, Q, 0.0, Qn);
+      if (!grid_barrier(a.bar, a.status)) return;
+      double *t1 = Y; Y = Yn; Yn = t1;
+      double *t2 = Q; Q = Qn; Qn = t2;
+    }
+    if (stage == 0) {
+      // sqrt(I/4 - Z) = Y / 2 ;  P = I/2 + Y/2 ; next: Y0 = P, Q0 = I
+      for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / l), j = (int)(e % l);
+        const double p = 0.5 * __ldcg(Y + e) + (i == j ? 0.5 : 0.0);
+        T[e] = p;
+      }
+      if (!grid_barrier(a.bar, a.status)) return;
+      for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / l), j = (int)(e % l);
+        Y0[e] = __ldcg(T + e);
+        Q0[e] = (i == j ? 1.0 : 0.0);
+      }
+      if (blockIdx.x == 0) {
+        double f = 0.0;
+        for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
+          const int i = (int)(e / l), j = (int)(e % l);
+          const double d = (i == j ? 1.0 : 0.0) - __ldcg(T + e);
+          f += d * d;
+        }
+        red[threadIdx.x] = f;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+          if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+          __syncthreads();
+        }
+        if (threadIdx.x == 0) scal[1] = (double)ns_steps(fmin(sqrt(red[0]), 0.5));
+      }
+      if (!grid_barrier(a.bar, a.status)) return;
+    } else {
+      // C = Y, Cinv = Q; F = C - Dc Cinv; err = ||C - I||_F
+      for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
+        a.C[e] = __ldcg(Y + e);
+        a.Cinv[e] = __ldcg(Q + e);
+      }
+      if (!grid_barrier(a.bar, a.status)) return;
+      mm_tiles(l, nr, 0, nt, -1.0, a.Dc, a.Cinv, 1.0, a.C, 0.0, a.F);
+      if (blockIdx.x == 0) {
+        double f = 0.0;
+        for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
+          const int i = (int)(e / l), j = (int)(e % l);
+          const double d = __ldcg(a.C + e) - (i == j ? 1.0 : 0.0);
+          f += d * d;
+        }
+        red[threadIdx.x] = f;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+          if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+          __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+          const double err = sqrt(red[0]);
+          *a.err = err;
+          if (!(err == err)) atomicExch(a.status, kErrNumerical);
+        }
+      }
+    }
+  }
+}
+
+size_t eig_smem(int n) {
+  const int ne = n + (n & 1), np = ne / 2;
+  return (size_t)n * n * 8 + (size_t)np * 16 + (size_t)n * 8 + (size_t)np * 8 + 16;
+}
+size_t svd_smem(int n) { return (size_t)n * n * 8 + (size_t)n * 8 + 16; }
+
+}  // namespace
+
+void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, int order, bool absval, int *status,
+                     cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return;
+  Runtime &rt = Runtime::get();
+  const size_t smem = eig_smem(n);
+  if (smem > rt.smem_optin) fail(kErrUnsupported, "symmetric eigensolver: l = %d exceeds on-chip capacity", n);
+  CK(cudaFuncSetAttribute(sym_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  sym_eig_kernel<<<batch, kEigThreads, smem, st>>>(n, A, V, w, order, absval, status);
+  KLAUNCHED();
+}
+
+void svd_jacobi_batched(int n, int batch, const double *B, double *U, double *s, double *V, int *status,
+                        cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return;
+  Runtime &rt = Runtime::get();
+  const size_t smem = svd_smem(n);
+  if (smem > rt.smem_optin) fail(kErrUnsupported, "Jacobi SVD: l = %d exceeds on-chip capacity", n);
+  CK(cudaFuncSetAttribute(svd_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  svd_jacobi_kernel<<<batch, kEigThreads, smem, st>>>(n, B, U, s, V, status);
+  KLAUNCHED();
+}
+
+void kn_step(const KnStep &a, cudaStream_t st) {
+  Runtime &rt = Runtime::get();
+  if (a.l > 160) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > 160", a.l);
+  const int nr = (a.l + 15) / 16;
+  int blocks = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kn_step_kernel, kKnThreads, 0));
+  int grid = std::min(2 * nr * nr, blocks * rt.num_sms);
+  grid = std::max(1, std::min(grid, rt.num_sms));
+  KnStep arg = a;
+  void *args[] = {&arg};
+  CK(cudaLaunchCooperativeKernel((void *)kn_step_kernel, dim3(grid), dim3(kKnThreads), args, 0, st));
+  KLAUNCHED();
+}
+
+}  // namespace isvdb

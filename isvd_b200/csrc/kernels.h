@@ -1,0 +1,83 @@
+// Launchers of the device kernels of libisvd_gpu_b200 (all enqueue on the library stream).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace isvdb {
+
+// ------------------------------------------------------------------ general matrix product
+// C(b) = alpha * A(b) * B(b) + beta * C(b) for b < batch, with
+//   A(i,k) = A[i*a_rs + k*a_cs],  B(k,j) = B[k*b_rs + j*b_cs],  C(i,j) = C[i*c_rs + j*c_cs]
+// and batch offsets a_bs / b_bs / c_bs.  One of each (rs, cs) pair must be 1.
+// Tout may be wider than T (double output of float products: split-K partials are
+// summed in double).
+template <class T, class Tout>
+struct Gemm {
+  int M = 0, N = 0, K = 0;
+  double alpha = 1.0, beta = 0.0;
+  const T *A = nullptr;
+  long long a_rs = 0, a_cs = 0, a_bs = 0;
+  const T *B = nullptr;
+  long long b_rs = 0, b_cs = 0, b_bs = 0;
+  Tout *C = nullptr;
+  long long c_rs = 0, c_cs = 0, c_bs = 0;
+  int batch = 1;
+  int splits = 0;  // 0: choose automatically
+};
+
+template <class T, class Tout>
+void gemm(const Gemm<T, Tout> &g, cudaStream_t st);
+
+// ------------------------------------------------------------------ elementwise
+// Omega(j, c) for j < rows, c < cols: standard normal values from Philox4x32-10 (key = seed)
+// with Box-Muller; value index = offset + j * cols + c.  Written at out[j*ld + c].
+template <class T>
+void rng_gaussian(T *out, long long rows, long long cols, long long ld, uint64_t seed, uint64_t offset,
+                  cudaStream_t st);
+
+// dst(i, j) = src(i, j) with arbitrary strides, converting type.
+template <class Ts, class Td>
+void copy2d(const Ts *src, long long s_rs, long long s_cs, Td *dst, long long d_rs, long long d_cs, long long rows,
+            long long cols, cudaStream_t st);
+
+// A (rows x cols, row-major, ld) := identity-padded: A(i,j) = (i == j)
+template <class T>
+void set_identity(T *a, long long rows, long long cols, long long ld, cudaStream_t st);
+
+// Column scaling: dst(i, j) = f(src(i, j), s[(i / rows_per_batch) * cols + j]) with
+//   kScaleMul: x * s,  kScaleDiv: x / s,  kScaleInvSqrt: x / sqrt(s),
+//   kScaleHr: x / sqrt(2 (1 + s)),  kSqrtOnly: sqrt(x)  (s unused).
+enum ScaleMode : int { kScaleMul = 0, kScaleDiv = 1, kScaleInvSqrt = 2, kScaleHr = 3, kSqrtOnly = 4 };
+template <class Ts, class Td>
+void scale_cols_batched(const Ts *src, long long lds, Td *dst, long long ldd, long long rows, long long cols,
+                        long long rows_per_batch, const double *s, int mode, cudaStream_t st);
+
+// ------------------------------------------------------------------ small dense FP64 (l x l)
+// Batched symmetric eigendecomposition by parallel cyclic Jacobi, one CTA per matrix.
+// A: batch x (n x n) row-major (only read), V: batch x (n x n) row-major eigenvectors (columns),
+// w: batch x n eigenvalues.  order > 0: sort by |lambda| descending (gesvd of a PSD matrix);
+// order < 0: ascending lambda (syev).  absval: return |lambda| in w.
+void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, int order, bool absval,
+                     int *status, cudaStream_t st);
+
+// Batched general SVD B = U diag(s) V' by one-sided Jacobi, one CTA per matrix.
+// B, U, V: batch x (n x n) row-major; s descending.
+void svd_jacobi_batched(int n, int batch, const double *B, double *U, double *s, double *V, int *status,
+                        cudaStream_t st);
+
+// Kolmogorov-Nagumo l x l step (reference core/stage/@x@_integrate_kolmogorov_nagumo.c:180-234):
+//   Z = Dgc - Dc^2; C = sqrt(I/2 + sqrt(I/4 - Z)); Cinv = C^-1; err = ||C - I||_F; F = C - Dc Cinv.
+// Matrix square roots by coupled Newton-Schulz iterations in a cooperative multi-CTA kernel.
+struct KnStep {
+  int l;
+  const double *Dc, *Dgc;
+  double *C, *Cinv, *F, *err;
+  double *work;     // 8 * l * l doubles + 64
+  int *status;      // set nonzero on failure (timeout / no convergence)
+  unsigned int *bar;  // 2 words, zero
+};
+void kn_step(const KnStep &a, cudaStream_t st);
+
+}  // namespace isvdb

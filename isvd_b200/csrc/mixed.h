@@ -1,0 +1,41 @@
+// MIXED precision engine: BF16x3 split products on tcgen05 tensor cores with FP32 accumulation.
+// Each FP32/FP64 operand x is split into bf16 pieces x = x0 + x1 + x2 (+ residual); a product
+// keeps the piece pairs whose combined magnitude is above the FP32 rounding level.
+#pragma once
+
+#include <cstdint>
+
+#include "stages.h"
+
+namespace isvdb {
+
+// Y = A * Omega (m x Nl, row-major ldy).  omega == nullptr: Omega is drawn exactly in bf16
+// (Philox + Box-Muller, rounded), so only A is split (3 products).  Otherwise Omega is split too.
+template <class T>
+void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
+                  long long ldom, uint64_t seed, T *y, long long ldy);
+
+// W_i = Y_i' Y_i for the N column blocks of Y (m x Nl, ld ldy) -> W (N x l x l, FP64).
+template <class T>
+void mixed_block_gram(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, double *W);
+
+// Q_i = Y_i Wp_i (Wp: N x l x l in T) -> out (m x Nl, ld ldo).
+template <class T>
+void mixed_block_apply(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, const T *Wp, T *out,
+                       long long ldo);
+
+// G = Qs' Qs (Nl x Nl, FP64 out).
+template <class T>
+void mixed_gram_full(const StageCtx &c, int m, int Nl, const T *qs, long long ldq, double *G);
+
+// Qbar = Qs M (M: Nl x l FP64, row-major) -> qt (m x l, ld ldqt).
+template <class T>
+void mixed_apply_coeff(const StageCtx &c, int m, int Nl, int l, const T *qs, long long ldq, const double *M, T *qt,
+                       long long ldqt);
+
+// Z = A' Qbar (n x l row-major).
+template <class T>
+void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+                   long long ldqt, T *z);
+
+}  // namespace isvdb

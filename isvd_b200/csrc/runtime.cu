@@ -1,0 +1,110 @@
+// Device context, errors and stream-ordered allocation for libisvd_gpu_b200.
+#include "runtime.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+
+namespace isvdb {
+
+std::atomic<unsigned long long> g_launches{0};
+
+static Runtime g_rt;
+static bool g_init = false;
+static std::mutex g_init_mu;
+static int g_precision = -1;
+
+void fail(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  throw Error(code, buf);
+}
+
+void check_cuda(cudaError_t e, const char *what, const char *file, int line) {
+  if (e == cudaSuccess) return;
+  int code = (e == cudaErrorMemoryAllocation) ? kErrMemory : kErrCuda;
+  fail(code, "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e), cudaGetErrorString(e), what, file, line);
+}
+
+bool Runtime::initialised() { return g_init; }
+
+Runtime &Runtime::get() {
+  if (g_init) return g_rt;
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (g_init) return g_rt;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  g_rt.device = dev;
+  g_rt.num_sms = prop.multiProcessorCount;
+  g_rt.cc_major = prop.major;
+  g_rt.cc_minor = prop.minor;
+  g_rt.smem_optin = prop.sharedMemPerBlockOptin;
+  CK(cudaStreamCreateWithFlags(&g_rt.stream, cudaStreamNonBlocking));
+  // Keep freed pool memory cached: repeated solves reuse it without new cudaMalloc calls.
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t thr = UINT64_MAX;
+  CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+  CK(cudaMalloc(&g_rt.ctl, 4096));
+  CK(cudaMemset(g_rt.ctl, 0, 4096));
+  g_init = true;
+  return g_rt;
+}
+
+void Runtime::reset() {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if (!g_init) return;
+  cudaStreamSynchronize(g_rt.stream);
+  cudaFree(g_rt.ctl);
+  cudaStreamDestroy(g_rt.stream);
+  g_rt = Runtime();
+  g_init = false;
+}
+
+int default_precision() {
+  if (g_precision < 0) {
+    const char *e = getenv("ISVD_GPU_PRECISION");
+    g_precision = (e && (!strcmp(e, "mixed") || !strcmp(e, "1"))) ? kMixed : kNative;
+  }
+  return g_precision;
+}
+
+void set_default_precision(int p) { g_precision = p; }
+
+void *dev_alloc(size_t bytes) {
+  Runtime &rt = Runtime::get();
+  void *p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, rt.stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(kErrMemory, "device allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
+  }
+  return p;
+}
+
+void dev_free(void *p) {
+  if (!p || !g_init) return;
+  cudaFreeAsync(p, g_rt.stream);
+}
+
+bool is_device_pointer(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes attr;
+  cudaError_t e = cudaPointerGetAttributes(&attr, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void sync() { CK(cudaStreamSynchronize(Runtime::get().stream)); }
+
+}  // namespace isvdb

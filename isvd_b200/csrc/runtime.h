@@ -1,0 +1,103 @@
+// Host-side runtime of libisvd_gpu_b200: device context, stream, errors, device buffers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace isvdb {
+
+// Status codes (mirror include/isvd/b200.h).
+enum Status : int {
+  kSuccess = 0,
+  kErrArgument = 1,
+  kErrCuda = 2,
+  kErrMemory = 3,
+  kErrTimeout = 4,
+  kErrNumerical = 5,
+  kErrUnsupported = 6,
+};
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] void fail(int code, const char *fmt, ...);
+void check_cuda(cudaError_t e, const char *what, const char *file, int line);
+
+#define CK(x) ::isvdb::check_cuda((x), #x, __FILE__, __LINE__)
+
+extern std::atomic<unsigned long long> g_launches;
+// Every kernel launch of the library goes through KLAUNCHED() right after the <<<>>>.
+#define KLAUNCHED()                                    \
+  do {                                                 \
+    ::isvdb::g_launches.fetch_add(1);                  \
+    ::isvdb::check_cuda(cudaGetLastError(), "kernel launch", __FILE__, __LINE__); \
+  } while (0)
+
+enum Precision : int { kNative = 0, kMixed = 1 };
+
+struct Runtime {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  int cc_major = 0, cc_minor = 0;
+  size_t smem_optin = 0;
+  // Device-resident control block (barrier counters, status words), zeroed at init.
+  unsigned int *ctl = nullptr;
+  static Runtime &get();  // initialises on first use (device = current device)
+  static bool initialised();
+  static void reset();    // releases stream and control block (isvd_Finalize_gpu)
+};
+
+int default_precision();
+void set_default_precision(int p);
+
+// Stream-ordered device buffer (cudaMallocAsync on the library stream; pool memory is retained).
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  explicit DBuf(size_t count) { alloc(count); }
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  DBuf(DBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf &operator=(DBuf &&o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void alloc(size_t count);
+  void release();
+  T *get() const { return p; }
+  operator T *() const { return p; }
+};
+
+void *dev_alloc(size_t bytes);
+void dev_free(void *p);
+
+template <class T>
+void DBuf<T>::alloc(size_t count) {
+  release();
+  n = count;
+  p = count ? static_cast<T *>(dev_alloc(count * sizeof(T))) : nullptr;
+}
+template <class T>
+void DBuf<T>::release() {
+  if (p) dev_free(p);
+  p = nullptr;
+  n = 0;
+}
+
+// Pointer classification: true when the GPU can dereference `p` directly.
+bool is_device_pointer(const void *p);
+
+void sync();  // synchronise the library stream, converting errors into Error
+
+}  // namespace isvdb

@@ -1,0 +1,338 @@
+// Device-level iSVD stages (one MPI rank).  NATIVE precision: products in the stage's type on
+// CUDA cores; l x l steps in FP64.  MIXED precision routes the large products to the tcgen05
+// BF16x3 engine (mixed.cu).
+#include <cmath>
+#include <vector>
+
+#include "kernels.h"
+#include "mixed.h"
+#include "runtime.h"
+#include "stages.h"
+
+namespace isvdb {
+namespace {
+
+template <class T>
+inline Gemm<T, T> gm(int M, int N, int K) {
+  Gemm<T, T> g;
+  g.M = M; g.N = N; g.K = K;
+  return g;
+}
+
+// A(i, j) of an m x n matrix stored per ordera ('R' row-major, 'C' column-major).
+template <class G>
+inline void set_a(G &g, char ordera, long long lda, bool transpose) {
+  const bool row = (ordera == 'R');
+  long long rs = row ? lda : 1, cs = row ? 1 : lda;
+  if (transpose) { long long t = rs; rs = cs; cs = t; }
+  g.a_rs = rs; g.a_cs = cs;
+}
+
+void read_status(const StageCtx &c, const char *what) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c.status, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  CK(cudaStreamSynchronize(c.st));
+  if (h == kErrTimeout) fail(kErrTimeout, "%s: a device-side wait timed out", what);
+  if (h) fail(kErrNumerical, "%s: small dense solver reported status %d", what, h);
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------ sketch
+template <class T>
+void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
+                long long ldom, uint64_t seed, T *y, long long ldy) {
+  if (c.precision == kMixed) {
+    mixed_sketch<T>(c, m, n, Nl, ordera, a, lda, omega, ldom, seed, y, ldy);
+    return;
+  }
+  DBuf<T> om;
+  if (!omega) {
+    om.alloc((size_t)n * Nl);
+    rng_gaussian<T>(om.p, n, Nl, Nl, seed, 0, c.st);
+    omega = om.p;
+    ldom = Nl;
+  }
+  Gemm<T, T> g = gm<T>(m, Nl, n);
+  g.A = a; set_a(g, ordera, lda, false);
+  g.B = omega; g.b_rs = ldom; g.b_cs = 1;
+  g.C = y; g.c_rs = ldy; g.c_cs = 1;
+  gemm(g, c.st);
+}
+
+// -------------------------------------------------------------------------- orthogonalize
+template <class T>
+void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy) {
+  const int Nl = N * l;
+  DBuf<double> W((size_t)N * l * l), V((size_t)N * l * l), w((size_t)N * l);
+  // W_i = Y_i' Y_i   (reference :82-84)
+  if (c.precision == kMixed) {
+    mixed_block_gram<T>(c, m, l, N, y, ldy, W.p);
+  } else {
+    Gemm<T, double> g;
+    g.M = l; g.N = l; g.K = m; g.batch = N;
+    g.A = y; g.a_rs = 1; g.a_cs = ldy; g.a_bs = l;
+    g.B = y; g.b_rs = ldy; g.b_cs = 1; g.b_bs = l;
+    g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)l * l;
+    gemm(g, c.st);
+  }
+  // eig(W_i) = W_i S_i^2 W_i'  (gesvd 'O' of the PSD Gram: |lambda| descending, :88-91)
+  sym_eig_batched(l, N, W.p, V.p, w.p, +1, true, c.status, c.st);
+  // W_i / S_i with S = sqrt(s)  (:94)
+  DBuf<T> Wp((size_t)N * l * l);
+  scale_cols_batched<double, T>(V.p, l, Wp.p, l, (long long)N * l, l, l, w.p, kScaleInvSqrt, c.st);
+  // Q_i = Y_i W_i / S_i  (:95-98; the reference copies Y first, here the product goes to a
+  // temporary and is copied back)
+  DBuf<T> tmp((size_t)m * Nl);
+  if (c.precision == kMixed) {
+    mixed_block_apply<T>(c, m, l, N, y, ldy, Wp.p, tmp.p, Nl);
+  } else {
+    Gemm<T, T> g = gm<T>(m, l, l);
+    g.batch = N;
+    g.A = y; g.a_rs = ldy; g.a_cs = 1; g.a_bs = l;
+    g.B = Wp.p; g.b_rs = l; g.b_cs = 1; g.b_bs = (long long)l * l;
+    g.C = tmp.p; g.c_rs = Nl; g.c_cs = 1; g.c_bs = l;
+    gemm(g, c.st);
+  }
+  CK(cudaMemcpy2DAsync(y, ldy * sizeof(T), tmp.p, (size_t)Nl * sizeof(T), (size_t)Nl * sizeof(T), m,
+                       cudaMemcpyDeviceToDevice, c.st));
+  read_status(c, "Gramian orthogonalization");
+}
+
+// ------------------------------------------------------------------------------- integrate
+//
+// Kolmogorov-Nagumo (reference @x@_integrate_kolmogorov_nagumo.c:153-266), carried in the
+// coordinates of Qs: with G = Qs' Qs (Nl x Nl), every m x l iterate is Qs * M for an Nl x l
+// coefficient matrix M, and
+//   Bc = Qs' Qc = G Mc,  Gc = Qs Bc / N  ->  coefficients Bc / N,  Bgc = Qs' Gc = G Bc / N,
+//   Q+ = Qc Fc + Gc C^-1  ->  M+ = Mc Fc + (Bc / N) C^-1,   B+ = Bc Fc + Bgc C^-1  (as the reference).
+// Each iteration then costs 2 Nl^2 l flops instead of 4 m Nl l, and Qbar = Qs M at the end.
+template <class T>
+IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs, long long ldq, T *qt,
+                            long long ldqt, int maxit, double tol) {
+  const int Nl = N * l;
+  const size_t nl = (size_t)Nl * l, ll = (size_t)l * l;
+  DBuf<double> G((size_t)Nl * Nl);
+  if (c.precision == kMixed) {
+    mixed_gram_full<T>(c, m, Nl, qs, ldq, G.p);
+  } else {
+    Gemm<T, double> g;
+    g.M = Nl; g.N = Nl; g.K = m;
+    g.A = qs; g.a_rs = 1; g.a_cs = ldq;
+    g.B = qs; g.b_rs = ldq; g.b_cs = 1;
+    g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  DBuf<double> Bb(2 * nl), Mb(2 * nl), Bgc(nl), Dc(ll), Dgc(ll), C(ll), Ci(ll), F(ll), work(8 * ll + 64), err(1);
+  double *Bc = Bb.p, *Bp = Bb.p + nl, *Mc = Mb.p, *Mp = Mb.p + nl;
+  copy2d<double, double>(G.p, Nl, 1, Bc, l, 1, Nl, l, c.st);   // Bc = Qs' Q0 = G[:, 0:l]   (:157)
+  set_identity<double>(Mc, Nl, l, l, c.st);                   // Qc = Q0 = Qs [I; 0]       (:154)
+  Runtime &rt = Runtime::get();
+  const double invN = 1.0 / N;
+  IterResult res;
+  double herr = 0.0;
+  const int cap = maxit > 0 ? maxit : 1000000;
+  int iter = 1;
+  for (;; ++iter) {
+    {  // Bgc = G Bc / N   (:174-177)
+      Gemm<double, double> g = gm<double>(Nl, l, Nl);
+      g.alpha = invN;
+      g.A = G.p; g.a_rs = Nl; g.a_cs = 1;
+      g.B = Bc; g.b_rs = l; g.b_cs = 1;
+      g.C = Bgc.p; g.c_rs = l; g.c_cs = 1;
+      gemm(g, c.st);
+    }
+    {  // Dc = Bc' Bc / N ; Dgc = Bc' Bgc / N   (:181-184)
+      Gemm<double, double> g = gm<double>(l, l, Nl);
+      g.alpha = invN;
+      g.A = Bc; g.a_rs = 1; g.a_cs = l;
+      g.B = Bc; g.b_rs = l; g.b_cs = 1;
+      g.C = Dc.p; g.c_rs = l; g.c_cs = 1;
+      gemm(g, c.st);
+      g.B = Bgc.p;
+      g.C = Dgc.p;
+      gemm(g, c.st);
+    }
+    // l x l step (:187-218)
+    CK(cudaMemsetAsync(rt.ctl, 0, 8, c.st));
+    KnStep s;
+    s.l = l; s.Dc = Dc.p; s.Dgc = Dgc.p; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = err.p;
+    s.work = work.p; s.status = c.status; s.bar = rt.ctl;
+    kn_step(s, c.st);
+    {  // M+ = Mc F + (Bc / N) C^-1 ;  B+ = Bc F + Bgc C^-1   (:221-226)
+      Gemm<double, double> g = gm<double>(Nl, l, l);
+      g.A = Mc; g.a_rs = l; g.a_cs = 1;
+      g.B = F.p; g.b_rs = l; g.b_cs = 1;
+      g.C = Mp; g.c_rs = l; g.c_cs = 1;
+      gemm(g, c.st);
+      g.A = Bc; g.B = Ci.p; g.alpha = invN; g.beta = 1.0;
+      gemm(g, c.st);
+      g.A = Bc; g.B = F.p; g.C = Bp; g.alpha = 1.0; g.beta = 0.0;
+      gemm(g, c.st);
+      g.A = Bgc.p; g.B = Ci.p; g.beta = 1.0;
+      gemm(g, c.st);
+    }
+    CK(cudaMemcpyAsync(&herr, err.p, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    read_status(c, "Kolmogorov-Nagumo integration");
+    if (herr <= tol) break;                                    // (:235-237)
+    if (iter == cap) { ++iter; break; }                        // (:238-241)
+    std::swap(Bc, Bp);
+    std::swap(Mc, Mp);
+  }
+  res.iterations = iter;
+  res.error = herr;
+  // Qbar = Qs M+  (:251)
+  if (c.precision == kMixed) {
+    mixed_apply_coeff<T>(c, m, Nl, l, qs, ldq, Mp, qt, ldqt);
+  } else {
+    DBuf<T> Mt(nl);
+    copy2d<double, T>(Mp, l, 1, Mt.p, l, 1, Nl, l, c.st);
+    Gemm<T, T> g = gm<T>(m, l, Nl);
+    g.A = qs; g.a_rs = ldq; g.a_cs = 1;
+    g.B = Mt.p; g.b_rs = l; g.b_cs = 1;
+    g.C = qt; g.c_rs = ldqt; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  return res;
+}
+
+// Hierarchical reduction (reference @x@_integrate_hierarchical_reduction.c:90-130).
+template <class T>
+void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt) {
+  const size_t ll = (size_t)l * l;
+  const int hmax = N / 2 > 0 ? N / 2 : 1;
+  DBuf<double> Bs(hmax * ll), W(hmax * ll), Vv(hmax * ll), s((size_t)hmax * l);
+  DBuf<T> Wt(hmax * ll), Tt(hmax * ll), tmp((size_t)m * l * hmax);
+  for (int h2 = N; h2 > 1; h2 = (h2 + 1) / 2) {
+    const int h = h2 / 2;
+    {  // B(i) = Q(i)' Q(i+h)
+      Gemm<T, double> g;
+      g.M = l; g.N = l; g.K = m; g.batch = h;
+      g.A = qs; g.a_rs = 1; g.a_cs = ldq; g.a_bs = l;
+      g.B = qs + (size_t)h * l; g.b_rs = ldq; g.b_cs = 1; g.b_bs = l;
+      g.C = Bs.p; g.c_rs = l; g.c_cs = 1; g.c_bs = ll;
+      gemm(g, c.st);
+    }
+    // svd(B(i)) = W S T'
+    svd_jacobi_batched(l, h, Bs.p, W.p, s.p, Vv.p, c.status, c.st);
+    // Q(i) := (Q(i) W + Q(i+h) T) / sqrt(2 (1 + s))
+    scale_cols_batched<double, T>(W.p, l, Wt.p, l, (long long)h * l, l, l, s.p, kScaleHr, c.st);
+    scale_cols_batched<double, T>(Vv.p, l, Tt.p, l, (long long)h * l, l, l, s.p, kScaleHr, c.st);
+    Gemm<T, T> g = gm<T>(m, l, l);
+    g.batch = h;
+    g.A = qs; g.a_rs = ldq; g.a_cs = 1; g.a_bs = l;
+    g.B = Wt.p; g.b_rs = l; g.b_cs = 1; g.b_bs = ll;
+    g.C = tmp.p; g.c_rs = (long long)l * h; g.c_cs = 1; g.c_bs = l;
+    gemm(g, c.st);
+    g.A = qs + (size_t)h * l; g.B = Tt.p; g.beta = 1.0;
+    gemm(g, c.st);
+    CK(cudaMemcpy2DAsync(qs, ldq * sizeof(T), tmp.p, (size_t)l * h * sizeof(T), (size_t)l * h * sizeof(T), m,
+                         cudaMemcpyDeviceToDevice, c.st));
+  }
+  CK(cudaMemcpy2DAsync(qt, ldqt * sizeof(T), qs, ldq * sizeof(T), (size_t)l * sizeof(T), m,
+                       cudaMemcpyDeviceToDevice, c.st));
+  read_status(c, "hierarchical reduction");
+}
+
+// ----------------------------------------------------------------------------- postprocess
+// Z = A' Qbar (reference @x@_postprocess.h:96-171, row block at P = 1).
+template <class T>
+static void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+                    long long ldqt, T *z) {
+  if (c.precision == kMixed) {
+    mixed_project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, z);
+    return;
+  }
+  Gemm<T, T> g = gm<T>(n, l, m);
+  g.A = a; set_a(g, ordera, lda, true);
+  g.B = qt; g.b_rs = ldqt; g.b_cs = 1;
+  g.C = z; g.c_rs = l; g.c_cs = 1;
+  gemm(g, c.st);
+}
+
+template <class T>
+void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
+                      const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
+                      bool wv) {
+  const size_t ll = (size_t)l * l;
+  DBuf<T> Z((size_t)n * l);
+  project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
+  DBuf<double> W(ll), V(ll), w(l);
+  {  // W = Z' Z  (reference @x@_postprocess_gramian.c:145)
+    Gemm<T, double> g;
+    g.M = l; g.N = l; g.K = n;
+    g.A = Z.p; g.a_rs = 1; g.a_cs = l;
+    g.B = Z.p; g.b_rs = l; g.b_cs = 1;
+    g.C = W.p; g.c_rs = l; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  sym_eig_batched(l, 1, W.p, V.p, w.p, +1, true, c.status, c.st);   // gesvd of W (:150)
+  scale_cols_batched<double, T>(w.p, 1, s, 1, l, 1, l, w.p, kSqrtOnly, c.st);  // sigma = sqrt(s) (:151)
+  if (wu) {  // U = Qbar W[:, :k]  (:158)
+    DBuf<T> Wk(ll);
+    copy2d<double, T>(V.p, l, 1, Wk.p, l, 1, l, l, c.st);
+    Gemm<T, T> g = gm<T>(m, k, l);
+    g.A = qt; g.a_rs = ldqt; g.a_cs = 1;
+    g.B = Wk.p; g.b_rs = l; g.b_cs = 1;
+    g.C = ut; g.c_rs = ldut; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  if (wv) {  // V = Z W[:, :k] / sigma  (:173-174)
+    DBuf<T> Ws(ll);
+    scale_cols_batched<double, T>(V.p, l, Ws.p, l, l, l, l, w.p, kScaleInvSqrt, c.st);
+    Gemm<T, T> g = gm<T>(n, k, l);
+    g.A = Z.p; g.a_rs = l; g.a_cs = 1;
+    g.B = Ws.p; g.b_rs = l; g.b_cs = 1;
+    g.C = vt; g.c_rs = ldvt; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  read_status(c, "Gramian postprocessing");
+}
+
+// Symmetric postprocessing (reference @x@_postprocess_symmetric.c:139-157): W = Qbar' A Qbar,
+// syev (ascending), U = Qbar W[:, :k].
+template <class T>
+void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
+                        const T *qt, long long ldqt, T *s, T *ut, long long ldut, bool wu) {
+  const size_t ll = (size_t)l * l;
+  DBuf<T> Z((size_t)n * l);
+  project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
+  DBuf<double> W(ll), V(ll), w(l);
+  {
+    Gemm<T, double> g;
+    g.M = l; g.N = l; g.K = n;
+    g.A = Z.p; g.a_rs = 1; g.a_cs = l;
+    g.B = qt; g.b_rs = ldqt; g.b_cs = 1;
+    g.C = W.p; g.c_rs = l; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  sym_eig_batched(l, 1, W.p, V.p, w.p, -1, false, c.status, c.st);
+  copy2d<double, T>(w.p, 1, 1, s, 1, 1, l, 1, c.st);
+  if (wu) {
+    DBuf<T> Wk(ll);
+    copy2d<double, T>(V.p, l, 1, Wk.p, l, 1, l, l, c.st);
+    Gemm<T, T> g = gm<T>(m, k, l);
+    g.A = qt; g.a_rs = ldqt; g.a_cs = 1;
+    g.B = Wk.p; g.b_rs = l; g.b_cs = 1;
+    g.C = ut; g.c_rs = ldut; g.c_cs = 1;
+    gemm(g, c.st);
+  }
+  read_status(c, "symmetric postprocessing");
+}
+
+#define ISVD_INST(T)                                                                                          \
+  template void sketch_dev<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, \
+                              uint64_t, T *, long long);                                                        \
+  template void orth_gramian_dev<T>(const StageCtx &, int, int, int, T *, long long);                           \
+  template IterResult integrate_kn_dev<T>(const StageCtx &, int, int, int, const T *, long long, T *, long long, \
+                                          int, double);                                                         \
+  template void integrate_hr_dev<T>(const StageCtx &, int, int, int, T *, long long, T *, long long);           \
+  template void post_gramian_dev<T>(const StageCtx &, int, int, int, int, char, const T *, long long, const T *, \
+                                    long long, T *, T *, long long, T *, long long, bool, bool);               \
+  template void post_symmetric_dev<T>(const StageCtx &, int, int, int, int, char, const T *, long long,         \
+                                      const T *, long long, T *, T *, long long, bool);
+ISVD_INST(float)
+ISVD_INST(double)
+#undef ISVD_INST
+
+}  // namespace isvdb

@@ -1,0 +1,65 @@
+// Device-level iSVD stages at one MPI rank.  All pointers are device pointers; matrices keep
+// the reference layouts (yst m x Nl row-major, qt m x l row-major, ut/vt row-major, A per ordera).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace isvdb {
+
+struct StageCtx {
+  cudaStream_t st;
+  int precision;   // kNative / kMixed
+  int *status;     // device status word (zeroed by the caller)
+};
+
+struct IterResult {
+  int iterations = 0;
+  double error = 0.0;
+};
+
+struct WyArgs {
+  int maxit = 256;
+  double tol = 1e-3, tau0 = 1.0, taumax = 1e14, taumin = 1e-14;
+  int taumaxit = 20;
+  double beta = 0.5, sigma = 1e-4, eta = 0.85;
+};
+
+// Y = A * Omega (reference core/stage/@x@_sketch.h:92-146).  omega == nullptr: drawn from seed.
+template <class T>
+void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
+                long long ldom, uint64_t seed, T *y, long long ldy);
+
+// In-place Gramian orthogonalization of the N blocks of yst (reference @x@_orthogonalize_gramian.c).
+template <class T>
+void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy);
+
+// In-place TSQR orthogonalization (reference @x@_orthogonalize_tall_skinny_qr.c), Householder QR per block.
+template <class T>
+void orth_tsqr_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy);
+
+template <class T>
+IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs, long long ldq, T *qt,
+                            long long ldqt, int maxit, double tol);
+
+template <class T>
+IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs, long long ldq, T *qt,
+                            long long ldqt, const WyArgs &w);
+
+template <class T>
+void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt);
+
+// Postprocessing.  s has l entries; ut (m x k, ldut), vt (n x k or n x l for TS, ldvt) when wanted.
+template <class T>
+void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
+                      const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
+                      bool wv);
+template <class T>
+void post_tsqr_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
+                   const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu, bool wv);
+template <class T>
+void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
+                        const T *qt, long long ldqt, T *s, T *ut, long long ldut, bool wu);
+
+}  // namespace isvdb
