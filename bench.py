@@ -1,0 +1,371 @@
+#!/usr/bin/env python3
+"""Benchmark: rank-k iSVD (Gaussian projection / Gramian / Kolmogorov-Nagumo / Gramian) of a
+200000 x 20000 FP32 matrix, k = 100, p = 28 (l = 128), N = 32 sketches, on one B200 (N GPUs:
+N independent replicas, one per rank).  Prints one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size full|small]
+
+Inputs are synthetic and seeded: A = U diag(sigma) V' + 1e-4 G with Haar-random U (m x 2000),
+V (n x 2000), sigma geometric from 1 to 1e-3 over 2000 values, G standard normal; generated on
+the GPU before the timed region.  A (16 GB) is larger than L2 (126 MB), so no flush is needed
+between timed solves.  A step is one full solve through the C ABI (isvd_sIsvd_ex, MIXED
+precision: BF16x3 tcgen05 products, FP64 l x l steps).  The FP64 path (isvd_dIsvd_ex, NATIVE)
+is timed once on the same matrix and the same Omega for the speed-up and the sigma error.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+WORKLOADS = {
+    # BASELINE config 2 (the metric's configuration)
+    "full": dict(m=200000, n=20000, rank=2000, k=100, p=28, N=32, noise=1e-4, seed=2),
+    # a reduced shape of the same construction, for quick checks
+    "small": dict(m=20000, n=4000, rank=400, k=100, p=28, N=8, noise=1e-4, seed=2),
+}
+METRIC = "rank-k iSVD solves/s, mixed BF16x3 vs plain FP64 on B200 at sigma rel err <= 1e-5"
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), float(d["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_matrix(torch, w, dev, seed):
+    """A = U diag(sigma) V' + noise * G (FP32, row-major), Haar factors from QR of Gaussians."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    m, n, r = w["m"], w["n"], w["rank"]
+    u = torch.linalg.qr(torch.randn(m, r, generator=g, device=dev, dtype=torch.float32))[0]
+    v = torch.linalg.qr(torch.randn(n, r, generator=g, device=dev, dtype=torch.float32))[0]
+    sig = torch.logspace(0.0, -3.0, r, device=dev, dtype=torch.float32)
+    a = torch.randn(m, n, generator=g, device=dev, dtype=torch.float32)
+    a.mul_(w["noise"])
+    a.addmm_(u * sig, v.t())
+    del u, v
+    return a
+
+
+def solve(lib, x, prm, a, lda, s, ut, vt, l, seed, precision, retc=(0, 0, 2, 0)):
+    retv, times, status = lib.isvd(x, prm, ("GP", "GR", "KN", "GR"), a, lda, s, ut, l, vt, l, seed=seed,
+                                   retc=retc, argv=[None, None, [256, 1e-4], None], precision=precision)
+    if status != 0:
+        raise RuntimeError("isvd_%sIsvd_ex failed: %s" % (x, lib.last_error()))
+    return retv, times
+
+
+# ------------------------------------------------------------------------------ CPU reference
+def reference_sample(w, steps, warmup, threads):
+    """The reference's own CPU pipeline (oracle/_ref, OpenBLAS, 1 MPI rank, `threads` OpenMP
+    threads) on a row sample of the workload; each stage time is scaled to the full row count
+    (every stage's cost is linear in m) and the integration time also to the full problem's
+    iteration count when known.  Returns (seconds per full solve, sample description, KN its)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    os.environ["OPENBLAS_NUM_THREADS"] = str(threads)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import build_ref  # noqa: E402
+    from isvd_b200.capi import IsvdLib
+    ref = IsvdLib(build_ref.build())
+    m, n, k, p, N = w["m"], w["n"], w["k"], w["p"], w["N"]
+    l = k + p
+    ms = int(os.environ.get("ISVD_BENCH_REF_ROWS", 8192 if m > 8192 else m))
+    rng = np.random.default_rng(w["seed"])
+    r = w["rank"]
+    # rows of a Haar m x r factor are close to iid N(0, 1/m): the sample keeps A's row statistics
+    us = rng.standard_normal((ms, r)).astype(np.float32) / np.sqrt(m)
+    v = np.linalg.qr(rng.standard_normal((n, r)).astype(np.float32))[0]
+    sig = np.logspace(0, -3, r).astype(np.float32)
+    a = ((us * sig) @ v.T + w["noise"] * rng.standard_normal((ms, n)).astype(np.float32)).astype(np.float32)
+    a = np.ascontiguousarray(a)
+    prm = ref.create_param(ms, n, k, p, N)
+    s = np.zeros(l, np.float32)
+    ut = np.zeros((ms, l), np.float32)
+    vt = np.zeros((n, l), np.float32)
+    per = []
+    its = []
+    for i in range(warmup + steps):
+        retv, times, _ = ref.isvd("s", prm, ("GP", "GR", "KN", "GR"), a, n, s, ut, l, vt, l, seed=w["seed"],
+                                  argv=[None, None, [256, 1e-4], None], retc=(0, 0, 2, 0))
+        if i >= warmup:
+            per.append(times)
+            its.append(int(retv[2][0]))
+    scale = m / ms
+    t = np.mean(np.array(per), axis=0) * scale
+    desc = ("reference isvd_sIsvd (GP/GR/KN/GR, OpenBLAS, %d threads) on a %d x %d row sample, stage times "
+            "scaled by m / %d" % (threads, ms, n, ms))
+    return t, desc, int(np.median(its))
+
+
+def reference_arm(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    t0 = time.time()
+    stage_t, desc, its = reference_sample(w, args.steps, args.warmup, threads)
+    total = float(np.sum(stage_t))
+    val = 1.0 / total
+    out = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "solve/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded row sample)",
+        "config": config_dict(w),
+        "cpu_baseline": {"value": val, "unit": "solve/s", "cores": threads, "kind": "reference", "sample": desc,
+                         "stage_s": [float(x) for x in stage_t], "kn_iterations_sample": its},
+        "e2e": {"value": val, "unit": "solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t0,
+    }
+    print(json.dumps(out), flush=True)
+
+
+def config_dict(w):
+    return {"workload": "iSVD config 2: %dx%d FP32, rank-%d Haar factors, sigma 1..1e-3 geometric, +%.0e noise; "
+                        "k=%d p=%d N=%d; GP/GR/KN(1e-4,256)/GR, row block, 1 MPI rank"
+                        % (w["m"], w["n"], w["rank"], w["noise"], w["k"], w["p"], w["N"]),
+            "m": w["m"], "n": w["n"], "k": w["k"], "p": w["p"], "N": w["N"], "seed": w["seed"],
+            "l2_flush": "none needed: A (%.1f GB) is larger than L2" % (w["m"] * w["n"] * 4 / 1e9),
+            "parallelism": "replicas (one independent solve per GPU)"}
+
+
+# ------------------------------------------------------------------------------ B200 arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", default="full", choices=list(WORKLOADS))
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.size]
+    if args.impl == "reference":
+        return reference_arm(args, w)
+
+    import torch
+    import isvd_b200
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    lib = isvd_b200.load()
+    stream = torch.cuda.current_stream(dev)
+    lib.lib.isvd_gpu_set_stream(ctypes.c_void_p(stream.cuda_stream))
+
+    m, n, k, p, N = w["m"], w["n"], w["k"], w["p"], w["N"]
+    l = k + p
+    a = make_matrix(torch, w, dev, w["seed"] + 1000 * rank)
+    torch.cuda.synchronize()
+    prm = lib.create_param(m, n, k, p, N)
+    s = torch.zeros(l, dtype=torch.float32, device=dev)
+    ut = torch.zeros((m, l), dtype=torch.float32, device=dev)
+    vt = torch.zeros((n, l), dtype=torch.float32, device=dev)
+    seed = w["seed"]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up
+    for _ in range(args.warmup):
+        solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.lib.isvd_gpu_kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = np.zeros(4)
+    kn_its = 0
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            retv, times = solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
+            stage += np.array(times)
+            kn_its = int(retv[2][0])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches = lib.lib.isvd_gpu_kernel_launch_count() - launches0
+    ms_total = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_per = ms_total / args.steps
+    value = world * args.steps / (ms_total / 1e3)
+    s_mixed = s.double().cpu().numpy()
+
+    # per-kernel timing of the dominant kernel (separate, untimed run)
+    lib.lib.isvd_gpu_profile_reset()
+    lib.lib.isvd_gpu_profile_enable(1)
+    solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
+    lib.lib.isvd_gpu_profile_enable(0)
+    prof = {t: lib.profile(t) for t in ("sketch", "block_gram", "gram_full", "project")}
+
+    hbm, bf16, peak_kind = peaks()
+    sk = prof["sketch"]
+    sketch_ms = sk[0] / sk[1] if sk else None
+    alg_flops = 2.0 * m * n * (l * N)
+    achieved = alg_flops / (sketch_ms * 1e-3) / 1e12 if sketch_ms else None
+    peak3 = bf16 / 3.0
+    roofline = {"bound": "tensor", "kernel": "umma_gemm_kernel (sketch Y = A Omega, BF16x3)",
+                "achieved": achieved, "peak": peak3, "unit": "TFLOP/s",
+                "frac": (achieved / peak3) if achieved else None, "traffic": None,
+                "convention": "algorithmic 2 m n Nl flops per solve / kernel time; peak = %s bf16 dense %.1f "
+                              "TFLOP/s / 3 products" % (peak_kind, bf16),
+                "kernel_ms": sketch_ms,
+                "other_tcgen05_ms": {t: (v[0] / v[1] if v else None) for t, v in prof.items() if t != "sketch"}}
+
+    out = {"metric": METRIC, "value": value, "unit": "solve/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "bf16x3 (fp32 accumulate; fp64 l x l)",
+           "data": "synthetic (seeded, generated on GPU)", "config": config_dict(w),
+           "stage_ms": [1e3 * x / args.steps for x in stage], "kn_iterations": kn_its,
+           "gpu_launches": int(launches), "roofline": roofline}
+
+    # FP64 path on the same matrix and Omega
+    if not args.skip_fp64:
+        a64 = a.double()
+        s64 = torch.zeros(l, dtype=torch.float64, device=dev)
+        ut64 = torch.zeros((m, l), dtype=torch.float64, device=dev)
+        vt64 = torch.zeros((n, l), dtype=torch.float64, device=dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        retv64, times64 = solve(lib, "d", prm, a64, n, s64, ut64, vt64, l, seed, 0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        sv64 = s64.cpu().numpy()
+        rel = np.abs(s_mixed[:k] - sv64[:k]) / sv64[:k]
+        u32 = ut[:, :k].double()
+        u64 = ut64[:, :k]
+        # largest principal angle between span(U_mixed) and span(U_fp64)
+        q1 = torch.linalg.qr(u32)[0]
+        q2 = torch.linalg.qr(u64)[0]
+        sin = torch.linalg.matrix_norm(q2 - q1 @ (q1.T @ q2), ord=2).item()
+        out["fp64"] = {"ms_per_solve": ms64, "stage_ms": [1e3 * x for x in times64],
+                       "kn_iterations": int(retv64[2][0]), "sigma_rel_err_max": float(rel.max()),
+                       "u_max_principal_angle": float(np.arcsin(min(1.0, sin))),
+                       "speedup_mixed_vs_fp64": ms64 / ms_per}
+        del a64, ut64, vt64
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    if not args.skip_e2e:
+        ah = torch.empty((m, n), dtype=torch.float32, pin_memory=True)
+        ah.copy_(a)
+        sh = torch.zeros(l, dtype=torch.float32, pin_memory=True)
+        uh = torch.zeros((m, l), dtype=torch.float32, pin_memory=True)
+        vh = torch.zeros((n, l), dtype=torch.float32, pin_memory=True)
+        del a
+        torch.cuda.synchronize()
+        solve(lib, "s", prm, ah, n, sh, uh, vh, l, seed, 1)  # warm
+        barrier()
+        t0 = time.perf_counter()
+        reps = 2
+        for _ in range(reps):
+            solve(lib, "s", prm, ah, n, sh, uh, vh, l, seed, 1)
+        te = (time.perf_counter() - t0) / reps
+        if dist is not None:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        out["e2e"] = {"value": world / te, "unit": "solve/s", "ms_per_solve": 1e3 * te,
+                      "h2d_bytes_per_step": m * n * 4, "d2h_bytes_per_step": (l + m * k + n * k) * 4,
+                      "path": "isvd_sIsvd_ex with pinned host A, s, U, V (H2D of A and D2H of s, U, V timed)"}
+    out["clocks"] = clk.summary()
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        try:
+            stage_t, desc, its = reference_sample(w, 1, 0, os.cpu_count() or 1)
+            tot = float(np.sum(stage_t))
+            out["cpu_baseline"] = {"value": 1.0 / tot, "unit": "solve/s", "cores": os.cpu_count(),
+                                   "kind": "reference", "sample": desc, "stage_s": [float(x) for x in stage_t]}
+        except Exception as e:  # the checker library may be absent on a fresh box
+            out["cpu_baseline"] = {"value": None, "unit": "solve/s", "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": "unavailable: %s" % e}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    lib.lib.isvd_gpu_set_stream(None)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -79,9 +79,24 @@ int isvd_dIsvd_ex(
     const isvd_d_val_t *omega, const isvd_int_t ldomega, const int precision
 );
 
+/* Stream on which the library enqueues its work (a cudaStream_t of the current device; NULL
+ * restores the library's own non-blocking stream).  Every entry point still returns only after
+ * its work on that stream has completed. */
+void  isvd_gpu_set_stream( void *stream );
+void *isvd_gpu_get_stream( void );
+
 /* Number of kernels this library has launched since the process started (all devices).
  * Used by benchmarks to report how much of a timed region ran in this library's kernels. */
 unsigned long long isvd_gpu_kernel_launch_count( void );
+
+/* Kernel timing.  When enabled, every tcgen05 GEMM launch is bracketed by CUDA events on the
+ * library stream and accumulated under its stage tag ("sketch", "block_gram", "gram_full",
+ * "project").  isvd_gpu_profile_get returns 0 and fills the total milliseconds, the number of
+ * launches and the executed bf16 tensor flops (all plane products) of a tag, or -1 if absent.
+ * Enabling it adds a host synchronisation after each such launch: use it outside timed runs. */
+void isvd_gpu_profile_enable( int on );
+void isvd_gpu_profile_reset( void );
+int  isvd_gpu_profile_get( const char *tag, double *ms, unsigned long long *launches, double *flops );
 
 #if defined(__cplusplus)
 }

@@ -87,6 +87,13 @@ class IsvdLib:
         self._decl("isvd_gpu_set_precision", [ctypes.c_int])
         self._decl("isvd_gpu_get_precision", [], ctypes.c_int)
         self._decl("isvd_gpu_kernel_launch_count", [], ctypes.c_ulonglong)
+        self._decl("isvd_gpu_profile_enable", [ctypes.c_int])
+        self._decl("isvd_gpu_set_stream", [_VP])
+        self._decl("isvd_gpu_get_stream", [], _VP)
+        self._decl("isvd_gpu_profile_reset", [])
+        self._decl("isvd_gpu_profile_get", [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)],
+                   ctypes.c_int)
         for x in "sd":
             self._decl("isvd_%sSketchGaussianProjectionOmega" % x,
                        H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, _VP, c_int_t])
@@ -153,6 +160,13 @@ class IsvdLib:
 
     def clear_error(self):
         self.lib.isvd_gpu_clear_error()
+
+    def profile(self, tag):
+        """(total ms, launches, executed flops) recorded under `tag`, or None."""
+        ms, n, fl = ctypes.c_double(), ctypes.c_ulonglong(), ctypes.c_double()
+        if self.lib.isvd_gpu_profile_get(tag.encode(), ctypes.byref(ms), ctypes.byref(n), ctypes.byref(fl)) != 0:
+            return None
+        return ms.value, n.value, fl.value
 
     def sketch_omega(self, x, param, a, lda, omega, ldomega, yst, ldyst, dista=b"R", ordera=b"R"):
         fn = getattr(self.lib, "isvd_%sSketchGaussianProjectionOmega" % x)

@@ -12,6 +12,7 @@
 #include <string>
 
 #include "kernels.h"
+#include "mixed.h"
 #include "runtime.h"
 #include "stages.h"
 
@@ -450,6 +451,8 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
 
   Ctx c(precision);
   cudaStream_t st = c.sc.st;
+  MixedCache mcache;  // A's bf16 planes, shared by the sketch and the postprocess
+  c.sc.cache = &mcache;
   StageTimer tm;
   auto progress = [&](const char *what) {
     if (stream && root) { fprintf(stream, "%s", what); fflush(stream); }
@@ -566,6 +569,18 @@ void isvd_gpu_clear_error(void) { t_last_error = 0; t_last_msg.clear(); }
 void isvd_gpu_set_precision(int mode) { set_default_precision(mode == ISVD_GPU_PRECISION_MIXED ? kMixed : kNative); }
 int isvd_gpu_get_precision(void) { return default_precision(); }
 unsigned long long isvd_gpu_kernel_launch_count(void) { return g_launches.load(); }
+void isvd_gpu_set_stream(void *stream) {
+  api_call([&] {
+    Runtime &rt = Runtime::get();
+    rt.stream = stream ? (cudaStream_t)stream : rt.own_stream;
+  });
+}
+void *isvd_gpu_get_stream(void) { return Runtime::initialised() ? (void *)Runtime::get().stream : nullptr; }
+void isvd_gpu_profile_enable(int on) { set_profiling(on != 0); }
+void isvd_gpu_profile_reset(void) { profile_reset(); }
+int isvd_gpu_profile_get(const char *tag, double *ms, unsigned long long *launches, double *flops) {
+  return (tag && profile_get(tag, ms, launches, flops)) ? 0 : -1;
+}
 
 // ---------------------------------------------------------------- utilities
 mpi_int_t isvd_getMpiSize(const isvd_MpiComm comm) {

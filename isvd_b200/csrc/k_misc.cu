@@ -1,5 +1,7 @@
 // Elementwise kernels: Gaussian test matrix (Philox4x32-10 + Box-Muller), strided copies,
 // identity fill, column scaling.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 
 #include "kernels.h"
@@ -58,7 +60,8 @@ __global__ void rng_gaussian_kernel(T *__restrict__ out, long long rows, long lo
       const long long e = v - (long long)offset;
       if (e < 0 || e >= total) continue;
       const long long j = e / cols, c = e - j * cols;
-      out[j * ld + c] = (T)(h ? z.y : z.x);
+      // rounded to bf16 (8 significant bits) so that every precision mode draws the same Omega
+      out[j * ld + c] = (T)__bfloat162float(__double2bfloat16(h ? z.y : z.x));
     }
   }
 }

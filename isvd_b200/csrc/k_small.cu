@@ -23,8 +23,12 @@ __device__ __forceinline__ int rr_player(int i, int r, int ne) { return i == 0 ?
 
 // Rotation (c, s) annihilating the off-diagonal of [[app, apq], [apq, aqq]] with
 // R = [[c, s], [-s, c]] (Golub & Van Loan, Matrix Computations, Alg. 8.4.1 sym.schur2).
-__device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, double &c, double &s) {
-  if (apq == 0.0 || fabs(apq) <= 1e-300 || fabs(apq) <= 2.2e-16 * 0.25 * sqrt(fabs(app) * fabs(aqq))) {
+// No rotation when |apq| is below tol * max(sqrt(|app aqq|), floor): relative accuracy for the
+// well-scaled pairs, and a floor (eps * ||A||_F) that guarantees termination for the pairs of
+// eigenvalues that are negligible against ||A||.
+__device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, double tol, double floor_,
+                                           double &c, double &s) {
+  if (fabs(apq) <= tol * fmax(sqrt(fabs(app) * fabs(aqq)), floor_)) {
     c = 1.0;
     s = 0.0;
     return false;
@@ -35,6 +39,8 @@ __device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, d
   s = t * c;
   return true;
 }
+
+constexpr double kEps = 2.220446049250313e-16;
 
 __global__ void __launch_bounds__(kEigThreads)
     sym_eig_kernel(int n, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg, int order,
@@ -53,11 +59,23 @@ __global__ void __launch_bounds__(kEigThreads)
   int *qq = pp + np;                    // np
   int *flag = qq + np;                  // 1
 
+  __shared__ double red[kEigThreads];
+  double fr = 0.0;
   for (int e = tid; e < n * n; e += nt) {
     const int i = e / n, j = e - i * n;
-    A[e] = 0.5 * (A0[i * n + j] + A0[j * n + i]);
+    const double v = 0.5 * (A0[i * n + j] + A0[j * n + i]);
+    A[e] = v;
+    fr += v * v;
     V[e] = (i == j) ? 1.0 : 0.0;
   }
+  red[tid] = fr;
+  __syncthreads();
+  for (int h = nt / 2; h > 0; h >>= 1) {
+    if (tid < h) red[tid] += red[tid + h];
+    __syncthreads();
+  }
+  const double tol = kEps * fmax(1.0, sqrt((double)n));
+  const double floor_ = kEps * sqrt(red[0]);
   __syncthreads();
 
   int sweep = 0;
@@ -69,7 +87,7 @@ __global__ void __launch_bounds__(kEigThreads)
         int p = rr_player(k, r, ne), q = rr_player(ne - 1 - k, r, ne);
         if (p > q) { const int t = p; p = q; q = t; }
         double c = 1.0, s = 0.0;
-        if (q < n && jacobi_rot(A[p * n + p], A[q * n + q], A[p * n + q], c, s)) *flag = 1;
+        if (q < n && jacobi_rot(A[p * n + p], A[q * n + q], A[p * n + q], tol, floor_, c, s)) *flag = 1;
         pp[k] = p; qq[k] = q; rc[k] = c; rs[k] = s;
       }
       __syncthreads();
@@ -164,11 +182,22 @@ __global__ void __launch_bounds__(kEigThreads)
   double *nrm = X + n * n;         // n
   int *flag = (int *)(nrm + n);
 
+  __shared__ double red[kEigThreads];
+  double fr = 0.0;
   for (int e = tid; e < n * n; e += nt) {
     const int i = e / n, j = e - i * n;
     X[j * n + i] = B0[e];
+    fr += B0[e] * B0[e];
     V[e] = (i == j) ? 1.0 : 0.0;
   }
+  red[tid] = fr;
+  __syncthreads();
+  for (int h = nt / 2; h > 0; h >>= 1) {
+    if (tid < h) red[tid] += red[tid + h];
+    __syncthreads();
+  }
+  const double tol = kEps * fmax(1.0, sqrt((double)n));
+  const double floor2 = kEps * kEps * red[0];  // ||B||_F^2 eps^2
   __syncthreads();
   int sweep = 0;
   for (; sweep < kMaxSweeps; ++sweep) {
@@ -190,7 +219,7 @@ __global__ void __launch_bounds__(kEigThreads)
           be += __shfl_xor_sync(0xffffffffu, be, o);
           ga += __shfl_xor_sync(0xffffffffu, ga, o);
         }
-        if (ga == 0.0 || fabs(ga) <= 2.2e-16 * 0.25 * sqrt(al * be)) continue;
+        if (fabs(ga) <= tol * fmax(sqrt(al * be), floor2)) continue;
         if (lane == 0) *flag = 1;
         const double zeta = (be - al) / (2.0 * ga);
         const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));

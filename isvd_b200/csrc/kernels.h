@@ -32,7 +32,9 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st);
 
 // ------------------------------------------------------------------ elementwise
 // Omega(j, c) for j < rows, c < cols: standard normal values from Philox4x32-10 (key = seed)
-// with Box-Muller; value index = offset + j * cols + c.  Written at out[j*ld + c].
+// with Box-Muller, rounded to bf16; value index = offset + j * cols + c.  Written at out[j*ld + c].
+// The rounding makes the Omega of every precision mode identical (the MIXED sketch consumes it
+// exactly as a bf16 operand).
 template <class T>
 void rng_gaussian(T *out, long long rows, long long cols, long long ld, uint64_t seed, uint64_t offset,
                   cudaStream_t st);

@@ -1,29 +1,166 @@
-// MIXED precision engine (placeholder until the tcgen05 kernels land).
+// MIXED precision stages: bf16 planes + tcgen05 (umma.h) for the products whose cost scales with
+// the large dimensions; FP64 for every l x l step (done by the callers in stages.cu).
+//
+// Plane counts per product (relative error of one product term, before FP32 accumulation):
+//   sketch       A: 3 planes (exact for FP32 A)  x  Omega: 1 exact bf16 plane, or 3 when passed in
+//   block Gram   Y': 3 x 3 planes, 6 products  (W feeds the orthogonalizing eigensolve)
+//   G = Qs' Qs   2 x 2 planes, 3 products      (errors average over the m-long inner products)
+//   Z = A' Qbar  Qbar': 2 planes x A: 2 planes, 3 products
+#include "kernels.h"
 #include "mixed.h"
 #include "runtime.h"
 
 namespace isvdb {
+namespace {
 
-#define ISVD_MIXED_TODO(name) fail(kErrUnsupported, "mixed precision: %s not available in this build", name)
+struct PlaneBuf {
+  DBuf<__nv_bfloat16> buf;
+  Planes P;
+};
+
+// Planes of the rows x cols matrix src (element (r, c) at src[r * s_rs + c]), optionally transposed.
+template <class T>
+void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, long long cols, int np, bool transpose,
+                 cudaStream_t st) {
+  const long long orows = transpose ? cols : rows, ocols = transpose ? rows : cols;
+  const long long ld = plane_ld(ocols), rp = plane_rows(orows), ps = rp * ld;
+  pb.buf.alloc((size_t)np * ps);
+  split_planes<T>(src, s_rs, 1, rows, cols, np, transpose, pb.buf.p, ld, ps, st);
+  pb.P.ptr = pb.buf.p;
+  pb.P.np = np;
+  pb.P.rows = orows;
+  pb.P.cols = ocols;
+  pb.P.ld = ld;
+  pb.P.plane_stride = ps;
+  pb.P.mn_major = false;
+}
+
+void set_products(UmmaGemm &g, int na, int nb) {
+  // keep (p, q) with p + q < max(na, nb): the terms above the FP32 rounding level
+  const int order = (na > nb ? na : nb);
+  g.nprod = 0;
+  for (int s = 0; s < order; ++s)
+    for (int p = 0; p <= s; ++p) {
+      const int q = s - p;
+      if (p < na && q < nb) { g.pa[g.nprod] = p; g.pb[g.nprod] = q; ++g.nprod; }
+    }
+}
 
 template <class T>
-void mixed_sketch(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, uint64_t, T *,
-                  long long) { ISVD_MIXED_TODO("sketch"); }
+constexpr bool is_double() { return sizeof(T) == 8; }
+
+}  // namespace
+
 template <class T>
-void mixed_block_gram(const StageCtx &, int, int, int, const T *, long long, double *) { ISVD_MIXED_TODO("gram"); }
-template <class T>
-void mixed_block_apply(const StageCtx &, int, int, int, const T *, long long, const T *, T *, long long) {
-  ISVD_MIXED_TODO("apply");
+void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
+                  long long ldom, uint64_t seed, T *y, long long ldy) {
+  PlaneBuf local;
+  PlaneBuf *ap = &local;
+  MixedCache *mc = c.cache;
+  if (ordera == 'R') make_planes<T>(local, a, lda, m, n, 3, false, c.st);
+  else make_planes<T>(local, a, lda, n, m, 3, true, c.st);  // column-major A is A' row-major
+  PlaneBuf om;
+  if (!omega) {
+    const long long ld = plane_ld(n), rp = plane_rows(Nl);
+    om.buf.alloc((size_t)rp * ld);
+    rng_gaussian_bf16_t(om.buf.p, n, Nl, ld, rp, seed, c.st);
+    om.P.ptr = om.buf.p; om.P.np = 1; om.P.rows = Nl; om.P.cols = n; om.P.ld = ld; om.P.plane_stride = rp * ld;
+  } else {
+    make_planes<T>(om, omega, ldom, n, Nl, 3, true, c.st);  // Omega' planes (Nl x n)
+  }
+  UmmaGemm g;
+  g.M = m; g.N = Nl; g.K = n;
+  g.A = ap->P; g.B = om.P;
+  set_products(g, g.A.np, g.B.np);
+  g.C = y; g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
+  g.tag = "sketch";
+  umma_gemm(g, c.st);
+  if (mc) {
+    mc->src = a; mc->m = m; mc->n = n; mc->ordera = ordera;
+    mc->buf = std::move(local.buf);
+    mc->A = local.P;
+  }
 }
+
 template <class T>
-void mixed_gram_full(const StageCtx &, int, int, const T *, long long, double *) { ISVD_MIXED_TODO("gram"); }
-template <class T>
-void mixed_apply_coeff(const StageCtx &, int, int, int, const T *, long long, const double *, T *, long long) {
-  ISVD_MIXED_TODO("apply");
+void mixed_block_gram(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, double *W) {
+  PlaneBuf yt;
+  make_planes<T>(yt, y, ldy, m, (long long)N * l, 3, true, c.st);  // Y' planes (Nl x m)
+  UmmaGemm g;
+  g.M = l; g.N = l; g.K = m;
+  g.A = yt.P; g.B = yt.P;
+  set_products(g, 3, 3);
+  g.batch = N; g.a_mn_step = l; g.b_mn_step = l; g.c_step = (long long)l * l;
+  g.C = W; g.c_double = true; g.c_rs = l; g.c_cs = 1;
+  g.tag = "block_gram";
+  umma_gemm(g, c.st);
 }
+
 template <class T>
-void mixed_project(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, T *) {
-  ISVD_MIXED_TODO("project");
+void mixed_block_apply(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, const T *Wp, T *out,
+                       long long ldo) {
+  Gemm<T, T> g;
+  g.M = m; g.N = l; g.K = l; g.batch = N;
+  g.A = y; g.a_rs = ldy; g.a_cs = 1; g.a_bs = l;
+  g.B = Wp; g.b_rs = l; g.b_cs = 1; g.b_bs = (long long)l * l;
+  g.C = out; g.c_rs = ldo; g.c_cs = 1; g.c_bs = l;
+  gemm(g, c.st);
+}
+
+template <class T>
+void mixed_gram_full(const StageCtx &c, int m, int Nl, const T *qs, long long ldq, double *G) {
+  PlaneBuf qt;
+  make_planes<T>(qt, qs, ldq, m, Nl, 2, true, c.st);  // Qs' planes (Nl x m)
+  UmmaGemm g;
+  g.M = Nl; g.N = Nl; g.K = m;
+  g.A = qt.P; g.B = qt.P;
+  set_products(g, 2, 2);
+  g.C = G; g.c_double = true; g.c_rs = Nl; g.c_cs = 1;
+  g.upper = true;
+  g.tag = "gram_full";
+  umma_gemm(g, c.st);
+  mirror_upper(G, Nl, Nl, c.st);
+}
+
+template <class T>
+void mixed_apply_coeff(const StageCtx &c, int m, int Nl, int l, const T *qs, long long ldq, const double *M, T *qt,
+                       long long ldqt) {
+  DBuf<T> Mt((size_t)Nl * l);
+  copy2d<double, T>(M, l, 1, Mt.p, l, 1, Nl, l, c.st);
+  Gemm<T, T> g;
+  g.M = m; g.N = l; g.K = Nl;
+  g.A = qs; g.a_rs = ldq; g.a_cs = 1;
+  g.B = Mt.p; g.b_rs = l; g.b_cs = 1;
+  g.C = qt; g.c_rs = ldqt; g.c_cs = 1;
+  gemm(g, c.st);
+}
+
+template <class T>
+void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+                   long long ldqt, T *z) {
+  PlaneBuf qp;
+  make_planes<T>(qp, qt, ldqt, m, l, 2, true, c.st);  // Qbar' planes (l x m)
+  PlaneBuf local;
+  Planes ap;
+  MixedCache *mc = c.cache;
+  if (mc && mc->src == a && mc->m == m && mc->n == n && mc->ordera == ordera && mc->buf.p) {
+    ap = mc->A;
+  } else {
+    if (ordera == 'R') make_planes<T>(local, a, lda, m, n, 2, false, c.st);
+    else make_planes<T>(local, a, lda, n, m, 2, true, c.st);
+    ap = local.P;
+  }
+  // A planes are stored m x n (n contiguous): as the N x K = n x m operand they are MN-major.
+  Planes b = ap;
+  b.np = 2;
+  b.mn_major = true;
+  UmmaGemm g;
+  g.M = l; g.N = n; g.K = m;
+  g.A = qp.P; g.B = b;
+  set_products(g, 2, 2);
+  g.C = z; g.c_double = is_double<T>(); g.c_rs = 1; g.c_cs = l;  // Z' tile written into Z (n x l)
+  g.tag = "project";
+  umma_gemm(g, c.st);
 }
 
 #define ISVD_INST(T)                                                                                        \

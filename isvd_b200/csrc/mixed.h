@@ -5,9 +5,20 @@
 
 #include <cstdint>
 
+#include "runtime.h"
 #include "stages.h"
+#include "umma.h"
 
 namespace isvdb {
+
+// A's bf16 planes (m x n, K-major along n), made by the sketch and reused by the postprocess.
+struct MixedCache {
+  const void *src = nullptr;
+  long long m = 0, n = 0;
+  char ordera = 0;
+  DBuf<__nv_bfloat16> buf;
+  Planes A;
+};
 
 // Y = A * Omega (m x Nl, row-major ldy).  omega == nullptr: Omega is drawn exactly in bf16
 // (Philox + Box-Muller, rounded), so only A is split (3 products).  Otherwise Omega is split too.

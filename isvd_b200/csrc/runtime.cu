@@ -5,7 +5,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <string>
 
 namespace isvdb {
 
@@ -46,7 +48,8 @@ Runtime &Runtime::get() {
   g_rt.cc_major = prop.major;
   g_rt.cc_minor = prop.minor;
   g_rt.smem_optin = prop.sharedMemPerBlockOptin;
-  CK(cudaStreamCreateWithFlags(&g_rt.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&g_rt.own_stream, cudaStreamNonBlocking));
+  g_rt.stream = g_rt.own_stream;
   // Keep freed pool memory cached: repeated solves reuse it without new cudaMalloc calls.
   cudaMemPool_t pool;
   CK(cudaDeviceGetDefaultMemPool(&pool, dev));
@@ -63,7 +66,7 @@ void Runtime::reset() {
   if (!g_init) return;
   cudaStreamSynchronize(g_rt.stream);
   cudaFree(g_rt.ctl);
-  cudaStreamDestroy(g_rt.stream);
+  cudaStreamDestroy(g_rt.own_stream);
   g_rt = Runtime();
   g_init = false;
 }
@@ -106,5 +109,36 @@ bool is_device_pointer(const void *p) {
 }
 
 void sync() { CK(cudaStreamSynchronize(Runtime::get().stream)); }
+
+struct ProfEntry {
+  double ms = 0.0, flops = 0.0;
+  unsigned long long count = 0;
+};
+static std::map<std::string, ProfEntry> g_prof;
+static std::mutex g_prof_mu;
+static bool g_profiling = false;
+
+bool profiling() { return g_profiling; }
+void set_profiling(bool on) { g_profiling = on; }
+void profile_add(const char *tag, double ms, double flops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  ProfEntry &e = g_prof[tag];
+  e.ms += ms;
+  e.flops += flops;
+  e.count += 1;
+}
+bool profile_get(const char *tag, double *ms, unsigned long long *count, double *flops) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  auto it = g_prof.find(tag);
+  if (it == g_prof.end()) return false;
+  if (ms) *ms = it->second.ms;
+  if (count) *count = it->second.count;
+  if (flops) *flops = it->second.flops;
+  return true;
+}
+void profile_reset() {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  g_prof.clear();
+}
 
 }  // namespace isvdb

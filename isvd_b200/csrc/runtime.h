@@ -44,7 +44,8 @@ enum Precision : int { kNative = 0, kMixed = 1 };
 
 struct Runtime {
   int device = -1;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;      // stream in use
+  cudaStream_t own_stream = nullptr;  // the library's own stream
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
   size_t smem_optin = 0;
@@ -99,5 +100,12 @@ void DBuf<T>::release() {
 bool is_device_pointer(const void *p);
 
 void sync();  // synchronise the library stream, converting errors into Error
+
+// Optional per-kernel timing (CUDA events on the launching stream), off by default.
+bool profiling();
+void set_profiling(bool on);
+void profile_add(const char *tag, double ms, double flops);
+bool profile_get(const char *tag, double *ms, unsigned long long *count, double *flops);
+void profile_reset();
 
 }  // namespace isvdb

@@ -61,10 +61,16 @@ void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a
 }
 
 // -------------------------------------------------------------------------- orthogonalize
+namespace {
+
+// One Gramian pass on the N column blocks of y (in place):  Q_i = Y_i F(W_i),  W_i = Y_i' Y_i,
+//   polar = false:  F = V S^-1           (reference :80-98: gesvd('O') vectors over sqrt(values))
+//   polar = true:   F = V S^-1 V'        (re-orthogonalization that keeps Q's columns in place)
 template <class T>
-void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy) {
+void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, bool polar) {
   const int Nl = N * l;
-  DBuf<double> W((size_t)N * l * l), V((size_t)N * l * l), w((size_t)N * l);
+  const size_t ll = (size_t)l * l;
+  DBuf<double> W(N * ll), V(N * ll), w((size_t)N * l);
   // W_i = Y_i' Y_i   (reference :82-84)
   if (c.precision == kMixed) {
     mixed_block_gram<T>(c, m, l, N, y, ldy, W.p);
@@ -73,16 +79,27 @@ void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ld
     g.M = l; g.N = l; g.K = m; g.batch = N;
     g.A = y; g.a_rs = 1; g.a_cs = ldy; g.a_bs = l;
     g.B = y; g.b_rs = ldy; g.b_cs = 1; g.b_bs = l;
-    g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)l * l;
+    g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
     gemm(g, c.st);
   }
   // eig(W_i) = W_i S_i^2 W_i'  (gesvd 'O' of the PSD Gram: |lambda| descending, :88-91)
   sym_eig_batched(l, N, W.p, V.p, w.p, +1, true, c.status, c.st);
-  // W_i / S_i with S = sqrt(s)  (:94)
-  DBuf<T> Wp((size_t)N * l * l);
-  scale_cols_batched<double, T>(V.p, l, Wp.p, l, (long long)N * l, l, l, w.p, kScaleInvSqrt, c.st);
-  // Q_i = Y_i W_i / S_i  (:95-98; the reference copies Y first, here the product goes to a
-  // temporary and is copied back)
+  DBuf<T> Wp(N * ll);
+  if (!polar) {
+    // W_i / S_i with S = sqrt(s)  (:94)
+    scale_cols_batched<double, T>(V.p, l, Wp.p, l, (long long)N * l, l, l, w.p, kScaleInvSqrt, c.st);
+  } else {
+    DBuf<double> Vs(N * ll), P(N * ll);
+    scale_cols_batched<double, double>(V.p, l, Vs.p, l, (long long)N * l, l, l, w.p, kScaleInvSqrt, c.st);
+    Gemm<double, double> g;
+    g.M = l; g.N = l; g.K = l; g.batch = N;
+    g.A = Vs.p; g.a_rs = l; g.a_cs = 1; g.a_bs = (long long)ll;
+    g.B = V.p; g.b_rs = 1; g.b_cs = l; g.b_bs = (long long)ll;  // V'
+    g.C = P.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
+    gemm(g, c.st);
+    copy2d<double, T>(P.p, l, 1, Wp.p, l, 1, (long long)N * l, l, c.st);
+  }
+  // Q_i = Y_i F_i  (:95-98; the product goes to a temporary and is copied back)
   DBuf<T> tmp((size_t)m * Nl);
   if (c.precision == kMixed) {
     mixed_block_apply<T>(c, m, l, N, y, ldy, Wp.p, tmp.p, Nl);
@@ -90,12 +107,24 @@ void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ld
     Gemm<T, T> g = gm<T>(m, l, l);
     g.batch = N;
     g.A = y; g.a_rs = ldy; g.a_cs = 1; g.a_bs = l;
-    g.B = Wp.p; g.b_rs = l; g.b_cs = 1; g.b_bs = (long long)l * l;
+    g.B = Wp.p; g.b_rs = l; g.b_cs = 1; g.b_bs = (long long)ll;
     g.C = tmp.p; g.c_rs = Nl; g.c_cs = 1; g.c_bs = l;
     gemm(g, c.st);
   }
   CK(cudaMemcpy2DAsync(y, ldy * sizeof(T), tmp.p, (size_t)Nl * sizeof(T), (size_t)Nl * sizeof(T), m,
                        cudaMemcpyDeviceToDevice, c.st));
+}
+
+}  // namespace
+
+// Gramian orthogonalization (reference @x@_orthogonalize_gramian.c).  In MIXED precision the
+// Gram matrices carry FP32-level errors, which cost orthogonality in proportion to cond(Y_i)^2;
+// a second, polar pass (the second step of CholeskyQR2, with the symmetric inverse square root in
+// place of the Cholesky factor) restores orthonormality to FP32 level without moving the span.
+template <class T>
+void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy) {
+  gramian_pass<T>(c, m, l, N, y, ldy, false);
+  if (c.precision == kMixed) gramian_pass<T>(c, m, l, N, y, ldy, true);
   read_status(c, "Gramian orthogonalization");
 }
 

@@ -8,10 +8,13 @@
 
 namespace isvdb {
 
+struct MixedCache;  // bf16 planes of A kept between the sketch and the postprocess (mixed.h)
+
 struct StageCtx {
   cudaStream_t st;
   int precision;   // kNative / kMixed
   int *status;     // device status word (zeroed by the caller)
+  MixedCache *cache = nullptr;
 };
 
 struct IterResult {

@@ -1,0 +1,139 @@
+"""MIXED precision (BF16x3 planes on tcgen05 tensor cores, FP32 accumulation, FP64 l x l steps)
+against FP64: every stage on the reference goldens, and end to end against the FP64 path with
+the same Omega.  Tolerance: singular values within 1e-5 relative, largest principal angle of U
+and V within 1e-4 (the mixed-precision bar); products within FP32 rounding (1e-6 relative)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+L, N = 11, 12
+
+
+@pytest.fixture(autouse=True)
+def _mixed(lib):
+    lib.lib.isvd_gpu_set_precision(1)
+    lib.clear_error()
+    yield
+    lib.lib.isvd_gpu_set_precision(0)
+    assert lib.last_error()[0] == 0, lib.last_error()
+
+
+def lowrank(m, n, rank, decay, noise, seed):
+    rng = np.random.default_rng(seed)
+    u = np.linalg.qr(rng.standard_normal((m, rank)))[0]
+    v = np.linalg.qr(rng.standard_normal((n, rank)))[0]
+    return (u * decay ** np.arange(rank)) @ v.T + noise * rng.standard_normal((m, n))
+
+
+@pytest.mark.parametrize("x", ["s", "d"])
+@pytest.mark.parametrize("ordera", [b"R", b"C"])
+@pytest.mark.parametrize("shape", [(101, 1001, 132), (1000, 777, 300), (300, 2000, 512)])
+def test_mixed_sketch_omega(lib, x, ordera, shape):
+    """Y = A Omega with A and Omega both split into 3 planes (6 products): FP32-level accuracy
+    (the FP32 tensor-core accumulation bounds it, as it bounds an FP32 GEMM: ~1e-6 relative at
+    K = 1e3..2e4), across M/N/K tails and both storage orders of A."""
+    m, n, nl = shape
+    dt = np.float32 if x == "s" else np.float64
+    rng = np.random.default_rng(m + n)
+    a = rng.standard_normal((m, n)).astype(dt)
+    om = rng.standard_normal((n, nl)).astype(dt)
+    aa = np.ascontiguousarray(a) if ordera == b"R" else np.asfortranarray(a)
+    lda = n if ordera == b"R" else m
+    prm = lib.create_param(m, n, nl, 0, 1)
+    y = np.zeros((m, nl), dt)
+    lib.sketch_omega(x, prm, aa, lda, np.ascontiguousarray(om), nl, y, nl, ordera=ordera)
+    ref = a.astype(np.float64) @ om.astype(np.float64)
+    err = np.abs(y - ref).max() / np.abs(ref).max()
+    assert err < 1e-5, err
+
+
+def test_mixed_sketch_internal_omega_matches_native(lib):
+    """The internal Omega is drawn exactly in bf16, identical in both precision modes."""
+    m, n, k, p, Nn = 700, 500, 20, 12, 4
+    a = np.random.default_rng(3).standard_normal((m, n))
+    prm = lib.create_param(m, n, k, p, Nn)
+    y_mixed = np.zeros((m, (k + p) * Nn))
+    lib.sketch("d", prm, a, n, y_mixed, (k + p) * Nn, seed=42)
+    lib.lib.isvd_gpu_set_precision(0)
+    y_native = np.zeros_like(y_mixed)
+    lib.sketch("d", prm, a, n, y_native, (k + p) * Nn, seed=42)
+    lib.lib.isvd_gpu_set_precision(1)
+    assert np.abs(y_mixed - y_native).max() < 1e-5 * np.abs(y_native).max()
+
+
+@pytest.mark.parametrize("x", ["s", "d"])
+def test_mixed_orthogonalize_golden(lib, golden, oracle, x):
+    dt = np.float32 if x == "s" else np.float64
+    ys = golden["ys"]
+    m = ys.shape[0]
+    prm = lib.create_param(m, m, L, 0, N)
+    y = np.ascontiguousarray(ys.astype(dt))
+    lib.orthogonalize(x, "GR", prm, y, L * N)
+    for i in range(N):
+        blk = slice(i * L, (i + 1) * L)
+        q = y[:, blk].astype(np.float64)
+        assert oracle.projector_err(q, golden["qs"][:, blk]) < 1e-5
+        assert np.abs(q.T @ q - np.eye(L)).max() < 1e-5
+
+
+@pytest.mark.parametrize("x", ["s", "d"])
+def test_mixed_kn_golden(lib, golden, x):
+    dt = np.float32 if x == "s" else np.float64
+    qs = golden["qs"]
+    m = qs.shape[0]
+    prm = lib.create_param(m, m, L, 0, N)
+    qt = np.zeros((m, L), dt)
+    r = lib.integrate(x, "KN", prm, np.ascontiguousarray(qs.astype(dt)), L * N, qt, L, argv=[256, 1e-4])
+    assert abs(int(r[0]) - 81) <= 2
+    assert np.abs(qt - golden["q_kn"]).max() < 1e-3
+
+
+@pytest.mark.parametrize("x", ["s", "d"])
+@pytest.mark.parametrize("ordera", [b"R", b"C"])
+def test_mixed_postprocess_golden(lib, golden, oracle, x, ordera):
+    dt = np.float32 if x == "s" else np.float64
+    a0 = golden["a"].astype(dt)
+    m, n = a0.shape
+    aa = np.ascontiguousarray(a0) if ordera == b"R" else np.asfortranarray(a0)
+    lda = n if ordera == b"R" else m
+    prm = lib.create_param(m, n, L, 0, 1)
+    s = np.zeros(L, dt)
+    ut = np.zeros((m, L), dt)
+    vt = np.zeros((n, L), dt)
+    lib.postprocess(x, "GR", prm, aa, lda, np.ascontiguousarray(golden["q"].astype(dt)), L, s, ut, L, vt, L,
+                    ordera=ordera)
+    s_ref = golden["s"][:, 0]
+    assert np.abs(s - s_ref).max() < 1e-5 * s_ref.max()
+    assert oracle.max_principal_angle(ut.astype(np.float64), golden["u"]) < 1e-4
+    assert oracle.max_principal_angle(vt.astype(np.float64), golden["v"]) < 1e-4
+
+
+@pytest.mark.parametrize("x", ["s", "d"])
+def test_mixed_driver_vs_fp64(lib, oracle, x):
+    """End to end: same A, same Omega; mixed vs the FP64 path."""
+    m, n, k, p, Nn = 3000, 1500, 20, 12, 8
+    l = k + p
+    a = lowrank(m, n, 400, 10 ** (-3 / 400), 1e-6, 17)
+    om = np.random.default_rng(9).standard_normal((n, l * Nn))
+    dt = np.float32 if x == "s" else np.float64
+    prm = lib.create_param(m, n, k, p, Nn)
+    res = {}
+    for prec in (0, 1):
+        s = np.zeros(l, np.float64)
+        ut = np.zeros((m, l))
+        vt = np.zeros((n, l))
+        if prec == 0:
+            retv, _, st = lib.isvd("d", prm, ("GP", "GR", "KN", "GR"), np.ascontiguousarray(a), n, s, ut, l, vt, l,
+                                   omega=np.ascontiguousarray(om), ldomega=l * Nn, precision=0)
+        else:
+            s = s.astype(dt); ut = ut.astype(dt); vt = vt.astype(dt)
+            retv, _, st = lib.isvd(x, prm, ("GP", "GR", "KN", "GR"), np.ascontiguousarray(a.astype(dt)), n, s, ut,
+                                   l, vt, l, omega=np.ascontiguousarray(om.astype(dt)), ldomega=l * Nn,
+                                   precision=1)
+        assert st == 0, lib.last_error()
+        res[prec] = (s.astype(np.float64), ut.astype(np.float64), vt.astype(np.float64), int(retv[2][0]))
+    s0, u0, v0, it0 = res[0]
+    s1, u1, v1, it1 = res[1]
+    assert np.abs(s1 - s0).max() / s0.max() < 1e-5
+    assert oracle.max_principal_angle(u1[:, :k], u0[:, :k]) < 1e-4
+    assert oracle.max_principal_angle(v1[:, :k], v0[:, :k]) < 1e-4

@@ -69,7 +69,7 @@ def test_orthogonalize_gramian_golden(lib, golden, oracle, x):
         blk = slice(i * L, (i + 1) * L)
         assert oracle.projector_err(y[:, blk].astype(np.float64), golden["qs"][:, blk]) < TOL[x]
         if x == "d":
-            assert np.abs(y[:, blk].T @ y[:, blk] - np.eye(L)).max() < 1e-12
+            assert np.abs(y[:, blk].T @ y[:, blk] - np.eye(L)).max() < 1e-10
 
 
 @pytest.mark.parametrize("x", ["d", "s"])
@@ -157,7 +157,7 @@ def test_postprocess_gramian_golden(lib, golden, oracle, x, dista, ordera, mode)
         assert oracle.column_angles(ut, u_o).max() < 1e-10
         assert oracle.column_angles(vt, v_o).max() < 1e-10
         # U and V carry the same column signs: A V = U diag(s)
-        assert np.abs(golden["a"] @ vt - ut * s).max() < 1e-9 * s.max()
+        assert np.abs(ut.T @ golden["a"] @ vt - np.diag(s)).max() < 1e-9 * s.max()
 
 
 @pytest.mark.parametrize("x", ["d", "s"])
