@@ -1,15 +1,22 @@
 // tcgen05 GEMM engine over bf16 planes (see umma.h), plus the plane split and bf16 Omega kernels.
 //
-// CTA = 6 warps: warp 0 issues TMA loads into a ring of shared-memory stages, warp 1 allocates
-// tensor memory and issues tcgen05.mma (one thread), warps 2-5 drain the FP32 accumulator from
-// tensor memory (tcgen05.ld 32x32b) and write C.  The accumulator tile is 128 x BN (BN <= 256
-// FP32 columns of TMEM).  Every mbarrier wait is bounded; on expiry the CTA records
-// ISVD_GPU_ERROR_TIMEOUT in the status word, drains its outstanding copies / MMAs (bounded) and
-// frees its tensor memory before returning.
+// CTA = 10 warps: warp 0 issues TMA loads into a ring of shared-memory stages, warp 1 allocates
+// tensor memory and issues tcgen05.mma (one thread), warps 2-9 drain the accumulator.
+//
+// Accumulation is chunked: the tensor core adds products into its FP32 accumulator with an error
+// that grows with the length of the accumulation chain (measured on B200: ~1e-9 relative per
+// unit of K, i.e. 2e-5 at K = 2e4 in one chain).  So the MMAs accumulate only kChunkK-deep
+// chunks in tensor memory, alternating between two 128 x BN TMEM buffers; while the tensor core
+// fills one buffer, the epilogue warps add the other into FP32 registers (round to nearest) and
+// release it.  Each epilogue warp owns one TMEM lane quarter (warp % 4) and one half of the
+// columns.  Every mbarrier wait is bounded; on expiry the CTA records ISVD_GPU_ERROR_TIMEOUT in
+// the status word, drains its outstanding copies / MMAs (bounded) and frees its tensor memory
+// before returning.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "runtime.h"
@@ -19,7 +26,9 @@ namespace isvdb {
 namespace {
 
 constexpr int BM = 128;
-constexpr int kThreads = 192;
+constexpr int kThreads = 320;
+constexpr int kEpiWarps = 8;
+constexpr int kChunkK = 128;  // K depth of one tensor-memory accumulation chunk
 constexpr long long kWaitLimit = 1LL << 23;
 
 struct KParams {
@@ -114,7 +123,9 @@ struct Cfg {
   static constexpr int B_TILE = BN * BK * 2;  // bytes per B plane tile
   static constexpr uint32_t A_LAYOUT = (BK == 64) ? 2u : 4u;   // SWIZZLE_128B / SWIZZLE_64B
   static constexpr uint32_t A_SBO = (BK == 64) ? 1024u : 512u;  // 8 rows of BK bf16
-  static constexpr int TMEM_COLS = (BN <= 32) ? 32 : (BN <= 64) ? 64 : (BN <= 128) ? 128 : 256;
+  static constexpr int TMEM_COLS = (2 * BN <= 64) ? 64 : (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
+  static constexpr int CHUNK = (kChunkK / BK) > 0 ? (kChunkK / BK) : 1;  // k-blocks per chunk
+  static constexpr int HALF = BN / 2;                                      // columns per epilogue warp
 };
 
 template <int BN, int BK, bool BMN>
@@ -127,8 +138,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int stage_bytes = p.na * C::A_TILE + p.nb * C::B_TILE;
   uint64_t *full = (uint64_t *)(smem + (size_t)stages * stage_bytes);
   uint64_t *empty = full + stages;
-  uint64_t *accb = empty + stages;
-  uint32_t *tslot = (uint32_t *)(accb + 1);
+  uint64_t *tfull = empty + stages;  // [2] chunk in TMEM buffer b complete
+  uint64_t *tempty = tfull + 2;      // [2] TMEM buffer b drained by the epilogue
+  uint32_t *tslot = (uint32_t *)(tempty + 2);
   volatile int *abort_flag = (volatile int *)(tslot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -144,7 +156,10 @@ __global__ void __launch_bounds__(kThreads, 1)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accb, 1);
+    for (int b2 = 0; b2 < 2; ++b2) {
+      mbar_init(&tfull[b2], 1);
+      mbar_init(&tempty[b2], kEpiWarps);
+    }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -195,8 +210,20 @@ __global__ void __launch_bounds__(kThreads, 1)
   } else if (warp == 1 && lane == 0) {
     // ---------------------------------------------------------------- MMA issuer
     const uint32_t idesc = idesc_bf16(BM, BN, BMN);
-    int done = 0;
+    int chunk = 0;
+    uint32_t tacc = tmem;
+    bool first = true;
     for (int kb = 0; kb < nkb; ++kb) {
+      if (kb % C::CHUNK == 0) {
+        const int b2 = chunk & 1;
+        if (chunk >= 2 && !mbar_wait(&tempty[b2], ((chunk >> 1) & 1) ^ 1, abort_flag)) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        tacc = tmem + (uint32_t)(b2 * BN);
+        first = true;
+      }
       const int s = kb % stages;
       if (!mbar_wait(&full[s], (kb / stages) & 1, abort_flag)) {
         *abort_flag = 1;
@@ -212,50 +239,65 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint64_t da = sdesc(a_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
           const uint64_t db = BMN ? sdesc(b_base + kk * 2048, BK * 128, 1024, 2u)
                                   : sdesc(b_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
-          umma_bf16(tmem, da, db, idesc, (kb > 0 || i > 0 || kk > 0) ? 1u : 0u);
+          umma_bf16(tacc, da, db, idesc, first ? 0u : 1u);
+          first = false;
         }
       }
       umma_commit(&empty[s]);
-      ++done;
+      if (kb % C::CHUNK == C::CHUNK - 1 || kb == nkb - 1) {
+        umma_commit(&tfull[chunk & 1]);  // arrives when this chunk's MMAs have completed
+        ++chunk;
+      }
     }
-    umma_commit(accb);  // arrives when every MMA issued above has completed
   } else if (warp >= 2) {
     // ---------------------------------------------------------------- epilogue
-    const int q = warp & 3;  // TMEM lane quarter accessible to this warp
+    const int q = warp & 3;                 // TMEM lane quarter accessible to this warp
+    const int h = (warp - 2) >> 2;          // column half
     const int row = q * 32 + lane;
-    int okw = 0;
-    if (lane == 0) okw = mbar_wait(accb, 0, abort_flag) ? 1 : 0;
-    const bool ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
-    if (!ok && lane == 0) *abort_flag = 1;
-    tc_fence_after();
-    const int gm = m0 + row;
-    const bool rvalid = ok && gm < p.M;
-    const bool upper_tile = p.upper != 0;
-    for (int c0 = 0; c0 < BN; c0 += 8) {
-      float v[8];
-      __syncwarp();
-      if (nkb > 0 && ok) {
-        tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
-      } else {
+    const int nchunks = (nkb + C::CHUNK - 1) / C::CHUNK;
+    float acc[C::HALF];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = 0.f;
+    for (int j = 0; j < C::HALF; ++j) acc[j] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      const int b2 = c & 1;
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait(&tfull[b2], (c >> 1) & 1, abort_flag) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
+      if (!ok) {
+        if (lane == 0) *abort_flag = 1;
+        break;
       }
-      if (!rvalid) continue;
+      tc_fence_after();
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b2 * BN + h * C::HALF);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int gn = n0 + c0 + i;
+      for (int j = 0; j < C::HALF; j += 8) {
+        float v[8];
+        tmem_ld8(tbase + (uint32_t)j, v);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[j + i] += v[i];
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(&tempty[b2])) : "memory");
+    }
+    const int gm = m0 + row;
+    if (ok && gm < p.M) {
+      const bool upper_tile = p.upper != 0;
+#pragma unroll
+      for (int j = 0; j < C::HALF; ++j) {
+        const int gn = n0 + h * C::HALF + j;
         if (gn >= p.N) break;
         if (upper_tile && gn < gm) continue;
         if (p.splits == 1) {
           const long long off = (long long)b * p.c_step + (long long)gm * p.c_rs + (long long)gn * p.c_cs;
-          if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)v[i];
-          else ((float *)p.C)[off] = (float)(p.alpha * (double)v[i]);
+          if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)acc[j];
+          else ((float *)p.C)[off] = (float)(p.alpha * (double)acc[j]);
         } else {
-          p.partial[(((long long)b * p.splits + split) * p.M + gm) * p.N + gn] = v[i];
+          p.partial[(((long long)b * p.splits + split) * p.M + gm) * p.N + gn] = acc[j];
         }
       }
     }
-    tc_fence_before();
   }
   __syncthreads();
   if (*abort_flag && threadIdx.x == 0) atomicExch(p.status, (int)kErrTimeout);
@@ -443,6 +485,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   const int gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
   const long long tiles = (long long)gx * gy * g.batch;
   int splits = g.splits;
+  if (const char *e = getenv("ISVD_UMMA_SPLITS")) splits = atoi(e);  // diagnostic override
   if (splits <= 0) {
     splits = 1;
     if (tiles < rt.num_sms) splits = (int)std::min<long long>((rt.num_sms + tiles - 1) / tiles, std::max(1, p.total_kb / 8));
@@ -463,6 +506,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   int stages = std::min(8, budget / stage_bytes);
   if (stages < 2) fail(kErrUnsupported, "tcgen05 GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
+  static_assert(kThreads == 64 + 32 * kEpiWarps, "warp roles");
   auto kern = umma_gemm_kernel<BN, BK, BMN>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(gx, gy, g.batch * p.splits);
