@@ -42,31 +42,46 @@ __device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, d
 
 constexpr double kEps = 2.220446049250313e-16;
 
+// Two-sided Jacobi on a symmetric n x n matrix held packed (upper triangle, row by row) in shared
+// memory, with the eigenvector matrix held transposed (row i = eigenvector i) in shared memory when
+// it fits (VS = true) or in the output buffer otherwise.  Each round rotates n/2 disjoint pairs:
+// the 2 x 2 blocks of A on pair rows x pair columns are updated independently (each packed entry
+// belongs to exactly one block), and the rotation acts on two rows of V' (contiguous, conflict-free).
+__device__ __forceinline__ int pk(int i, int j, int n) {
+  if (i > j) { const int t = i; i = j; j = t; }
+  return i * n - (i * (i - 1)) / 2 + (j - i);
+}
+
+template <bool VS>
 __global__ void __launch_bounds__(kEigThreads)
     sym_eig_kernel(int n, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg, int order,
-                   bool absval, int *status) {
+                   bool absval, double *__restrict__ scratch, int *status) {
   extern __shared__ double sm[];
   const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const double *A0 = Ag + (size_t)b * n * n;
   double *V = Vg + (size_t)b * n * n;
   double *w = wg + (size_t)b * n;
   const int ne = n + (n & 1), np = ne / 2;
-  double *A = sm;                       // n * n
-  double *rc = A + n * n;               // np
-  double *rs = rc + np;                 // np
-  double *key = rs + np;                // n
-  int *pp = (int *)(key + n);           // np
-  int *qq = pp + np;                    // np
-  int *flag = qq + np;                  // 1
+  const int npk = n * (n + 1) / 2;
+  double *A = sm;                                                           // packed upper triangle
+  double *Vt = VS ? (A + ((npk + 1) & ~1)) : (scratch + (size_t)b * n * n);  // V' (row i = eigenvector i)
+  double *rc = VS ? (Vt + (size_t)n * n) : (A + ((npk + 1) & ~1));
+  double *rs = rc + np;
+  double *key = rs + np;
+  int *pp = (int *)(key + n);
+  int *qq = pp + np;
+  int *flag = qq + np;
 
   __shared__ double red[kEigThreads];
   double fr = 0.0;
   for (int e = tid; e < n * n; e += nt) {
     const int i = e / n, j = e - i * n;
-    const double v = 0.5 * (A0[i * n + j] + A0[j * n + i]);
-    A[e] = v;
-    fr += v * v;
-    V[e] = (i == j) ? 1.0 : 0.0;
+    if (i <= j) {
+      const double v = 0.5 * (A0[i * n + j] + A0[j * n + i]);
+      A[pk(i, j, n)] = v;
+      fr += (i == j ? 1.0 : 2.0) * v * v;
+    }
+    Vt[e] = (i == j) ? 1.0 : 0.0;
   }
   red[tid] = fr;
   __syncthreads();
@@ -78,6 +93,7 @@ __global__ void __launch_bounds__(kEigThreads)
   const double floor_ = kEps * sqrt(red[0]);
   __syncthreads();
 
+  const int nblk = np * (np + 1) / 2;
   int sweep = 0;
   for (; sweep < kMaxSweeps; ++sweep) {
     if (tid == 0) *flag = 0;
@@ -86,54 +102,57 @@ __global__ void __launch_bounds__(kEigThreads)
       for (int k = tid; k < np; k += nt) {
         int p = rr_player(k, r, ne), q = rr_player(ne - 1 - k, r, ne);
         if (p > q) { const int t = p; p = q; q = t; }
-        double c = 1.0, s = 0.0;
-        if (q < n && jacobi_rot(A[p * n + p], A[q * n + q], A[p * n + q], tol, floor_, c, s)) *flag = 1;
-        pp[k] = p; qq[k] = q; rc[k] = c; rs[k] = s;
+        double c = 1.0, sn = 0.0;
+        if (q < n && jacobi_rot(A[pk(p, p, n)], A[pk(q, q, n)], A[pk(p, q, n)], tol, floor_, c, sn)) *flag = 1;
+        pp[k] = p; qq[k] = q; rc[k] = c; rs[k] = sn;
       }
       __syncthreads();
-      // A := R' A R on every 2 x 2 block of pair rows x pair columns (I <= J).
-      const int nblk = np * (np + 1) / 2;
+      // A := R' A R, one 2 x 2 block (pair J rows x pair I columns, J <= I) per work item
       for (int e = tid; e < nblk; e += nt) {
-        // decode e -> (I, J), I <= J
         int I = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
         while ((I + 1) * (I + 2) / 2 <= e) ++I;
         while (I * (I + 1) / 2 > e) --I;
-        int J = e - I * (I + 1) / 2;  // J <= I; swap roles so that we process (J, I)
-        const int pi = pp[J], qi = qq[J], pj = pp[I], qj = qq[I];
-        const double ci = rc[J], si = rs[J], cj = rc[I], sj = rs[I];
+        const int J = e - I * (I + 1) / 2;
+        const double si = rs[J], sj = rs[I];
         if (si == 0.0 && sj == 0.0) continue;
+        const int pi = pp[J], qi = qq[J], pj = pp[I], qj = qq[I];
+        const double ci = rc[J], cj = rc[I];
         const bool qiv = qi < n, qjv = qj < n;
-        const double x11 = A[pi * n + pj];
-        const double x12 = qjv ? A[pi * n + qj] : 0.0;
-        const double x21 = qiv ? A[qi * n + pj] : 0.0;
-        const double x22 = (qiv && qjv) ? A[qi * n + qj] : 0.0;
-        // left: rows (pi, qi)
+        if (I == J) {
+          if (!qiv) continue;
+          const double app = A[pk(pi, pi, n)], aqq = A[pk(qi, qi, n)], apq = A[pk(pi, qi, n)];
+          // rotated 2 x 2 diagonal block: off-diagonal annihilated
+          const double t = si / ci;
+          A[pk(pi, pi, n)] = app - t * apq;
+          A[pk(qi, qi, n)] = aqq + t * apq;
+          A[pk(pi, qi, n)] = 0.0;
+          continue;
+        }
+        const int i11 = pk(pi, pj, n);
+        const int i12 = qjv ? pk(pi, qj, n) : 0;
+        const int i21 = qiv ? pk(qi, pj, n) : 0;
+        const int i22 = (qiv && qjv) ? pk(qi, qj, n) : 0;
+        const double x11 = A[i11];
+        const double x12 = qjv ? A[i12] : 0.0;
+        const double x21 = qiv ? A[i21] : 0.0;
+        const double x22 = (qiv && qjv) ? A[i22] : 0.0;
         const double y11 = ci * x11 - si * x21, y12 = ci * x12 - si * x22;
         const double y21 = si * x11 + ci * x21, y22 = si * x12 + ci * x22;
-        // right: cols (pj, qj)
-        double z11 = y11 * cj - y12 * sj, z12 = y11 * sj + y12 * cj;
-        double z21 = y21 * cj - y22 * sj, z22 = y21 * sj + y22 * cj;
-        if (I == J) {
-          if (si != 0.0) { z12 = 0.0; z21 = 0.0; }
-          A[pi * n + pi] = z11;
-          if (qiv) { A[qi * n + qi] = z22; A[pi * n + qi] = z12; A[qi * n + pi] = z12; }
-        } else {
-          A[pi * n + pj] = z11; A[pj * n + pi] = z11;
-          if (qjv) { A[pi * n + qj] = z12; A[qj * n + pi] = z12; }
-          if (qiv) { A[qi * n + pj] = z21; A[pj * n + qi] = z21; }
-          if (qiv && qjv) { A[qi * n + qj] = z22; A[qj * n + qi] = z22; }
-        }
+        A[i11] = y11 * cj - y12 * sj;
+        if (qjv) A[i12] = y11 * sj + y12 * cj;
+        if (qiv) A[i21] = y21 * cj - y22 * sj;
+        if (qiv && qjv) A[i22] = y21 * sj + y22 * cj;
       }
-      // V := V R (columns p, q of every row)
-      for (int e = tid; e < n * np; e += nt) {
-        const int row = e / np, k = e - row * np;
-        const double s = rs[k];
-        if (s == 0.0) continue;
+      // V' := R' V' : rows p and q of V'
+      for (int e = tid; e < np * n; e += nt) {
+        const int k = e / n, col = e - k * n;
+        const double sn = rs[k];
+        if (sn == 0.0) continue;
         const double c = rc[k];
         const int p = pp[k], q = qq[k];
-        const double v1 = V[row * n + p], v2 = V[row * n + q];
-        V[row * n + p] = c * v1 - s * v2;
-        V[row * n + q] = s * v1 + c * v2;
+        const double v1 = Vt[p * n + col], v2 = Vt[q * n + col];
+        Vt[p * n + col] = c * v1 - sn * v2;
+        Vt[q * n + col] = sn * v1 + c * v2;
       }
       __syncthreads();
     }
@@ -143,26 +162,22 @@ __global__ void __launch_bounds__(kEigThreads)
   }
   if (sweep == kMaxSweeps && tid == 0) atomicExch(status, kErrNumerical);
 
-  // Sort eigenpairs: order > 0 by |lambda| descending, order < 0 by lambda ascending.
-  for (int i = tid; i < n; i += nt) key[i] = A[i * n + i];
+  // Sort eigenpairs: order > 0 by |lambda| descending, order < 0 by lambda ascending; write the
+  // eigenvectors as the columns of V (row-major).
+  for (int i = tid; i < n; i += nt) key[i] = A[pk(i, i, n)];
   __syncthreads();
-  // reuse A as the permuted eigenvector buffer
   for (int i = tid; i < n; i += nt) {
     const double ki = key[i];
     int rank = 0;
     for (int j = 0; j < n; ++j) {
       const double kj = key[j];
-      bool before;
-      if (order > 0) before = fabs(kj) > fabs(ki) || (fabs(kj) == fabs(ki) && j < i);
-      else before = kj < ki || (kj == ki && j < i);
+      const bool before = (order > 0) ? (fabs(kj) > fabs(ki) || (fabs(kj) == fabs(ki) && j < i))
+                                      : (kj < ki || (kj == ki && j < i));
       rank += before;
     }
     w[rank] = absval ? fabs(ki) : ki;
-    pp[0] = pp[0];  // no-op keeps pp live
-    for (int r = 0; r < n; ++r) A[r * n + rank] = V[r * n + i];
+    for (int r2 = 0; r2 < n; ++r2) V[r2 * n + rank] = Vt[i * n + r2];
   }
-  __syncthreads();
-  for (int e = tid; e < n * n; e += nt) V[e] = A[e];
 }
 
 // One-sided Jacobi SVD: B (row-major n x n) -> U diag(s) V'.
@@ -314,14 +329,27 @@ __device__ void mm_tiles(int l, int ntile_row, int tile_begin, int tile_end, dou
   for (int t = tile_begin + blockIdx.x; t < tile_end; t += gridDim.x) {
     const int tt = t - tile_begin;
     const int i0 = (tt / ntile_row) * 16, j0 = (tt % ntile_row) * 16;
-    __syncthreads();
-    for (int e = threadIdx.x; e < 16 * l; e += blockDim.x) {
+    // all loads of the tile are issued before any is used (one L2 round trip)
+    constexpr int kPer = (16 * 160 + kKnThreads - 1) / kKnThreads;
+    double ra[kPer], rb[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + u * kKnThreads;
       const int r = e / l, k = e - r * l;
-      As[r][k] = (i0 + r < l) ? __ldcg(A + (size_t)(i0 + r) * l + k) : 0.0;
+      ra[u] = (e < 16 * l && i0 + r < l) ? __ldcg(A + (size_t)(i0 + r) * l + k) : 0.0;
+      const int kb = e / 16, cb = e - kb * 16;
+      rb[u] = (e < 16 * l && j0 + cb < l) ? __ldcg(B + (size_t)kb * l + j0 + cb) : 0.0;
     }
-    for (int e = threadIdx.x; e < 16 * l; e += blockDim.x) {
-      const int k = e / 16, c = e - k * 16;
-      Bs[k][c] = (j0 + c < l) ? __ldcg(B + (size_t)k * l + j0 + c) : 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+      const int e = threadIdx.x + u * kKnThreads;
+      if (e < 16 * l) {
+        const int r = e / l, k = e - r * l;
+        As[r][k] = ra[u];
+        const int kb = e / 16, cb = e - kb * 16;
+        Bs[kb][cb] = rb[u];
+      }
     }
     __syncthreads();
     const int i = i0 + ty, j = j0 + tx;
@@ -475,9 +503,10 @@ __global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
   }
 }
 
-size_t eig_smem(int n) {
+size_t eig_smem(int n, bool vs) {
   const int ne = n + (n & 1), np = ne / 2;
-  return (size_t)n * n * 8 + (size_t)np * 16 + (size_t)n * 8 + (size_t)np * 8 + 16;
+  const size_t npk = ((size_t)n * (n + 1) / 2 + 1) & ~(size_t)1;
+  return npk * 8 + (vs ? (size_t)n * n * 8 : 0) + (size_t)np * 16 + (size_t)n * 8 + (size_t)np * 8 + 16;
 }
 size_t svd_smem(int n) { return (size_t)n * n * 8 + (size_t)n * 8 + 16; }
 
@@ -487,10 +516,18 @@ void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, in
                      cudaStream_t st) {
   if (n <= 0 || batch <= 0) return;
   Runtime &rt = Runtime::get();
-  const size_t smem = eig_smem(n);
+  const size_t smem_vs = eig_smem(n, true);
+  if (smem_vs <= rt.smem_optin) {
+    CK(cudaFuncSetAttribute(sym_eig_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_vs));
+    sym_eig_kernel<true><<<batch, kEigThreads, smem_vs, st>>>(n, A, V, w, order, absval, nullptr, status);
+    KLAUNCHED();
+    return;
+  }
+  const size_t smem = eig_smem(n, false);
   if (smem > rt.smem_optin) fail(kErrUnsupported, "symmetric eigensolver: l = %d exceeds on-chip capacity", n);
-  CK(cudaFuncSetAttribute(sym_eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  sym_eig_kernel<<<batch, kEigThreads, smem, st>>>(n, A, V, w, order, absval, status);
+  DBuf<double> scratch((size_t)batch * n * n);
+  CK(cudaFuncSetAttribute(sym_eig_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  sym_eig_kernel<false><<<batch, kEigThreads, smem, st>>>(n, A, V, w, order, absval, scratch.p, status);
   KLAUNCHED();
 }
 

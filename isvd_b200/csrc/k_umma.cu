@@ -348,41 +348,67 @@ __device__ __forceinline__ void split3(T x, __nv_bfloat16 *o, int np) {
   }
 }
 
-// Non-transposed: plane(r, c) for r < rows_pad, c < ld (zero outside rows x cols).
+__device__ __forceinline__ uint4 pack8(const __nv_bfloat16 *v) {
+  uint4 u;
+  u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
+  u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
+  u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
+  u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
+  return u;
+}
+
+// Non-transposed: plane(r, c) for r < rows_pad, c < ld (zero outside rows x cols); each thread
+// converts 8 consecutive columns and writes one 16-byte vector per plane.
 template <class T>
 __global__ void split_kernel(const T *__restrict__ src, long long s_rs, long long s_cs, long long rows,
                              long long cols, long long rows_pad, int np, __nv_bfloat16 *__restrict__ dst,
                              long long ld, long long ps) {
-  const long long total = rows_pad * ld;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long r = e / ld, c = e % ld;
-    __nv_bfloat16 o[3] = {__float2bfloat16(0.f), __float2bfloat16(0.f), __float2bfloat16(0.f)};
-    if (r < rows && c < cols) split3<T>(src[r * s_rs + c * s_cs], o, np);
-    for (int q = 0; q < np; ++q) dst[q * ps + e] = o[q];
+  const long long gpr = ld / 8;
+  const long long total = rows_pad * gpr;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const long long r = g / gpr, c0 = (g - r * gpr) * 8;
+    __nv_bfloat16 o[3][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const long long c = c0 + i;
+      const T x = (r < rows && c < cols) ? src[r * s_rs + c * s_cs] : T(0);
+      __nv_bfloat16 t[3];
+      split3<T>(x, t, 3);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) o[q][i] = t[q];
+    }
+    for (int q = 0; q < np; ++q) *(uint4 *)(dst + q * ps + r * ld + c0) = pack8(o[q]);
   }
 }
 
-// Transposed through a 32 x 33 shared tile: plane(c, r) = piece(src(r, c)); plane has rows_pad
-// (>= cols) rows of ld (>= rows) elements.
+// Transposed: plane(c, r) = piece(src(r, c)) through a 64 (r) x 32 (c) shared tile; each thread
+// writes 8 consecutive r of one output row c (16-byte vectors).  Plane rows beyond cols and
+// columns beyond rows are zeroed separately.
 template <class T>
 __global__ void split_t_kernel(const T *__restrict__ src, long long s_rs, long long s_cs, long long rows,
                                long long cols, long long rows_pad, int np, __nv_bfloat16 *__restrict__ dst,
                                long long ld, long long ps) {
-  __shared__ T tile[32][33];
-  const long long r0 = (long long)blockIdx.x * 32, c0 = (long long)blockIdx.y * 32;
+  __shared__ T tile[64][33];
+  const long long r0 = (long long)blockIdx.x * 64, c0 = (long long)blockIdx.y * 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
-  for (int j = ty; j < 32; j += 8) {
+  for (int j = ty; j < 64; j += 8) {
     const long long r = r0 + j, c = c0 + tx;
     tile[j][tx] = (r < rows && c < cols) ? src[r * s_rs + c * s_cs] : T(0);
   }
   __syncthreads();
-  for (int j = ty; j < 32; j += 8) {
-    const long long c = c0 + j, r = r0 + tx;  // output row c, column r
-    if (c >= rows_pad || r >= ld) continue;
-    __nv_bfloat16 o[3];
-    split3<T>(tile[tx][j], o, np);
-    for (int q = 0; q < np; ++q) dst[q * ps + c * ld + r] = o[q];
+  const int cl = threadIdx.x >> 3, seg = threadIdx.x & 7;  // output row c0 + cl, columns r0 + 8 seg ..
+  const long long c = c0 + cl, rr = r0 + 8 * seg;
+  if (c < rows_pad && rr < ld) {
+    __nv_bfloat16 o[3][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      __nv_bfloat16 t[3];
+      split3<T>(tile[8 * seg + i][cl], t, 3);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) o[q][i] = t[q];
+    }
+    for (int q = 0; q < np; ++q) *(uint4 *)(dst + q * ps + c * ld + rr) = pack8(o[q]);
   }
 }
 
@@ -545,7 +571,8 @@ void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, 
   const long long rows_pad = plane_stride / ld;
   if (rows_pad < out_rows || ld < (transpose ? rows : cols)) fail(kErrArgument, "split_planes: plane too small");
   if (!transpose) {
-    const long long total = rows_pad * ld;
+    if (ld % 8) fail(kErrArgument, "split_planes: ld must be a multiple of 8");
+    const long long total = rows_pad * (ld / 8);
     const int blocks = (int)std::min<long long>((total + 255) / 256, 32LL * rt.num_sms);
     split_kernel<T><<<blocks, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows_pad, np, dst, ld, plane_stride);
     KLAUNCHED();
@@ -559,7 +586,8 @@ void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, 
         CK(cudaMemset2DAsync(pl + rows, ld * sizeof(__nv_bfloat16), 0, (ld - rows) * sizeof(__nv_bfloat16), cols,
                              st));
     }
-    dim3 grid((unsigned)((rows + 31) / 32), (unsigned)((cols + 31) / 32));
+    if (ld % 8) fail(kErrArgument, "split_planes: ld must be a multiple of 8");
+    dim3 grid((unsigned)((rows + 63) / 64), (unsigned)((cols + 31) / 32));
     split_t_kernel<T><<<grid, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows_pad, np, dst, ld, plane_stride);
     KLAUNCHED();
   }

@@ -11,14 +11,6 @@
 #include "runtime.h"
 
 namespace isvdb {
-namespace {
-
-struct PlaneBuf {
-  DBuf<__nv_bfloat16> buf;
-  Planes P;
-};
-
-// Planes of the rows x cols matrix src (element (r, c) at src[r * s_rs + c]), optionally transposed.
 template <class T>
 void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, long long cols, int np, bool transpose,
                  cudaStream_t st) {
@@ -34,6 +26,11 @@ void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, lon
   pb.P.plane_stride = ps;
   pb.P.mn_major = false;
 }
+template void make_planes<float>(PlaneBuf &, const float *, long long, long long, long long, int, bool, cudaStream_t);
+template void make_planes<double>(PlaneBuf &, const double *, long long, long long, long long, int, bool,
+                                  cudaStream_t);
+
+namespace {
 
 void set_products(UmmaGemm &g, int na, int nb) {
   // keep (p, q) with p + q < max(na, nb): the terms above the FP32 rounding level
@@ -161,6 +158,23 @@ void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T 
   g.C = z; g.c_double = is_double<T>(); g.c_rs = 1; g.c_cs = l;  // Z' tile written into Z (n x l)
   g.tag = "project";
   umma_gemm(g, c.st);
+}
+
+void MixedGProduct::prepare(const StageCtx &c, int Nl_, const double *G) {
+  Nl = Nl_;
+  make_planes<double>(g, G, Nl, Nl, Nl, 3, false, c.st);  // G is symmetric: rows (M) x K
+}
+
+void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, double alpha, double *Bgc) {
+  make_planes<double>(b, Bc, l, Nl, l, 3, true, c.st);  // Bc' planes (l x Nl): N x K
+  UmmaGemm gg;
+  gg.M = Nl; gg.N = l; gg.K = Nl;
+  gg.A = g.P; gg.B = b.P;
+  set_products(gg, 3, 3);
+  gg.C = Bgc; gg.c_double = true; gg.c_rs = l; gg.c_cs = 1;
+  gg.alpha = alpha;
+  gg.tag = "kn_product";
+  umma_gemm(gg, c.st);
 }
 
 #define ISVD_INST(T)                                                                                        \

@@ -11,6 +11,26 @@
 
 namespace isvdb {
 
+// An owned set of bf16 planes.
+struct PlaneBuf {
+  DBuf<__nv_bfloat16> buf;
+  Planes P;
+};
+
+// Planes of the rows x cols matrix src (element (r, c) at src[r * s_rs + c]), optionally transposed.
+template <class T>
+void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, long long cols, int np, bool transpose,
+                 cudaStream_t st);
+
+// Kolmogorov-Nagumo products with a fixed Nl x Nl FP64 matrix G on the tensor cores:
+// Bgc = alpha * G * Bc (Bc: Nl x l FP64 row-major), G held as 3 bf16 planes, Bc split per call.
+struct MixedGProduct {
+  PlaneBuf g, b;
+  int Nl = 0;
+  void prepare(const StageCtx &c, int Nl_, const double *G);
+  void apply(const StageCtx &c, int l, const double *Bc, double alpha, double *Bgc);
+};
+
 // A's bf16 planes (m x n, K-major along n), made by the sketch and reused by the postprocess.
 struct MixedCache {
   const void *src = nullptr;

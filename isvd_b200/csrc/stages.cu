@@ -158,12 +158,16 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   set_identity<double>(Mc, Nl, l, l, c.st);                   // Qc = Q0 = Qs [I; 0]       (:154)
   Runtime &rt = Runtime::get();
   const double invN = 1.0 / N;
+  MixedGProduct gprod;  // MIXED: G's bf16 planes, reused by every iteration
+  if (c.precision == kMixed) gprod.prepare(c, Nl, G.p);
   IterResult res;
   double herr = 0.0;
   const int cap = maxit > 0 ? maxit : 1000000;
   int iter = 1;
   for (;; ++iter) {
-    {  // Bgc = G Bc / N   (:174-177)
+    if (c.precision == kMixed) {  // Bgc = G Bc / N   (:174-177)
+      gprod.apply(c, l, Bc, invN, Bgc.p);
+    } else {
       Gemm<double, double> g = gm<double>(Nl, l, Nl);
       g.alpha = invN;
       g.A = G.p; g.a_rs = Nl; g.a_cs = 1;
