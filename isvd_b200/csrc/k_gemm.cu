@@ -198,7 +198,10 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
   const bool b_nc = (g.b_cs == 1);
   if (!a_kc && g.a_rs != 1) fail(kErrArgument, "gemm: operand A has no unit stride");
   if (!b_nc && g.b_rs != 1) fail(kErrArgument, "gemm: operand B has no unit stride");
-  if (g.M <= 64 || g.N <= 64)
+  // 128 x 128 tiles when they fill the GPU; otherwise 64 x 64 tiles (4x more CTAs)
+  const long long tiles128 = (long long)((g.M + 127) / 128) * ((g.N + 127) / 128) * g.batch;
+  const int sms = Runtime::get().num_sms;
+  if (g.M <= 64 || g.N <= 64 || tiles128 < 2LL * sms)
     launch<T, Tout, 64, 64, 16>(g, a_kc, b_nc, st);
   else
     launch<T, Tout, 128, 128, 16>(g, a_kc, b_nc, st);

@@ -94,6 +94,18 @@ __global__ void __launch_bounds__(kEigThreads)
   __syncthreads();
 
   const int nblk = np * (np + 1) / 2;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  constexpr int kMaxMine = 8;  // np <= 80: nblk <= 3240 <= 8 * 512 (covers n <= 160)
+  short myI[kMaxMine], myJ[kMaxMine];
+  int nmy = 0;
+  for (int e = tid; e < nblk && nmy < kMaxMine; e += nt) {
+    int I = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while ((I + 1) * (I + 2) / 2 <= e) ++I;
+    while (I * (I + 1) / 2 > e) --I;
+    myI[nmy] = (short)I;
+    myJ[nmy] = (short)(e - I * (I + 1) / 2);
+    ++nmy;
+  }
   int sweep = 0;
   for (; sweep < kMaxSweeps; ++sweep) {
     if (tid == 0) *flag = 0;
@@ -107,12 +119,11 @@ __global__ void __launch_bounds__(kEigThreads)
         pp[k] = p; qq[k] = q; rc[k] = c; rs[k] = sn;
       }
       __syncthreads();
-      // A := R' A R, one 2 x 2 block (pair J rows x pair I columns, J <= I) per work item
-      for (int e = tid; e < nblk; e += nt) {
-        int I = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
-        while ((I + 1) * (I + 2) / 2 <= e) ++I;
-        while (I * (I + 1) / 2 > e) --I;
-        const int J = e - I * (I + 1) / 2;
+      // A := R' A R, one 2 x 2 block (pair J rows x pair I columns, J <= I) per work item; the
+      // block list of each thread is fixed (decoded once, below the sweep loop)
+#pragma unroll 1
+      for (int u = 0; u < nmy; ++u) {
+        const int I = myI[u], J = myJ[u];
         const double si = rs[J], sj = rs[I];
         if (si == 0.0 && sj == 0.0) continue;
         const int pi = pp[J], qi = qq[J], pj = pp[I], qj = qq[I];
@@ -120,12 +131,12 @@ __global__ void __launch_bounds__(kEigThreads)
         const bool qiv = qi < n, qjv = qj < n;
         if (I == J) {
           if (!qiv) continue;
-          const double app = A[pk(pi, pi, n)], aqq = A[pk(qi, qi, n)], apq = A[pk(pi, qi, n)];
-          // rotated 2 x 2 diagonal block: off-diagonal annihilated
-          const double t = si / ci;
-          A[pk(pi, pi, n)] = app - t * apq;
-          A[pk(qi, qi, n)] = aqq + t * apq;
-          A[pk(pi, qi, n)] = 0.0;
+          const int ipp = pk(pi, pi, n), iqq = pk(qi, qi, n), ipq = pk(pi, qi, n);
+          const double app = A[ipp], aqq = A[iqq], apq = A[ipq];
+          const double t = si / ci;  // rotated 2 x 2 diagonal block: off-diagonal annihilated
+          A[ipp] = app - t * apq;
+          A[iqq] = aqq + t * apq;
+          A[ipq] = 0.0;
           continue;
         }
         const int i11 = pk(pi, pj, n);
@@ -143,16 +154,18 @@ __global__ void __launch_bounds__(kEigThreads)
         if (qiv) A[i21] = y21 * cj - y22 * sj;
         if (qiv && qjv) A[i22] = y21 * sj + y22 * cj;
       }
-      // V' := R' V' : rows p and q of V'
-      for (int e = tid; e < np * n; e += nt) {
-        const int k = e / n, col = e - k * n;
+      // V' := R' V' : rows p and q of V'; warp w takes pairs w, w + nwarp, ..., each lane a
+      // strided set of columns
+      for (int k = warp; k < np; k += nwarp) {
         const double sn = rs[k];
         if (sn == 0.0) continue;
         const double c = rc[k];
-        const int p = pp[k], q = qq[k];
-        const double v1 = Vt[p * n + col], v2 = Vt[q * n + col];
-        Vt[p * n + col] = c * v1 - sn * v2;
-        Vt[q * n + col] = sn * v1 + c * v2;
+        double *vp = Vt + (size_t)pp[k] * n, *vq = Vt + (size_t)qq[k] * n;
+        for (int col = lane; col < n; col += 32) {
+          const double v1 = vp[col], v2 = vq[col];
+          vp[col] = c * v1 - sn * v2;
+          vq[col] = sn * v1 + c * v2;
+        }
       }
       __syncthreads();
     }
@@ -364,11 +377,11 @@ __device__ void mm_tiles(int l, int ntile_row, int tile_begin, int tile_end, dou
   }
 }
 
-// Number of coupled Newton-Schulz steps so that rho^(2^k) <= 1e-18 (rho: bound of ||I - X||_2).
-__device__ int ns_steps(double rho) {
+// Number of coupled Newton-Schulz steps so that rho^(2^k) <= target (rho: bound of ||I - X||_2).
+__device__ int ns_steps(double rho, double target) {
   if (!(rho < 0.999)) return 40;
   if (rho < 1e-300) return 1;
-  const double need = 41.45 / -log(rho);  // ln(1e18)
+  const double need = -log(target) / -log(rho);
   int k = 0;
   double p = 1.0;
   while (p < need && k < 40) { p *= 2.0; ++k; }
@@ -424,7 +437,7 @@ __global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
     if (threadIdx.x == 0) {
       const double rho = fmin(fro, red[0]);
       scal[0] = rho;
-      scal[1] = (double)ns_steps(rho);
+      scal[1] = (double)ns_steps(rho, a.ns_target);
     }
   }
   if (!grid_barrier(a.bar, a.status)) return;
@@ -469,7 +482,7 @@ __global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
           if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
           __syncthreads();
         }
-        if (threadIdx.x == 0) scal[1] = (double)ns_steps(fmin(sqrt(red[0]), 0.5));
+        if (threadIdx.x == 0) scal[1] = (double)ns_steps(fmin(sqrt(red[0]), 0.5), a.ns_target);
       }
       if (!grid_barrier(a.bar, a.status)) return;
     } else {

@@ -37,6 +37,7 @@ struct KParams {
   int pa[8], pb[8];
   int batch;
   long long a_mn_step, b_mn_step, c_step;
+  long long a_k_step, b_k_step;  // per-batch K offsets (elements)
   void *C;
   int c_double;
   long long c_rs, c_cs;
@@ -88,10 +89,10 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46) | ((uint64_t)layout << 61);
 }
 
-// Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B, K-major A, B major per flag.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool b_mn) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((b_mn ? 1u : 0u) << 16) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B, operand majors per flags.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, bool a_mn, bool b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
@@ -117,7 +118,7 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-template <int BN, int BK, bool BMN>
+template <int BN, int BK, bool AMN, bool BMN>
 struct Cfg {
   static constexpr int A_TILE = BM * BK * 2;  // bytes per A plane tile
   static constexpr int B_TILE = BN * BK * 2;  // bytes per B plane tile
@@ -128,11 +129,11 @@ struct Cfg {
   static constexpr int HALF = BN / 2;                                      // columns per epilogue warp
 };
 
-template <int BN, int BK, bool BMN>
+template <int BN, int BK, bool AMN, bool BMN>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                      const KParams p, const int stages) {
-  using C = Cfg<BN, BK, BMN>;
+  using C = Cfg<BN, BK, AMN, BMN>;
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const int stage_bytes = p.na * C::A_TILE + p.nb * C::B_TILE;
@@ -187,15 +188,24 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint8_t *st = smem + (size_t)s * stage_bytes;
       mbar_expect_tx(&full[s], (uint32_t)stage_bytes);
       const int k0 = (kb0 + kb) * BK;
-      for (int q = 0; q < p.na; ++q) tma_load_3d(st + q * C::A_TILE, &mapA, &full[s], k0, a_row, q);
+      const int ka = k0 + (int)(b * p.a_k_step), kbb = k0 + (int)(b * p.b_k_step);
+      for (int q = 0; q < p.na; ++q) {
+        if (!AMN) {
+          tma_load_3d(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q);
+        } else {
+#pragma unroll
+          for (int j = 0; j < BM / 64; ++j)
+            tma_load_3d(st + q * C::A_TILE + j * (BK * 128), &mapA, &full[s], a_row + 64 * j, ka, q);
+        }
+      }
       uint8_t *bt = st + p.na * C::A_TILE;
       for (int q = 0; q < p.nb; ++q) {
         if (!BMN) {
-          tma_load_3d(bt + q * C::B_TILE, &mapB, &full[s], k0, b_row, q);
+          tma_load_3d(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q);
         } else {
 #pragma unroll
           for (int j = 0; j < BN / 64; ++j)
-            tma_load_3d(bt + q * C::B_TILE + j * (BK * 128), &mapB, &full[s], b_row + 64 * j, k0, q);
+            tma_load_3d(bt + q * C::B_TILE + j * (BK * 128), &mapB, &full[s], b_row + 64 * j, kbb, q);
         }
       }
       ++issued;
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------------------------------------------------------- MMA issuer
-    const uint32_t idesc = idesc_bf16(BM, BN, BMN);
+    const uint32_t idesc = idesc_bf16(BM, BN, AMN, BMN);
     int chunk = 0;
     uint32_t tacc = tmem;
     bool first = true;
@@ -236,7 +246,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t b_base = st + p.na * C::A_TILE + p.pb[i] * C::B_TILE;
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
-          const uint64_t da = sdesc(a_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
+          const uint64_t da = AMN ? sdesc(a_base + kk * 2048, BK * 128, 1024, 2u)
+                                  : sdesc(a_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
           const uint64_t db = BMN ? sdesc(b_base + kk * 2048, BK * 128, 1024, 2u)
                                   : sdesc(b_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
           umma_bf16(tacc, da, db, idesc, first ? 0u : 1u);
@@ -491,9 +502,9 @@ CUtensorMap make_map(const Planes &P, int bx, int by, CUtensorMapSwizzle sw) {
   return m;
 }
 
-template <int BN, int BK, bool BMN>
+template <int BN, int BK, bool AMN, bool BMN>
 void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
-  using C = Cfg<BN, BK, BMN>;
+  using C = Cfg<BN, BK, AMN, BMN>;
   Runtime &rt = Runtime::get();
   KParams p;
   memset(&p, 0, sizeof(p));
@@ -502,6 +513,14 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   for (int i = 0; i < g.nprod; ++i) { p.pa[i] = g.pa[i]; p.pb[i] = g.pb[i]; }
   p.batch = g.batch;
   p.a_mn_step = g.a_mn_step; p.b_mn_step = g.b_mn_step; p.c_step = g.c_step;
+  p.a_k_step = g.a_k_step; p.b_k_step = g.b_k_step;
+  if ((g.a_k_step | g.b_k_step) % 8 || ((g.a_k_step || g.b_k_step) && g.K % BK))
+    fail(kErrArgument, "tcgen05 GEMM: per-batch K offsets need K %% %d == 0 and 8-element alignment", BK);
+  // TMA requires the innermost coordinate of every box to start on a 16-byte boundary: for an
+  // MN-major operand that coordinate is the MN offset (batch step + tile origin), for a K-major
+  // operand the K offset (checked above).  Tile origins are multiples of 64.
+  if ((AMN && g.a_mn_step % 8) || (BMN && g.b_mn_step % 8))
+    fail(kErrArgument, "tcgen05 GEMM: MN-major operand batch steps must be multiples of 8 elements");
   p.C = g.C; p.c_double = g.c_double;
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
@@ -525,7 +544,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
     p.partial = part.p;
   }
   const CUtensorMapSwizzle swa = (BK == 64) ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
-  CUtensorMap ma = make_map(g.A, BK, BM, swa);
+  CUtensorMap ma = AMN ? make_map(g.A, 64, BK, CU_TENSOR_MAP_SWIZZLE_128B) : make_map(g.A, BK, BM, swa);
   CUtensorMap mb = BMN ? make_map(g.B, 64, BK, CU_TENSOR_MAP_SWIZZLE_128B) : make_map(g.B, BK, BN, swa);
   const int stage_bytes = g.A.np * C::A_TILE + g.B.np * C::B_TILE;
   const int budget = (int)rt.smem_optin - 1024 - 256;
@@ -533,7 +552,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   if (stages < 2) fail(kErrUnsupported, "tcgen05 GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
   static_assert(kThreads == 64 + 32 * kEpiWarps, "warp roles");
-  auto kern = umma_gemm_kernel<BN, BK, BMN>;
+  auto kern = umma_gemm_kernel<BN, BK, AMN, BMN>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   dim3 grid(gx, gy, g.batch * p.splits);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -614,17 +633,21 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
                               rt.cc_minor);
   int *status = reinterpret_cast<int *>(rt.ctl + 32);
   CK(cudaMemsetAsync(status, 0, sizeof(int), st));
-  const bool bmn = g.B.mn_major;
+  const bool amn = g.A.mn_major, bmn = g.B.mn_major;
   const int stage64 = g.A.np * BM * 64 * 2 + g.B.np * 256 * 64 * 2;
   const bool small_n = g.N <= 128;
-  if (bmn) {
-    launch_t<128, 64, true>(g, st, status);
+  if (amn && bmn) {
+    launch_t<128, 64, true, true>(g, st, status);
+  } else if (amn) {
+    fail(kErrUnsupported, "tcgen05 GEMM: MN-major A needs MN-major B");
+  } else if (bmn) {
+    launch_t<128, 64, false, true>(g, st, status);
   } else if (small_n) {
-    launch_t<128, 64, false>(g, st, status);
+    launch_t<128, 64, false, false>(g, st, status);
   } else if (3 * stage64 <= (int)rt.smem_optin - 2048) {
-    launch_t<256, 64, false>(g, st, status);
+    launch_t<256, 64, false, false>(g, st, status);
   } else {
-    launch_t<256, 32, false>(g, st, status);
+    launch_t<256, 32, false, false>(g, st, status);
   }
   int h = 0;
   CK(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -79,6 +79,7 @@ struct KnStep {
   double *work;     // 8 * l * l doubles + 64
   int *status;      // set nonzero on failure (timeout / no convergence)
   unsigned int *bar;  // 2 words, zero
+  double ns_target = 1e-18;  // Newton-Schulz steps are chosen so that rho^(2^k) <= ns_target
 };
 void kn_step(const KnStep &a, cudaStream_t st);
 

@@ -80,11 +80,23 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
 }
 
 template <class T>
-void mixed_block_gram(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, double *W) {
-  PlaneBuf yt;
-  make_planes<T>(yt, y, ldy, m, (long long)N * l, 3, true, c.st);  // Y' planes (Nl x m)
+void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
+                      double *W) {
   UmmaGemm g;
   g.M = l; g.N = l; g.K = m;
+  if (l % 8 == 0) {
+    Planes a = yp;
+    a.mn_major = true;  // stored m x Nl: as the l x m operand Y_i' it is MN-major
+    g.A = a; g.B = a;
+    set_products(g, a.np, a.np);
+    g.batch = N; g.a_mn_step = l; g.b_mn_step = l; g.c_step = (long long)l * l;
+    g.C = W; g.c_double = true; g.c_rs = l; g.c_cs = 1;
+    g.tag = "block_gram";
+    umma_gemm(g, c.st);
+    return;
+  }
+  PlaneBuf yt;
+  make_planes<T>(yt, y, ldy, m, (long long)N * l, 3, true, c.st);  // Y' planes (Nl x m)
   g.A = yt.P; g.B = yt.P;
   set_products(g, 3, 3);
   g.batch = N; g.a_mn_step = l; g.b_mn_step = l; g.c_step = (long long)l * l;
@@ -94,8 +106,21 @@ void mixed_block_gram(const StageCtx &c, int m, int l, int N, const T *y, long l
 }
 
 template <class T>
-void mixed_block_apply(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, const T *Wp, T *out,
-                       long long ldo) {
+void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
+                       const T *Wp, T *out, long long ldo) {
+  if (l % 64 == 0) {
+    PlaneBuf wt;
+    make_planes<T>(wt, Wp, l, (long long)N * l, l, 3, true, c.st);  // [Wp_0' .. Wp_N-1'] (l x Nl)
+    UmmaGemm g;
+    g.M = m; g.N = l; g.K = l;
+    g.A = yp; g.B = wt.P;
+    set_products(g, yp.np, 3);
+    g.batch = N; g.a_k_step = l; g.b_k_step = l; g.c_step = l;
+    g.C = out; g.c_double = is_double<T>(); g.c_rs = ldo; g.c_cs = 1;
+    g.tag = "block_apply";
+    umma_gemm(g, c.st);
+    return;
+  }
   Gemm<T, T> g;
   g.M = m; g.N = l; g.K = l; g.batch = N;
   g.A = y; g.a_rs = ldy; g.a_cs = 1; g.a_bs = l;
@@ -105,12 +130,19 @@ void mixed_block_apply(const StageCtx &c, int m, int l, int N, const T *y, long 
 }
 
 template <class T>
-void mixed_gram_full(const StageCtx &c, int m, int Nl, const T *qs, long long ldq, double *G) {
-  PlaneBuf qt;
-  make_planes<T>(qt, qs, ldq, m, Nl, 2, true, c.st);  // Qs' planes (Nl x m)
+void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G) {
   UmmaGemm g;
   g.M = Nl; g.N = Nl; g.K = m;
-  g.A = qt.P; g.B = qt.P;
+  PlaneBuf qt;
+  if (Nl % 8 == 0) {
+    Planes a = qp;
+    a.np = 2;
+    a.mn_major = true;
+    g.A = a; g.B = a;
+  } else {
+    make_planes<T>(qt, qs, ldq, m, Nl, 2, true, c.st);  // Qs' planes (Nl x m)
+    g.A = qt.P; g.B = qt.P;
+  }
   set_products(g, 2, 2);
   g.C = G; g.c_double = true; g.c_rs = Nl; g.c_cs = 1;
   g.upper = true;
@@ -120,16 +152,18 @@ void mixed_gram_full(const StageCtx &c, int m, int Nl, const T *qs, long long ld
 }
 
 template <class T>
-void mixed_apply_coeff(const StageCtx &c, int m, int Nl, int l, const T *qs, long long ldq, const double *M, T *qt,
-                       long long ldqt) {
-  DBuf<T> Mt((size_t)Nl * l);
-  copy2d<double, T>(M, l, 1, Mt.p, l, 1, Nl, l, c.st);
-  Gemm<T, T> g;
+void mixed_apply_coeff(const StageCtx &c, const Planes &qp, int m, int Nl, int l, const T *qs, long long ldq,
+                       const double *M, T *qt, long long ldqt) {
+  (void)qs; (void)ldq;
+  PlaneBuf mt;
+  make_planes<double>(mt, M, l, Nl, l, 3, true, c.st);  // M' planes (l x Nl)
+  UmmaGemm g;
   g.M = m; g.N = l; g.K = Nl;
-  g.A = qs; g.a_rs = ldq; g.a_cs = 1;
-  g.B = Mt.p; g.b_rs = l; g.b_cs = 1;
-  g.C = qt; g.c_rs = ldqt; g.c_cs = 1;
-  gemm(g, c.st);
+  g.A = qp; g.B = mt.P;
+  set_products(g, qp.np, 3);
+  g.C = qt; g.c_double = is_double<T>(); g.c_rs = ldqt; g.c_cs = 1;
+  g.tag = "coeff_apply";
+  umma_gemm(g, c.st);
 }
 
 template <class T>
@@ -180,12 +214,14 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, double alp
 #define ISVD_INST(T)                                                                                        \
   template void mixed_sketch<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *,      \
                                 long long, uint64_t, T *, long long);                                      \
-  template void mixed_block_gram<T>(const StageCtx &, int, int, int, const T *, long long, double *);         \
-  template void mixed_block_apply<T>(const StageCtx &, int, int, int, const T *, long long, const T *, T *,  \
-                                     long long);                                                           \
-  template void mixed_gram_full<T>(const StageCtx &, int, int, const T *, long long, double *);              \
-  template void mixed_apply_coeff<T>(const StageCtx &, int, int, int, const T *, long long, const double *,  \
-                                     T *, long long);                                                      \
+  template void mixed_block_gram<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,    \
+                                    double *);                                                             \
+  template void mixed_block_apply<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
+                                     const T *, T *, long long);                                           \
+  template void mixed_gram_full<T>(const StageCtx &, const Planes &, int, int, const T *, long long,          \
+                                   double *);                                                              \
+  template void mixed_apply_coeff<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
+                                     const double *, T *, long long);                                      \
   template void mixed_project<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *,     \
                                  long long, T *);
 ISVD_INST(float)

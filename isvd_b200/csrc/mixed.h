@@ -46,23 +46,28 @@ template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                   long long ldom, uint64_t seed, T *y, long long ldy);
 
-// W_i = Y_i' Y_i for the N column blocks of Y (m x Nl, ld ldy) -> W (N x l x l, FP64).
+// The next four take bf16 planes `yp` of an m x Nl row-major matrix (split without transpose,
+// make_planes(.., false)) and the matrix itself (`y`, used when the block width rules out the
+// plane path: l % 8 != 0 for MN-major operands, l % 64 != 0 for per-block K offsets).
+
+// W_i = Y_i' Y_i for the N column blocks (W: N x l x l, FP64), as an MN-major x MN-major product.
 template <class T>
-void mixed_block_gram(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, double *W);
+void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
+                      double *W);
 
 // Q_i = Y_i Wp_i (Wp: N x l x l in T) -> out (m x Nl, ld ldo).
 template <class T>
-void mixed_block_apply(const StageCtx &c, int m, int l, int N, const T *y, long long ldy, const T *Wp, T *out,
-                       long long ldo);
+void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
+                       const T *Wp, T *out, long long ldo);
 
-// G = Qs' Qs (Nl x Nl, FP64 out).
+// G = Qs' Qs (Nl x Nl, FP64 out; symmetric, computed on the upper triangle and mirrored).
 template <class T>
-void mixed_gram_full(const StageCtx &c, int m, int Nl, const T *qs, long long ldq, double *G);
+void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G);
 
 // Qbar = Qs M (M: Nl x l FP64, row-major) -> qt (m x l, ld ldqt).
 template <class T>
-void mixed_apply_coeff(const StageCtx &c, int m, int Nl, int l, const T *qs, long long ldq, const double *M, T *qt,
-                       long long ldqt);
+void mixed_apply_coeff(const StageCtx &c, const Planes &qp, int m, int Nl, int l, const T *qs, long long ldq,
+                       const double *M, T *qt, long long ldqt);
 
 // Z = A' Qbar (n x l row-major).
 template <class T>

@@ -71,9 +71,11 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
   const int Nl = N * l;
   const size_t ll = (size_t)l * l;
   DBuf<double> W(N * ll), V(N * ll), w((size_t)N * l);
+  PlaneBuf yp;  // MIXED: bf16 planes of Y, shared by the Gram and the apply
+  if (c.precision == kMixed) make_planes<T>(yp, y, ldy, m, Nl, 3, false, c.st);
   // W_i = Y_i' Y_i   (reference :82-84)
   if (c.precision == kMixed) {
-    mixed_block_gram<T>(c, m, l, N, y, ldy, W.p);
+    mixed_block_gram<T>(c, yp.P, m, l, N, y, ldy, W.p);
   } else {
     Gemm<T, double> g;
     g.M = l; g.N = l; g.K = m; g.batch = N;
@@ -102,7 +104,7 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
   // Q_i = Y_i F_i  (:95-98; the product goes to a temporary and is copied back)
   DBuf<T> tmp((size_t)m * Nl);
   if (c.precision == kMixed) {
-    mixed_block_apply<T>(c, m, l, N, y, ldy, Wp.p, tmp.p, Nl);
+    mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, tmp.p, Nl);
   } else {
     Gemm<T, T> g = gm<T>(m, l, l);
     g.batch = N;
@@ -142,8 +144,10 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   const int Nl = N * l;
   const size_t nl = (size_t)Nl * l, ll = (size_t)l * l;
   DBuf<double> G((size_t)Nl * Nl);
+  PlaneBuf qp;  // MIXED: bf16 planes of Qs, shared by G and the final Qbar = Qs M
+  if (c.precision == kMixed) make_planes<T>(qp, qs, ldq, m, Nl, 3, false, c.st);
   if (c.precision == kMixed) {
-    mixed_gram_full<T>(c, m, Nl, qs, ldq, G.p);
+    mixed_gram_full<T>(c, qp.P, m, Nl, qs, ldq, G.p);
   } else {
     Gemm<T, double> g;
     g.M = Nl; g.N = Nl; g.K = m;
@@ -191,6 +195,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     KnStep s;
     s.l = l; s.Dc = Dc.p; s.Dgc = Dgc.p; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = err.p;
     s.work = work.p; s.status = c.status; s.bar = rt.ctl;
+    s.ns_target = (c.precision == kMixed) ? 1e-12 : 1e-18;  // MIXED carries FP32-level errors anyway
     kn_step(s, c.st);
     {  // M+ = Mc F + (Bc / N) C^-1 ;  B+ = Bc F + Bgc C^-1   (:221-226)
       Gemm<double, double> g = gm<double>(Nl, l, l);
@@ -216,7 +221,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   res.error = herr;
   // Qbar = Qs M+  (:251)
   if (c.precision == kMixed) {
-    mixed_apply_coeff<T>(c, m, Nl, l, qs, ldq, Mp, qt, ldqt);
+    mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mp, qt, ldqt);
   } else {
     DBuf<T> Mt(nl);
     copy2d<double, T>(Mp, l, 1, Mt.p, l, 1, Nl, l, c.st);

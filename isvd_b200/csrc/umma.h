@@ -33,6 +33,7 @@ struct UmmaGemm {
   // C at c + b * c_step.
   int batch = 1;
   long long a_mn_step = 0, b_mn_step = 0, c_step = 0;
+  long long a_k_step = 0, b_k_step = 0;  // per-batch K offsets (multiples of 8, with K % BK == 0)
   // output
   void *C = nullptr;          // C(i, j) at C[i * c_rs + j * c_cs] (+ b * c_step)
   bool c_double = false;
