@@ -464,12 +464,18 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   // ---- sketch (includes moving A to the device when it is on the host)
   progress("Sketching ..................... ");
   tm.mark(0, st);
+  // MIXED precision streams a host A through the device in panels inside the sketch and keeps
+  // only its bf16 planes (reused by the postprocess); NATIVE precision copies A once.
+  const bool mixed = c.sc.precision == kMixed;
   View<T> A, Om;
-  if (ordera_ == 'R') A.bind(a, n, m, lda, true, st);
-  else A.bind(a, m, n, lda, true, st);
+  if (!mixed) {
+    if (ordera_ == 'R') A.bind(a, n, m, lda, true, st);
+    else A.bind(a, m, n, lda, true, st);
+  }
+  const T *a_use = mixed ? a : A.d;
   if (omega) Om.bind(omega, Nl, n, ldomega, true, st);
   DBuf<T> Y((size_t)m * Nl), Q((size_t)m * l);
-  sketch_dev<T>(c.sc, m, n, Nl, ordera_, A.d, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
+  sketch_dev<T>(c.sc, m, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
                 Nl);
   tm.mark(1, st);
   sync();
@@ -524,7 +530,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
     T *u = (ut_root >= -1) ? ut : vt;
     const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
     U.bind(u, k, m, ld, false, st);
-    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ld, wu);
+    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, U.d, ld, wu);
     tm.mark(4, st);
     S.back(st);
     if (wu) U.back(st, k);
@@ -542,9 +548,9 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
     if (wu) U.bind(ut, k, m, ldut, false, st);
     if (wv) V.bind(vt, vcols, n, ldvt, false, st);
     if (bp == "GR")
-      post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+      post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
     else
-      post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+      post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, U.d, ldut, V.d, ldvt, wu, wv);
     tm.mark(4, st);
     S.back(st);
     if (wu) U.back(st, k);

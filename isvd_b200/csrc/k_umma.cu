@@ -612,6 +612,31 @@ void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, 
   }
 }
 
+template <class T>
+void split_rows(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np, bool transpose,
+                __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st) {
+  Runtime &rt = Runtime::get();
+  if (ld % 8) fail(kErrArgument, "split_rows: ld must be a multiple of 8");
+  if (!transpose) {
+    if (ld < cols) fail(kErrArgument, "split_rows: plane too narrow");
+    const long long total = rows * (ld / 8);
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 32LL * rt.num_sms);
+    split_kernel<T><<<blocks, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows, np, dst, ld, plane_stride);
+    KLAUNCHED();
+  } else {
+    // output rows = cols of src, output columns = rows of src; the grid covers ld when
+    // ld == roundup(rows, 64)
+    if (ld != (rows + 63) / 64 * 64) fail(kErrArgument, "split_rows: transposed rows need ld = roundup(rows, 64)");
+    dim3 grid((unsigned)((rows + 63) / 64), (unsigned)((cols + 31) / 32));
+    split_t_kernel<T><<<grid, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, cols, np, dst, ld, plane_stride);
+    KLAUNCHED();
+  }
+}
+template void split_rows<float>(const float *, long long, long long, long long, long long, int, bool, __nv_bfloat16 *,
+                                long long, long long, cudaStream_t);
+template void split_rows<double>(const double *, long long, long long, long long, long long, int, bool,
+                                 __nv_bfloat16 *, long long, long long, cudaStream_t);
+
 void rng_gaussian_bf16_t(__nv_bfloat16 *dst, long long n, long long Nl, long long ld, long long rows_pad,
                          uint64_t seed, cudaStream_t st) {
   Runtime &rt = Runtime::get();
@@ -631,8 +656,8 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   Runtime &rt = Runtime::get();
   if (rt.cc_major != 10) fail(kErrUnsupported, "tcgen05 GEMM needs an sm_100 device (found sm_%d%d)", rt.cc_major,
                               rt.cc_minor);
-  int *status = reinterpret_cast<int *>(rt.ctl + 32);
-  CK(cudaMemsetAsync(status, 0, sizeof(int), st));
+  int *status = g.status ? g.status : reinterpret_cast<int *>(rt.ctl + 32);
+  if (!g.status) CK(cudaMemsetAsync(status, 0, sizeof(int), st));
   const bool amn = g.A.mn_major, bmn = g.B.mn_major;
   const int stage64 = g.A.np * BM * 64 * 2 + g.B.np * 256 * 64 * 2;
   const bool small_n = g.N <= 128;
@@ -649,6 +674,7 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   } else {
     launch_t<256, 32, false, false>(g, st, status);
   }
+  if (g.status) return;  // the caller checks the status word (no host synchronisation here)
   int h = 0;
   CK(cudaMemcpyAsync(&h, status, sizeof(int), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));

@@ -6,6 +6,9 @@
 //   block Gram   Y': 3 x 3 planes, 6 products  (W feeds the orthogonalizing eigensolve)
 //   G = Qs' Qs   2 x 2 planes, 3 products      (errors average over the m-long inner products)
 //   Z = A' Qbar  Qbar': 2 planes x A: 2 planes, 3 products
+#include <algorithm>
+#include <cstdlib>
+
 #include "kernels.h"
 #include "mixed.h"
 #include "runtime.h"
@@ -48,35 +51,102 @@ constexpr bool is_double() { return sizeof(T) == 8; }
 
 }  // namespace
 
+// Rows per streamed panel of A: about 1 GiB of A, a multiple of 128 rows (environment override
+// ISVD_GPU_PANEL_ROWS, rounded to 128).
+static long long panel_rows(long long m, long long n, size_t elem) {
+  long long p = (long long)((1ll << 30) / ((long long)n * (long long)elem));
+  if (const char *e = getenv("ISVD_GPU_PANEL_ROWS")) p = atoll(e);
+  p = std::max<long long>(128, p / 128 * 128);
+  return std::min<long long>(p, m);
+}
+
+// Sketch Y = A Omega with A processed in row panels: each panel is split into A's three bf16 planes
+// (kept for the postprocess) and multiplied by Omega' on the tensor cores.  When A is in host
+// memory, panel p + 1 is copied to the device on the copy stream while panel p is split and
+// multiplied, so that the PCIe transfer overlaps the tensor-core work (the reference streams A in
+// column panels through the GPU for the same reason, gpu/stage/@x@_sketch_gpu.h:238-254).  The
+// FP32 A is never resident on the device in this mode.
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                   long long ldom, uint64_t seed, T *y, long long ldy) {
-  PlaneBuf local;
-  PlaneBuf *ap = &local;
-  MixedCache *mc = c.cache;
-  if (ordera == 'R') make_planes<T>(local, a, lda, m, n, 3, false, c.st);
-  else make_planes<T>(local, a, lda, n, m, 3, true, c.st);  // column-major A is A' row-major
+  Runtime &rt = Runtime::get();
+  const bool a_dev = is_device_pointer(a);
+  const long long ld = plane_ld(n), rp = plane_rows(m), ps = rp * ld;
+  MixedCache local;
+  MixedCache *mc = c.cache ? c.cache : &local;
+  mc->buf.alloc((size_t)3 * ps);
+  for (int q = 0; q < 3; ++q)  // zero rows [m, rp): TMA boxes of the last tile read them
+    if (rp > m)
+      CK(cudaMemsetAsync(mc->buf.p + (size_t)q * ps + (size_t)m * ld, 0, (size_t)(rp - m) * ld * 2, c.st));
+  Planes all;
+  all.ptr = mc->buf.p; all.np = 3; all.rows = m; all.cols = n; all.ld = ld; all.plane_stride = ps;
   PlaneBuf om;
   if (!omega) {
-    const long long ld = plane_ld(n), rp = plane_rows(Nl);
-    om.buf.alloc((size_t)rp * ld);
-    rng_gaussian_bf16_t(om.buf.p, n, Nl, ld, rp, seed, c.st);
-    om.P.ptr = om.buf.p; om.P.np = 1; om.P.rows = Nl; om.P.cols = n; om.P.ld = ld; om.P.plane_stride = rp * ld;
+    const long long old = plane_ld(n), orp = plane_rows(Nl);
+    om.buf.alloc((size_t)orp * old);
+    rng_gaussian_bf16_t(om.buf.p, n, Nl, old, orp, seed, c.st);
+    om.P.ptr = om.buf.p; om.P.np = 1; om.P.rows = Nl; om.P.cols = n; om.P.ld = old; om.P.plane_stride = orp * old;
   } else {
     make_planes<T>(om, omega, ldom, n, Nl, 3, true, c.st);  // Omega' planes (Nl x n)
   }
-  UmmaGemm g;
-  g.M = m; g.N = Nl; g.K = n;
-  g.A = ap->P; g.B = om.P;
-  set_products(g, g.A.np, g.B.np);
-  g.C = y; g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
-  g.tag = "sketch";
-  umma_gemm(g, c.st);
-  if (mc) {
-    mc->src = a; mc->m = m; mc->n = n; mc->ordera = ordera;
-    mc->buf = std::move(local.buf);
-    mc->A = local.P;
+  const long long P = panel_rows(m, n, sizeof(T));
+  DBuf<T> stage[2];
+  cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr}, ready = nullptr;
+  if (!a_dev) {
+    for (int b = 0; b < 2; ++b) {
+      stage[b].alloc((size_t)P * n);
+      CK(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&consumed[b], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    CK(cudaEventRecord(ready, c.st));  // staging buffers allocated on the compute stream
+    CK(cudaStreamWaitEvent(rt.copy_stream, ready, 0));
   }
+  int p = 0;
+  for (long long r0 = 0; r0 < m; r0 += P, ++p) {
+    const long long rows = std::min<long long>(P, m - r0);
+    __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
+    if (a_dev) {
+      if (ordera == 'R') split_rows<T>(a + r0 * lda, lda, 1, rows, n, 3, false, dst, ld, ps, c.st);
+      else split_rows<T>(a + r0, lda, 1, n, rows, 3, true, dst, ld, ps, c.st);  // A' rows r0.. as n x rows
+    } else {
+      const int b = p & 1;
+      if (p >= 2) CK(cudaStreamWaitEvent(rt.copy_stream, consumed[b], 0));
+      if (ordera == 'R') {
+        CK(cudaMemcpy2DAsync(stage[b].p, n * sizeof(T), a + r0 * lda, lda * sizeof(T), n * sizeof(T), rows,
+                             cudaMemcpyHostToDevice, rt.copy_stream));
+      } else {
+        CK(cudaMemcpy2DAsync(stage[b].p, rows * sizeof(T), a + r0, lda * sizeof(T), rows * sizeof(T), n,
+                             cudaMemcpyHostToDevice, rt.copy_stream));
+      }
+      CK(cudaEventRecord(copied[b], rt.copy_stream));
+      CK(cudaStreamWaitEvent(c.st, copied[b], 0));
+      if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, 3, false, dst, ld, ps, c.st);
+      else split_rows<T>(stage[b].p, rows, 1, n, rows, 3, true, dst, ld, ps, c.st);
+      CK(cudaEventRecord(consumed[b], c.st));
+    }
+    Planes ap = all;
+    ap.ptr = dst;
+    ap.rows = rows;
+    UmmaGemm g;
+    g.M = (int)rows; g.N = Nl; g.K = n;
+    g.A = ap; g.B = om.P;
+    set_products(g, 3, om.P.np);
+    g.C = y + r0 * ldy; g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
+    g.status = c.status;
+    g.tag = "sketch";
+    umma_gemm(g, c.st);
+  }
+  if (!a_dev) {
+    CK(cudaStreamSynchronize(c.st));
+    for (int b = 0; b < 2; ++b) {
+      cudaEventDestroy(copied[b]);
+      cudaEventDestroy(consumed[b]);
+    }
+    cudaEventDestroy(ready);
+  }
+  mc->src = a; mc->m = m; mc->n = n; mc->ordera = ordera;
+  mc->A = all;
 }
 
 template <class T>
@@ -91,7 +161,8 @@ void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, 
     set_products(g, a.np, a.np);
     g.batch = N; g.a_mn_step = l; g.b_mn_step = l; g.c_step = (long long)l * l;
     g.C = W; g.c_double = true; g.c_rs = l; g.c_cs = 1;
-    g.tag = "block_gram";
+    g.status = c.status;
+  g.tag = "block_gram";
     umma_gemm(g, c.st);
     return;
   }
@@ -101,6 +172,7 @@ void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, 
   set_products(g, 3, 3);
   g.batch = N; g.a_mn_step = l; g.b_mn_step = l; g.c_step = (long long)l * l;
   g.C = W; g.c_double = true; g.c_rs = l; g.c_cs = 1;
+  g.status = c.status;
   g.tag = "block_gram";
   umma_gemm(g, c.st);
 }
@@ -117,7 +189,8 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
     set_products(g, yp.np, 3);
     g.batch = N; g.a_k_step = l; g.b_k_step = l; g.c_step = l;
     g.C = out; g.c_double = is_double<T>(); g.c_rs = ldo; g.c_cs = 1;
-    g.tag = "block_apply";
+    g.status = c.status;
+  g.tag = "block_apply";
     umma_gemm(g, c.st);
     return;
   }
@@ -146,6 +219,7 @@ void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T
   set_products(g, 2, 2);
   g.C = G; g.c_double = true; g.c_rs = Nl; g.c_cs = 1;
   g.upper = true;
+  g.status = c.status;
   g.tag = "gram_full";
   umma_gemm(g, c.st);
   mirror_upper(G, Nl, Nl, c.st);
@@ -162,6 +236,7 @@ void mixed_apply_coeff(const StageCtx &c, const Planes &qp, int m, int Nl, int l
   g.A = qp; g.B = mt.P;
   set_products(g, qp.np, 3);
   g.C = qt; g.c_double = is_double<T>(); g.c_rs = ldqt; g.c_cs = 1;
+  g.status = c.status;
   g.tag = "coeff_apply";
   umma_gemm(g, c.st);
 }
@@ -177,6 +252,7 @@ void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T 
   if (mc && mc->src == a && mc->m == m && mc->n == n && mc->ordera == ordera && mc->buf.p) {
     ap = mc->A;
   } else {
+    if (!is_device_pointer(a)) fail(kErrArgument, "mixed postprocess: A is not on the device and not cached");
     if (ordera == 'R') make_planes<T>(local, a, lda, m, n, 2, false, c.st);
     else make_planes<T>(local, a, lda, n, m, 2, true, c.st);
     ap = local.P;
@@ -190,6 +266,7 @@ void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T 
   g.A = qp.P; g.B = b;
   set_products(g, 2, 2);
   g.C = z; g.c_double = is_double<T>(); g.c_rs = 1; g.c_cs = l;  // Z' tile written into Z (n x l)
+  g.status = c.status;
   g.tag = "project";
   umma_gemm(g, c.st);
 }
@@ -207,6 +284,7 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, double alp
   set_products(gg, 3, 3);
   gg.C = Bgc; gg.c_double = true; gg.c_rs = l; gg.c_cs = 1;
   gg.alpha = alpha;
+  gg.status = c.status;
   gg.tag = "kn_product";
   umma_gemm(gg, c.st);
 }

@@ -50,6 +50,7 @@ Runtime &Runtime::get() {
   g_rt.smem_optin = prop.sharedMemPerBlockOptin;
   CK(cudaStreamCreateWithFlags(&g_rt.own_stream, cudaStreamNonBlocking));
   g_rt.stream = g_rt.own_stream;
+  CK(cudaStreamCreateWithFlags(&g_rt.copy_stream, cudaStreamNonBlocking));
   // Keep freed pool memory cached: repeated solves reuse it without new cudaMalloc calls.
   cudaMemPool_t pool;
   CK(cudaDeviceGetDefaultMemPool(&pool, dev));
@@ -67,6 +68,7 @@ void Runtime::reset() {
   cudaStreamSynchronize(g_rt.stream);
   cudaFree(g_rt.ctl);
   cudaStreamDestroy(g_rt.own_stream);
+  cudaStreamDestroy(g_rt.copy_stream);
   g_rt = Runtime();
   g_init = false;
 }

@@ -46,6 +46,7 @@ struct Runtime {
   int device = -1;
   cudaStream_t stream = nullptr;      // stream in use
   cudaStream_t own_stream = nullptr;  // the library's own stream
+  cudaStream_t copy_stream = nullptr; // host-to-device panel transfers overlapped with compute
   int num_sms = 0;
   int cc_major = 0, cc_minor = 0;
   size_t smem_optin = 0;

@@ -44,6 +44,7 @@ void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a
                 long long ldom, uint64_t seed, T *y, long long ldy) {
   if (c.precision == kMixed) {
     mixed_sketch<T>(c, m, n, Nl, ordera, a, lda, omega, ldom, seed, y, ldy);
+    read_status(c, "Gaussian projection sketching");
     return;
   }
   DBuf<T> om;

@@ -42,6 +42,7 @@ struct UmmaGemm {
   int splits = 0;      // split-K (0: automatic); partial sums are added in FP64
   bool upper = false;  // symmetric output: only tiles touching the upper triangle, j >= i written
   const char *tag = "gemm";  // name under which launches are recorded when profiling is enabled
+  int *status = nullptr;     // device status word: set, the call returns without a host synchronisation
 };
 
 // Geometry of a plane buffer for a rows x cols matrix: ld = cols rounded up to 64, rows padded to
@@ -54,6 +55,12 @@ inline long long plane_rows(long long rows) { return (rows + 255) / 256 * 256; }
 template <class T>
 void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np,
                   bool transpose, __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st);
+
+// Planes for a block of rows only (no padding rows written): rows x cols of src (transpose:
+// cols x rows output, requiring ld == roundup(rows, 64)) into dst (already offset to the first row).
+template <class T>
+void split_rows(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np, bool transpose,
+                __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st);
 
 // Omega' drawn directly in bf16: plane(c, j) = bf16(N(0,1) value with index j * cols_total + c)
 // so that Omega(j, c) matches rng_gaussian's value index convention (rounded).

@@ -137,3 +137,38 @@ def test_mixed_driver_vs_fp64(lib, oracle, x):
     assert np.abs(s1 - s0).max() / s0.max() < 1e-5
     assert oracle.max_principal_angle(u1[:, :k], u0[:, :k]) < 1e-4
     assert oracle.max_principal_angle(v1[:, :k], v0[:, :k]) < 1e-4
+
+
+@pytest.mark.parametrize("ordera", [b"R", b"C"])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_mixed_streamed_panels(lib, oracle, ordera, where, monkeypatch):
+    """A in many row panels (panel size forced to 256 rows): host A streams through the copy stream;
+    the result equals the single-panel device result."""
+    torch = pytest.importorskip("torch")
+    m, n, k, p, Nn = 3000, 1500, 12, 8, 6
+    l = k + p
+    a = lowrank(m, n, 300, 0.98, 1e-6, 23)
+    om = np.random.default_rng(4).standard_normal((n, l * Nn))
+    aa = np.ascontiguousarray(a) if ordera == b"R" else np.asfortranarray(a)
+    lda = n if ordera == b"R" else m
+    prm = lib.create_param(m, n, k, p, Nn)
+
+    def run(arr):
+        s = np.zeros(l)
+        ut = np.zeros((m, l))
+        vt = np.zeros((n, l))
+        retv, _, st = lib.isvd("d", prm, ("GP", "GR", "KN", "GR"), arr, lda, s, ut, l, vt, l, ordera=ordera,
+                               omega=np.ascontiguousarray(om), ldomega=l * Nn, precision=1)
+        assert st == 0, lib.last_error()
+        return s, ut, vt, int(retv[2][0])
+
+    ref = run(aa)
+    monkeypatch.setenv("ISVD_GPU_PANEL_ROWS", "256")
+    if where == "host":
+        got = run(aa)
+    else:
+        ad = torch.from_numpy(np.ascontiguousarray(aa.T) if ordera == b"C" else aa).cuda()
+        got = run(ad)
+    assert got[3] == ref[3]
+    assert np.abs(got[0] - ref[0]).max() < 1e-6 * ref[0].max()
+    assert oracle.max_principal_angle(got[1][:, :k], ref[1][:, :k]) < 1e-5
