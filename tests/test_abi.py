@@ -102,3 +102,20 @@ def test_query_defaults_without_gpu(lib, reflib):
     for alg, n in (("KN", 2), ("WY", 9)):
         assert list(lib.query("d", alg, n)) == list(reflib.query("d", alg, n))
         assert np.allclose(lib.query("s", alg, n), reflib.query("s", alg, n))
+
+
+def build_c_demo(tmp_path, lib):
+    """Compile tests/c/isvd_demo.c against include/ and link it with the library (plain gcc)."""
+    exe = str(tmp_path / "isvd_demo")
+    libdir = os.path.dirname(lib.path)
+    cmd = ["gcc", "-std=gnu99", "-O1", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"), "-I",
+           os.path.join(REPO, "include", "mpi_shim"), os.path.join(REPO, "tests", "c", "isvd_demo.c"), "-o", exe,
+           "-L" + libdir, "-lisvd_gpu_b200", "-Wl,-rpath," + libdir, "-lm"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return exe
+
+
+def test_c_caller_compiles_and_links(tmp_path, lib):
+    """A C program written against include/isvd.h builds and links against the library alone."""
+    exe = build_c_demo(tmp_path, lib)
+    assert os.path.exists(exe)
