@@ -207,6 +207,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--single", action="store_true",
+                    help="one MIXED solve and its stage times, nothing else (for ncu launch lists / captures)")
     args = ap.parse_args()
     w = WORKLOADS[args.size]
     if args.impl == "reference":
@@ -238,6 +240,11 @@ def main():
     ut = torch.zeros((m, l), dtype=torch.float32, device=dev)
     vt = torch.zeros((n, l), dtype=torch.float32, device=dev)
     seed = w["seed"]
+    if args.single:
+        retv, times = solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
+        print(json.dumps({"stage_ms": [1e3 * t for t in times], "kn_iterations": int(retv[2][0])}), flush=True)
+        lib.lib.isvd_gpu_set_stream(None)
+        return
 
     def barrier():
         if dist is not None:

@@ -22,7 +22,7 @@ int main(int argc, char **argv) {
   for (int i = 0; i < m; ++i)
     for (int j = 0; j < n; ++j) {
       double v = 0.0;
-      for (int r = 0; r < 40; ++r) v += pow(0.8, r) * cos(0.37 * (r + 1) * (i + 1)) * sin(0.53 * (r + 1) * (j + 1));
+      for (int r = 0; r < 12; ++r) v += pow(0.8, r) * cos(0.37 * (r + 1) * (i + 1)) * sin(0.53 * (r + 1) * (j + 1));
       a[(size_t)i * n + j] = v;
     }
   isvd_Param param = isvd_createParam(m, n, k, p, N, 0, MPI_COMM_WORLD);
