@@ -98,6 +98,33 @@ void isvd_gpu_profile_enable( int on );
 void isvd_gpu_profile_reset( void );
 int  isvd_gpu_profile_get( const char *tag, double *ms, unsigned long long *launches, double *flops );
 
+/* ---------------------------------------------------------------- no device allocation
+ * Kolmogorov-Nagumo integration in FP64 that allocates no device memory: no cudaMalloc or
+ * cudaFree, no stream-ordered pool, no allocating library routine.  It has no counterpart in the
+ * reference (whose isvd_dIntegrateKolmogorovNagumo, core/stage/@x@_integrate_kolmogorov_nagumo.c:
+ * 97-137, mallocs its workspace on every call); it is for callers that must not allocate once
+ * they run, e.g. a process whose device memory is all held by its own pool allocator.
+ * Arguments, argv / retv and results as isvd_dIntegrateKolmogorovNagumo, except:
+ *   - yst and qt must be device (or managed) memory of the current device;
+ *   - the work is enqueued on `stream` (a cudaStream_t of the current device; NULL is the legacy
+ *     default stream) and the call returns once it has completed; FP64 whatever the precision mode;
+ *   - every intermediate lives in one statically allocated device array of 8 MiB (1,048,576
+ *     doubles) per device.  Sizes that do not fit -- (N l)^2 + 5 N l^2 + 13 l^2 + 96 doubles, each
+ *     term rounded up to 32 -- or l > 160 are rejected with ISVD_GPU_ERROR_ARGUMENT and a message
+ *     (N l = 512 with l = 64 fits; N l = 1024 does not).
+ * The first call on each device sets up: it looks up the array's address (which loads the device
+ * code that holds it) and reads the SM count; make that first call before any stream capture on
+ * the device.  Nothing in the array has to be zero on entry: each call clears its own status and
+ * barrier words.  The array is shared by all calls on a device, so overlapping calls would race
+ * on it; each call holds the library's process-wide lock until its work has completed, which makes
+ * calls from several threads or streams run one after another.
+ * Returns an ISVD_GPU_* status. */
+int isvd_dIntegrateKolmogorovNagumo_noalloc(
+    const isvd_Param param, const isvd_d_val_t *argv, const isvd_int_t argc, isvd_d_val_t *retv,
+    const isvd_int_t retc, const isvd_d_val_t *yst, const isvd_int_t ldyst, isvd_d_val_t *qt,
+    const isvd_int_t ldqt, void *stream
+);
+
 #if defined(__cplusplus)
 }
 #endif

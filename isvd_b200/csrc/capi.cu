@@ -771,5 +771,35 @@ isvd_Param isvd_createParam(const isvd_int_t nrow, const isvd_int_t ncol, const 
 ISVD_STAGES(s, float)
 ISVD_STAGES(d, double)
 
+// Kolmogorov-Nagumo integration without device allocation (isvd/b200.h).  Argument meaning and
+// checks as isvd_dIntegrateKolmogorovNagumo; the stage itself is integrate_kn_static.
+int isvd_dIntegrateKolmogorovNagumo_noalloc(const isvd_Param param, const isvd_d_val_t *argv, const isvd_int_t argc,
+                                            isvd_d_val_t *retv, const isvd_int_t retc, const isvd_d_val_t *yst,
+                                            const isvd_int_t ldyst, isvd_d_val_t *qt, const isvd_int_t ldqt,
+                                            void *stream) {
+  return api_call([&] {
+    if (argc > 0) REQUIRE(argv != nullptr);
+    if (retc > 0) REQUIRE(retv != nullptr);
+    if (argc < 0) {
+      query_kn(retv, retc);
+      return;
+    }
+    require_single_rank(param);
+    const int m = param.nrow_proc, l = param.dim_sketch, N = param.num_sketch, Nl = param.dim_sketch_total;
+    REQUIRE(ldyst >= Nl);
+    REQUIRE(ldqt >= l);
+    int ai = -1;
+    const int maxit = (argc > ++ai) ? (int)argv[ai] : 256;
+    const double tol = (argc > ++ai) ? argv[ai] : 1e-4;
+    REQUIRE(maxit >= 0);
+    REQUIRE(tol >= 0);
+    const IterResult r = integrate_kn_static(static_cast<cudaStream_t>(stream), m, l, N, yst, ldyst, qt, ldqt,
+                                             maxit, tol);
+    int ri = -1;
+    if (retc > ++ri) retv[ri] = (double)r.iterations;
+    if (retc > ++ri) retv[ri] = r.error;
+  });
+}
+
 }  // extern "C"
 #pragma GCC visibility pop

@@ -185,6 +185,49 @@ void launch(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, cudaStream_t st) {
   }
 }
 
+// As launch(), for callers that cannot allocate: the SM count comes from the caller and the
+// split-K partial sums go to the caller's buffer of `cap` elements (fewer splits when it is short).
+template <class T, class Tout, int BM, int BN, int BK>
+void launch_fixed(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, int sms, T *partial, size_t cap, cudaStream_t st) {
+  const int gx = (g.M + BM - 1) / BM, gy = (g.N + BN - 1) / BN;
+  const long long tiles = (long long)gx * gy * g.batch;
+  int splits = g.splits;
+  if (splits <= 0) {
+    const long long target = 2LL * sms;
+    splits = 1;
+    if (tiles < target) {
+      long long s = (target + tiles - 1) / tiles;
+      long long smax = std::max<long long>(1, g.K / (8 * BK));
+      splits = (int)std::min<long long>(s, smax);
+    }
+  }
+  const long long per_split = (long long)g.batch * g.M * g.N;
+  const long long fit = partial ? (long long)(cap / (size_t)per_split) : 1;
+  splits = (int)std::max<long long>(1, std::min<long long>(splits, fit));
+  int kchunk = (g.K + splits - 1) / splits;
+  kchunk = ((kchunk + BK - 1) / BK) * BK;
+  if (kchunk <= 0) kchunk = BK;
+  splits = std::max(1, (g.K + kchunk - 1) / kchunk);
+  T *part = splits > 1 ? partial : nullptr;
+  dim3 grid(gx, gy, g.batch * splits);
+#define ISVD_GEMM_CASE(AK, BN_)                                                                   \
+  if (a_kc == AK && b_nc == BN_) {                                                                \
+    gemm_kernel<T, Tout, BM, BN, BK, AK, BN_><<<grid, kThreads, 0, st>>>(g, splits, kchunk, part); \
+    KLAUNCHED();                                                                                  \
+  }
+  ISVD_GEMM_CASE(true, true)
+  ISVD_GEMM_CASE(true, false)
+  ISVD_GEMM_CASE(false, true)
+  ISVD_GEMM_CASE(false, false)
+#undef ISVD_GEMM_CASE
+  if (splits > 1) {
+    const long long total = (long long)g.M * g.N * g.batch;
+    int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * sms);
+    splitk_reduce_kernel<T, Tout><<<blocks, 256, 0, st>>>(g, splits, part);
+    KLAUNCHED();
+  }
+}
+
 }  // namespace
 
 template <class T, class Tout>
@@ -206,6 +249,26 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
   else
     launch<T, Tout, 128, 128, 16>(g, a_kc, b_nc, st);
 }
+
+template <class T, class Tout>
+void gemm_fixed(const Gemm<T, Tout> &g, int num_sms, T *partial, size_t cap, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
+  if (g.K <= 0) {
+    if (g.beta == 1.0) return;
+    fail(kErrArgument, "gemm: empty inner dimension with beta != 1");
+  }
+  const bool a_kc = (g.a_cs == 1);
+  const bool b_nc = (g.b_cs == 1);
+  if (!a_kc && g.a_rs != 1) fail(kErrArgument, "gemm: operand A has no unit stride");
+  if (!b_nc && g.b_rs != 1) fail(kErrArgument, "gemm: operand B has no unit stride");
+  const long long tiles128 = (long long)((g.M + 127) / 128) * ((g.N + 127) / 128) * g.batch;
+  if (g.M <= 64 || g.N <= 64 || tiles128 < 2LL * num_sms)
+    launch_fixed<T, Tout, 64, 64, 16>(g, a_kc, b_nc, num_sms, partial, cap, st);
+  else
+    launch_fixed<T, Tout, 128, 128, 16>(g, a_kc, b_nc, num_sms, partial, cap, st);
+}
+
+template void gemm_fixed<double, double>(const Gemm<double, double> &, int, double *, size_t, cudaStream_t);
 
 template void gemm<double, double>(const Gemm<double, double> &, cudaStream_t);
 template void gemm<float, float>(const Gemm<float, float> &, cudaStream_t);

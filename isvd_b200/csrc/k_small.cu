@@ -569,4 +569,17 @@ void kn_step(const KnStep &a, cudaStream_t st) {
   KLAUNCHED();
 }
 
+void kn_step_fixed(const KnStep &a, int num_sms, cudaStream_t st) {
+  if (a.l > 160) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > 160", a.l);
+  const int nr = (a.l + 15) / 16;
+  int blocks = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kn_step_kernel, kKnThreads, 0));
+  int grid = std::min(2 * nr * nr, blocks * num_sms);
+  grid = std::max(1, std::min(grid, num_sms));
+  KnStep arg = a;
+  void *args[] = {&arg};
+  CK(cudaLaunchCooperativeKernel((void *)kn_step_kernel, dim3(grid), dim3(kKnThreads), args, 0, st));
+  KLAUNCHED();
+}
+
 }  // namespace isvdb

@@ -83,4 +83,12 @@ struct KnStep {
 };
 void kn_step(const KnStep &a, cudaStream_t st);
 
+// Launchers for the entry points that run on static scratch and must not allocate: they take the
+// SM count from the caller instead of the library runtime (whose set-up allocates), and gemm_fixed
+// puts split-K partial sums in the caller's buffer of `cap` elements (splitting less, or not at
+// all, when it is short).
+template <class T, class Tout>
+void gemm_fixed(const Gemm<T, Tout> &g, int num_sms, T *partial, size_t cap, cudaStream_t st);
+void kn_step_fixed(const KnStep &a, int num_sms, cudaStream_t st);
+
 }  // namespace isvdb

@@ -46,6 +46,11 @@ template <class T>
 IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs, long long ldq, T *qt,
                             long long ldqt, int maxit, double tol);
 
+// Kolmogorov-Nagumo integration in FP64 on the static device scratch of noalloc.cu: no device
+// allocation, operands in device memory, enqueued on `st`; returns once the work has completed.
+IterResult integrate_kn_static(cudaStream_t st, int m, int l, int N, const double *qs, long long ldq, double *qt,
+                               long long ldqt, int maxit, double tol);
+
 template <class T>
 IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs, long long ldq, T *qt,
                             long long ldqt, const WyArgs &w);
