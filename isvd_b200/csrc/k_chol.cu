@@ -1,0 +1,236 @@
+// Small dense FP64 kernels of the QR-based stages and of Wen-Yin integration: batched Cholesky
+// with an in-place triangular inverse, the Householder sign rule of a QR factor, batched dot
+// products and small linear combinations.  One CTA per l x l matrix, the matrix in shared memory.
+#include <algorithm>
+#include <cmath>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace isvdb {
+namespace {
+
+constexpr int kCholThreads = 512;
+
+// Sum over the block; every thread returns the same value (same summation order).
+__device__ double block_sum(double v, double *red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int i = 0; i < nw; ++i) s += red[i];
+  return s;
+}
+
+// A = alpha W + (shift_abs + shift_rel trace(alpha W)) I from the upper triangle of W (n x n,
+// row-major, batch stride n^2).  Cholesky A = R' R (R upper; right-looking), then X = R^-1 in
+// place, column by column from the already inverted leading block (the order of LAPACK's trti2).
+// A pivot that is not above piv_rel times its starting diagonal value (or is not finite) stops
+// the CTA and sets *status = kStatusNotPD.  Output: X with zeros below the diagonal (kCholFactor)
+// or out_scale X X' = out_scale A^-1 (kCholInverse).
+__global__ void __launch_bounds__(kCholThreads)
+    chol_inv_kernel(int n, const double *__restrict__ W, double alpha, double shift_abs, double shift_rel,
+                    double piv_rel, double *__restrict__ out, double out_scale, int mode, int *status) {
+  extern __shared__ double sm[];
+  __shared__ double red[kCholThreads / 32];
+  const int ld = n + 1, tid = threadIdx.x, nt = blockDim.x;
+  double *R = sm;                       // n x ld
+  double *aux = sm + (size_t)n * ld;    // n: starting diagonal, then the column being inverted
+  const double *w = W + (size_t)blockIdx.x * n * n;
+  double tr = 0.0;
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e - i * n;
+    const double v = alpha * ((i <= j) ? w[(size_t)i * n + j] : w[(size_t)j * n + i]);
+    R[i * ld + j] = v;
+    if (i == j) tr += v;
+  }
+  const double shift = shift_abs + shift_rel * block_sum(tr, red);
+  for (int i = tid; i < n; i += nt) {
+    R[i * ld + i] += shift;
+    aux[i] = R[i * ld + i];
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const double d = R[k * ld + k];
+    if (!(d > piv_rel * aux[k]) || !(d > 0.0) || !(d < INFINITY)) {  // same decision in every thread
+      if (tid == 0) atomicExch(status, kStatusNotPD);
+      return;
+    }
+    const double r = sqrt(d);
+    __syncthreads();
+    if (tid == 0) R[k * ld + k] = r;
+    for (int j = k + 1 + tid; j < n; j += nt) R[k * ld + j] /= r;
+    __syncthreads();
+    const int mm = n - k - 1;
+    for (int e = tid; e < mm * mm; e += nt) {
+      const int i = k + 1 + e / mm, j = k + 1 + e % mm;
+      if (j >= i) R[i * ld + j] -= R[k * ld + i] * R[k * ld + j];
+    }
+    __syncthreads();
+  }
+  // X(0:j, j) = -X(0:j, 0:j) R(0:j, j) / r_jj ;  x_jj = 1 / r_jj.  Four threads per row.
+  const int quad = tid >> 2, ql = tid & 3, nq = nt >> 2;
+  for (int j = 0; j < n; ++j) {
+    const double inv = 1.0 / R[j * ld + j];
+    for (int i = tid; i < j; i += nt) aux[i] = R[i * ld + j];
+    __syncthreads();
+    for (int i0 = 0; i0 < j; i0 += nq) {
+      const int i = i0 + quad;
+      double acc = 0.0;
+      if (i < j)
+        for (int k = i + ql; k < j; k += 4) acc += R[i * ld + k] * aux[k];
+      acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+      acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+      if (i < j && ql == 0) R[i * ld + j] = -inv * acc;
+    }
+    if (tid == 0) R[j * ld + j] = inv;
+    __syncthreads();
+  }
+  double *o = out + (size_t)blockIdx.x * n * n;
+  if (mode == kCholFactor) {
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e - i * n;
+      o[e] = (j >= i) ? out_scale * R[i * ld + j] : 0.0;
+    }
+  } else {
+    for (int e = tid; e < n * n; e += nt) {
+      const int i = e / n, j = e - i * n;
+      double acc = 0.0;
+      for (int k = (i > j ? i : j); k < n; ++k) acc += R[i * ld + k] * R[j * ld + k];
+      o[e] = out_scale * acc;
+    }
+  }
+}
+
+// Householder sign rule.  P = Qtop X is the top n x n block of the next Q factor (positive-
+// diagonal convention).  A Householder QR (LAPACK geqrf / gelqf) of the same matrix returns
+// Q diag(s) with s_j = -sign(pivot_j) of the LU factorization of P - diag(s) carried out with
+// exactly that choice of s (Ballard, Demmel, Grigori, Jacquelin, Knight, Nguyen, "Reconstructing
+// Householder vectors from tall-skinny QR", J. Parallel Distrib. Comput. 85 (2015)).  X's
+// columns are multiplied by s, so that Q X is the Householder factor.
+template <class T>
+__global__ void __launch_bounds__(kCholThreads)
+    hh_sign_kernel(int n, const T *__restrict__ Q, long long q_ld, long long q_bs, double *__restrict__ X) {
+  extern __shared__ double sm[];
+  const int ld = n + 1, tid = threadIdx.x, nt = blockDim.x;
+  double *P = sm, *sg = sm + (size_t)n * ld;
+  const T *q = Q + blockIdx.x * q_bs;
+  double *x = X + (size_t)blockIdx.x * n * n;
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e - i * n;
+    double acc = 0.0;
+    for (int k = 0; k <= j; ++k) acc += (double)q[i * q_ld + k] * x[(size_t)k * n + j];
+    P[i * ld + j] = acc;
+  }
+  __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    const double piv = P[j * ld + j];
+    const double s = (piv >= 0.0) ? -1.0 : 1.0;
+    const double u = piv - s;  // |u| >= 1
+    __syncthreads();
+    if (tid == 0) sg[j] = s;
+    for (int i = j + 1 + tid; i < n; i += nt) P[i * ld + j] /= u;
+    __syncthreads();
+    const int mm = n - j - 1;
+    for (int e = tid; e < mm * mm; e += nt) {
+      const int i = j + 1 + e / mm, c = j + 1 + e % mm;
+      P[i * ld + c] -= P[i * ld + j] * P[j * ld + c];
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < n * n; e += nt) x[e] *= sg[e % n];
+}
+
+constexpr int kDotThreads = 1024;
+
+__global__ void __launch_bounds__(kDotThreads) dots_kernel(DotJobs jobs, double *__restrict__ out) {
+  __shared__ double red[kDotThreads / 32];
+  const DotJob jb = jobs.job[blockIdx.x];
+  double v = 0.0;
+  if (jb.trace) {
+    for (long long i = threadIdx.x; i < jb.n; i += blockDim.x) v += jb.a[i * jb.n + i];
+  } else {
+    for (long long i = threadIdx.x; i < jb.n; i += blockDim.x) {
+      const double x = jb.a[i] - (jb.b ? jb.b[i] : 0.0);
+      const double y = jb.c[i] - (jb.d ? jb.d[i] : 0.0);
+      v += x * y;
+    }
+  }
+  v = block_sum(v, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = v;
+}
+
+// (out may alias x or y: each entry is read and written by the same thread)
+__global__ void lincomb_kernel(double *out, const double *x, double a, const double *y, double b, double c,
+                               long long rows, long long cols) {
+  const long long total = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e / cols, j = e - i * cols;
+    double v = (i == j) ? c : 0.0;
+    if (x) v += a * x[e];
+    if (y) v += b * y[e];
+    out[e] = v;
+  }
+}
+
+// d_i = num / (half * max(lambda_i, 0) + add)
+__global__ void recip_affine_kernel(const double *__restrict__ lam, int n, double num, double half, double add,
+                                    double *__restrict__ d) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) d[i] = num / (half * fmax(lam[i], 0.0) + add);
+}
+
+size_t chol_smem(int n) { return ((size_t)n * (n + 1) + n) * sizeof(double); }
+
+}  // namespace
+
+void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
+                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return;
+  const size_t smem = chol_smem(n);
+  if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "Cholesky: l = %d exceeds on-chip capacity", n);
+  CK(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  chol_inv_kernel<<<batch, kCholThreads, smem, st>>>(n, W, alpha, shift_abs, shift_rel, piv_rel, out, out_scale,
+                                                     mode, status);
+  KLAUNCHED();
+}
+
+template <class T>
+void hh_sign_batched(int n, int batch, const T *Q, long long q_ld, long long q_bs, double *X, cudaStream_t st) {
+  if (n <= 0 || batch <= 0) return;
+  const size_t smem = chol_smem(n);
+  if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "QR sign rule: l = %d exceeds on-chip capacity", n);
+  CK(cudaFuncSetAttribute(hh_sign_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  hh_sign_kernel<T><<<batch, kCholThreads, smem, st>>>(n, Q, q_ld, q_bs, X);
+  KLAUNCHED();
+}
+
+void dots(const DotJobs &jobs, double *out, cudaStream_t st) {
+  if (jobs.count <= 0) return;
+  if (jobs.count > kMaxDotJobs) fail(kErrArgument, "dots: %d jobs > %d", jobs.count, kMaxDotJobs);
+  dots_kernel<<<jobs.count, kDotThreads, 0, st>>>(jobs, out);
+  KLAUNCHED();
+}
+
+void lincomb(double *out, const double *x, double a, const double *y, double b, double c, long long rows,
+             long long cols, cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return;
+  const long long total = rows * cols;
+  const int grid = (int)std::min<long long>((total + 255) / 256, 8LL * Runtime::get().num_sms);
+  lincomb_kernel<<<grid, 256, 0, st>>>(out, x, a, y, b, c, rows, cols);
+  KLAUNCHED();
+}
+
+void recip_affine(const double *lam, int n, double num, double half, double add, double *d, cudaStream_t st) {
+  if (n <= 0) return;
+  recip_affine_kernel<<<1, 256, 0, st>>>(lam, n, num, half, add, d);
+  KLAUNCHED();
+}
+
+template void hh_sign_batched<double>(int, int, const double *, long long, long long, double *, cudaStream_t);
+template void hh_sign_batched<float>(int, int, const float *, long long, long long, double *, cudaStream_t);
+
+}  // namespace isvdb

@@ -83,6 +83,47 @@ struct KnStep {
 };
 void kn_step(const KnStep &a, cudaStream_t st);
 
+// ---------------------------------------------------------------- k_chol.cu
+enum CholMode { kCholFactor = 0, kCholInverse = 1 };
+constexpr int kStatusNotPD = 7;  // status word: a Cholesky pivot was not positive (or lost its magnitude)
+
+// Per n x n matrix (row-major, batch stride n^2; upper triangle read):
+//   A = alpha W + (shift_abs + shift_rel trace(alpha W)) I = R' R,  X = R^-1 (upper);
+//   out = X (kCholFactor) or out_scale X X' = out_scale A^-1 (kCholInverse).
+// A pivot not above piv_rel times its starting diagonal value sets *status = kStatusNotPD.
+void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
+                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st);
+// X_b := X_b diag(s_b) with the Householder signs of the QR factor whose top n x n block is
+// Qtop_b X_b (Qtop_b = rows 0..n-1 of Q + b q_bs, row stride q_ld).
+template <class T>
+void hh_sign_batched(int n, int batch, const T *Q, long long q_ld, long long q_bs, double *X, cudaStream_t st);
+
+constexpr int kMaxDotJobs = 8;
+// value = trace(a) (a n x n) when trace, else sum_i (a_i - b_i)(c_i - d_i) over n entries (b, d optional)
+struct DotJob {
+  const double *a = nullptr, *b = nullptr, *c = nullptr, *d = nullptr;
+  long long n = 0;
+  int trace = 0;
+};
+struct DotJobs {
+  DotJob job[kMaxDotJobs];
+  int count = 0;
+  void dot(const double *a, const double *b, const double *c, const double *d, long long n) {
+    DotJob &j = job[count++];
+    j.a = a; j.b = b; j.c = c; j.d = d; j.n = n; j.trace = 0;
+  }
+  void trace(const double *a, long long n) {
+    DotJob &j = job[count++];
+    j.a = a; j.n = n; j.trace = 1;
+  }
+};
+void dots(const DotJobs &jobs, double *out, cudaStream_t st);  // out[k] = value of job k
+// out = a x + b y + c I  (rows x cols, contiguous; x or y may be null)
+void lincomb(double *out, const double *x, double a, const double *y, double b, double c, long long rows,
+             long long cols, cudaStream_t st);
+// d_i = num / (half max(lambda_i, 0) + add)
+void recip_affine(const double *lam, int n, double num, double half, double add, double *d, cudaStream_t st);
+
 // Launchers for the entry points that run on static scratch and must not allocate: they take the
 // SM count from the caller instead of the library runtime (whose set-up allocates), and gemm_fixed
 // puts split-K partial sums in the caller's buffer of `cap` elements (splitting less, or not at

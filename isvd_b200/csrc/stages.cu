@@ -276,7 +276,7 @@ void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long l
 // ----------------------------------------------------------------------------- postprocess
 // Z = A' Qbar (reference @x@_postprocess.h:96-171, row block at P = 1).
 template <class T>
-static void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
                     long long ldqt, T *z) {
   if (c.precision == kMixed) {
     mixed_project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, z);
@@ -363,6 +363,7 @@ void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char orde
   template void sketch_dev<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, \
                               uint64_t, T *, long long);                                                        \
   template void orth_gramian_dev<T>(const StageCtx &, int, int, int, T *, long long);                           \
+  template void project<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, T *); \
   template IterResult integrate_kn_dev<T>(const StageCtx &, int, int, int, const T *, long long, T *, long long, \
                                           int, double);                                                         \
   template void integrate_hr_dev<T>(const StageCtx &, int, int, int, T *, long long, T *, long long);           \

@@ -59,6 +59,11 @@ template <class T>
 void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt);
 
 // Postprocessing.  s has l entries; ut (m x k, ldut), vt (n x k or n x l for TS, ldvt) when wanted.
+// Z = A' Qbar (n x l, row-major, ld l) for A m x n stored per ordera.
+template <class T>
+void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+             long long ldqt, T *z);
+
 template <class T>
 void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                       const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
