@@ -76,10 +76,15 @@ struct KnStep {
   int l;
   const double *Dc, *Dgc;
   double *C, *Cinv, *F, *err;
-  double *work;     // 8 * l * l doubles + 64
+  double *work;     // kn_step: kKnWorkMatrices l^2 + 64 doubles; kn_step_fixed: 8 l^2 + 64
   int *status;      // set nonzero on failure (timeout / no convergence)
   unsigned int *bar;  // 2 words, zero
   double ns_target = 1e-18;  // Newton-Schulz steps are chosen so that rho^(2^k) <= ns_target
+};
+constexpr int kKnWorkMatrices = 29;
+constexpr int kSeriesLen = 64;
+struct KnSeries {  // power-series coefficients of C(Z) and C(Z)^-1 (k_small.cu)
+  double c[kSeriesLen], d[kSeriesLen];
 };
 void kn_step(const KnStep &a, cudaStream_t st);
 

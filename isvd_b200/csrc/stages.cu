@@ -157,7 +157,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, c.st);
   }
-  DBuf<double> Bb(2 * nl), Mb(2 * nl), Bgc(nl), Dc(ll), Dgc(ll), C(ll), Ci(ll), F(ll), work(8 * ll + 64), err(1);
+  DBuf<double> Bb(2 * nl), Mb(2 * nl), Bgc(nl), Dc(ll), Dgc(ll), C(ll), Ci(ll), F(ll), work(kKnWorkMatrices * ll + 64), err(1);
   double *Bc = Bb.p, *Bp = Bb.p + nl, *Mc = Mb.p, *Mp = Mb.p + nl;
   copy2d<double, double>(G.p, Nl, 1, Bc, l, 1, Nl, l, c.st);   // Bc = Qs' Q0 = G[:, 0:l]   (:157)
   set_identity<double>(Mc, Nl, l, l, c.st);                   // Qc = Q0 = Qs [I; 0]       (:154)
