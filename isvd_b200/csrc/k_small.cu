@@ -347,7 +347,9 @@ __device__ void mm_tiles(int l, int ntile_row, int tile_begin, int tile_end, dou
   for (int t = first; t < tile_end; t += G) {
     const int tt = t - tile_begin;
     const int i0 = (tt / ntile_row) * 16, j0 = (tt % ntile_row) * 16;
-    // all loads of the tile are issued before any is used (one L2 round trip)
+    // all loads of the tile, Cin included, are issued before any is used (one L2 round trip)
+    const double cin = (beta != 0.0 && i0 + ty < l && j0 + tx < l) ? __ldcg(Cin + (size_t)(i0 + ty) * l + j0 + tx)
+                                                                    : 0.0;
     constexpr int kPer = (16 * 160 + kKnThreads - 1) / kKnThreads;
     double ra[kPer], rb[kPer];
 #pragma unroll
@@ -375,7 +377,7 @@ __device__ void mm_tiles(int l, int ntile_row, int tile_begin, int tile_end, dou
     for (int k = 0; k < l; ++k) acc = fma(As[ty][k], Bs[k][tx], acc);
     if (i < l && j < l) {
       double v = alpha * acc;
-      if (beta != 0.0) v += beta * __ldcg(Cin + (size_t)i * l + j);
+      if (beta != 0.0) v += beta * cin;
       if (i == j) v += diag;
       C[(size_t)i * l + j] = v;
     }
@@ -702,10 +704,19 @@ __global__ void __launch_bounds__(kKnThreads) kn_series_kernel(KnStep a, KnSerie
   }
   // F = C - Dc Cinv (:218); err = ||C - I||_F (:230-234)
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
+    const double ci = __ldcg(Ci + e);
     a.C[e] = __ldcg(C + e);
-    a.Cinv[e] = __ldcg(Ci + e);
+    a.Cinv[e] = ci;
+    if (a.fstack) {
+      a.fstack[ll + e] = a.fstack_scale * ci;
+      a.fstack[3 * ll + e] = ci;
+    }
   }
   mm_tiles(l, nr, 0, nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.F);
+  if (a.fstack) {
+    mm_tiles(l, nr, nt, 2 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack);
+    mm_tiles(l, nr, 2 * nt, 3 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack + 2 * ll);
+  }
   if (blockIdx.x == 0) {
     double f = 0.0;
     for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
@@ -797,8 +808,8 @@ void kn_step(const KnStep &a, cudaStream_t st) {
   const int nr = (a.l + 15) / 16;
   int blocks = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kn_series_kernel, kKnThreads, 0));
-  // enough CTAs for the widest phase (up to 4 products of nr^2 tiles), all co-resident
-  int grid = std::min(4 * nr * nr, blocks * rt.num_sms);
+  // two CTAs per tile of one product: phases with more products take several tiles per CTA
+  int grid = std::min(2 * nr * nr, blocks * rt.num_sms);
   grid = std::max(1, std::min(grid, rt.num_sms));
   KnStep arg = a;
   KnSeries ser = series;

@@ -80,6 +80,9 @@ struct KnStep {
   int *status;      // set nonzero on failure (timeout / no convergence)
   unsigned int *bar;  // 2 words, zero
   double ns_target = 1e-18;  // Newton-Schulz steps are chosen so that rho^(2^k) <= ns_target
+  // kn_step only: when set, also written as the 4l x l stack [F; Cinv * fstack_scale; F; Cinv]
+  double *fstack = nullptr;
+  double fstack_scale = 1.0;
 };
 constexpr int kKnWorkMatrices = 29;
 constexpr int kSeriesLen = 64;

@@ -276,13 +276,14 @@ void MixedGProduct::prepare(const StageCtx &c, int Nl_, const double *G) {
   make_planes<double>(g, G, Nl, Nl, Nl, 3, false, c.st);  // G is symmetric: rows (M) x K
 }
 
-void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, double alpha, double *Bgc) {
-  make_planes<double>(b, Bc, l, Nl, l, 3, true, c.st);  // Bc' planes (l x Nl): N x K
+void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, long long ldb, double alpha, double *Bgc,
+                          long long ldo) {
+  make_planes<double>(b, Bc, ldb, Nl, l, 3, true, c.st);  // Bc' planes (l x Nl): N x K
   UmmaGemm gg;
   gg.M = Nl; gg.N = l; gg.K = Nl;
   gg.A = g.P; gg.B = b.P;
   set_products(gg, 3, 3);
-  gg.C = Bgc; gg.c_double = true; gg.c_rs = l; gg.c_cs = 1;
+  gg.C = Bgc; gg.c_double = true; gg.c_rs = ldo; gg.c_cs = 1;
   gg.alpha = alpha;
   gg.status = c.status;
   gg.tag = "kn_product";

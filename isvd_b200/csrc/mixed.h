@@ -28,7 +28,8 @@ struct MixedGProduct {
   PlaneBuf g, b;
   int Nl = 0;
   void prepare(const StageCtx &c, int Nl_, const double *G);
-  void apply(const StageCtx &c, int l, const double *Bc, double alpha, double *Bgc);
+  // Bgc = alpha G Bc (Nl x l, row strides ldb and ldo)
+  void apply(const StageCtx &c, int l, const double *Bc, long long ldb, double alpha, double *Bgc, long long ldo);
 };
 
 // A's bf16 planes (m x n, K-major along n), made by the sketch and reused by the postprocess.

@@ -144,6 +144,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
                             long long ldqt, int maxit, double tol) {
   const int Nl = N * l;
   const size_t nl = (size_t)Nl * l, ll = (size_t)l * l;
+  const long long lw = 3LL * l;  // row stride of the iterate [M | B | Bgc]
   DBuf<double> G((size_t)Nl * Nl);
   PlaneBuf qp;  // MIXED: bf16 planes of Qs, shared by G and the final Qbar = Qs M
   if (c.precision == kMixed) make_planes<T>(qp, qs, ldq, m, Nl, 3, false, c.st);
@@ -157,10 +158,11 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, c.st);
   }
-  DBuf<double> Bb(2 * nl), Mb(2 * nl), Bgc(nl), Dc(ll), Dgc(ll), C(ll), Ci(ll), F(ll), work(kKnWorkMatrices * ll + 64), err(1);
-  double *Bc = Bb.p, *Bp = Bb.p + nl, *Mc = Mb.p, *Mp = Mb.p + nl;
-  copy2d<double, double>(G.p, Nl, 1, Bc, l, 1, Nl, l, c.st);   // Bc = Qs' Q0 = G[:, 0:l]   (:157)
-  set_identity<double>(Mc, Nl, l, l, c.st);                   // Qc = Q0 = Qs [I; 0]       (:154)
+  // iterates W = [M | B | Bgc] (Nl x 3l, current and next), [Dc; Dgc], step outputs
+  DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64), err(1);
+  double *Wc = Wb.p, *Wp = Wb.p + 3 * nl;
+  copy2d<double, double>(G.p, Nl, 1, Wc + l, lw, 1, Nl, l, c.st);  // Bc = Qs' Q0 = G[:, 0:l]   (:157)
+  set_identity<double>(Wc, Nl, l, lw, c.st);                       // Qc = Q0 = Qs [I; 0]       (:154)
   Runtime &rt = Runtime::get();
   const double invN = 1.0 / N;
   MixedGProduct gprod;  // MIXED: G's bf16 planes, reused by every iteration
@@ -170,62 +172,58 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   const int cap = maxit > 0 ? maxit : 1000000;
   int iter = 1;
   for (;; ++iter) {
+    double *Bc = Wc + l, *Bgc = Wc + 2 * l;
     if (c.precision == kMixed) {  // Bgc = G Bc / N   (:174-177)
-      gprod.apply(c, l, Bc, invN, Bgc.p);
+      gprod.apply(c, l, Bc, lw, invN, Bgc, lw);
     } else {
       Gemm<double, double> g = gm<double>(Nl, l, Nl);
       g.alpha = invN;
       g.A = G.p; g.a_rs = Nl; g.a_cs = 1;
-      g.B = Bc; g.b_rs = l; g.b_cs = 1;
-      g.C = Bgc.p; g.c_rs = l; g.c_cs = 1;
+      g.B = Bc; g.b_rs = lw; g.b_cs = 1;
+      g.C = Bgc; g.c_rs = lw; g.c_cs = 1;
       gemm(g, c.st);
     }
-    {  // Dc = Bc' Bc / N ; Dgc = Bc' Bgc / N   (:181-184)
+    {  // [Dc, Dgc] = Bc' [Bc, Bgc] / N   (:181-184), one batched product
       Gemm<double, double> g = gm<double>(l, l, Nl);
+      g.batch = 2;
       g.alpha = invN;
-      g.A = Bc; g.a_rs = 1; g.a_cs = l;
-      g.B = Bc; g.b_rs = l; g.b_cs = 1;
-      g.C = Dc.p; g.c_rs = l; g.c_cs = 1;
-      gemm(g, c.st);
-      g.B = Bgc.p;
-      g.C = Dgc.p;
+      g.A = Bc; g.a_rs = 1; g.a_cs = lw; g.a_bs = 0;
+      g.B = Bc; g.b_rs = lw; g.b_cs = 1; g.b_bs = l;
+      g.C = DD.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
       gemm(g, c.st);
     }
     // l x l step (:187-218)
     CK(cudaMemsetAsync(rt.ctl, 0, 8, c.st));
     KnStep s;
-    s.l = l; s.Dc = Dc.p; s.Dgc = Dgc.p; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = err.p;
+    s.l = l; s.Dc = DD.p; s.Dgc = DD.p + ll; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = err.p;
     s.work = work.p; s.status = c.status; s.bar = rt.ctl;
     s.ns_target = (c.precision == kMixed) ? 1e-12 : 1e-18;  // MIXED carries FP32-level errors anyway
+    s.fstack = Fs.p; s.fstack_scale = invN;
     kn_step(s, c.st);
-    {  // M+ = Mc F + (Bc / N) C^-1 ;  B+ = Bc F + Bgc C^-1   (:221-226)
-      Gemm<double, double> g = gm<double>(Nl, l, l);
-      g.A = Mc; g.a_rs = l; g.a_cs = 1;
-      g.B = F.p; g.b_rs = l; g.b_cs = 1;
-      g.C = Mp; g.c_rs = l; g.c_cs = 1;
-      gemm(g, c.st);
-      g.A = Bc; g.B = Ci.p; g.alpha = invN; g.beta = 1.0;
-      gemm(g, c.st);
-      g.A = Bc; g.B = F.p; g.C = Bp; g.alpha = 1.0; g.beta = 0.0;
-      gemm(g, c.st);
-      g.A = Bgc.p; g.B = Ci.p; g.beta = 1.0;
+    {  // [M+ | B+] = [Mc Bc] [F; C^-1 / N] , [Bc Bgc] [F; C^-1]   (:221-226), one batched product
+      Gemm<double, double> g = gm<double>(Nl, l, 2 * l);
+      g.batch = 2;
+      g.A = Wc; g.a_rs = lw; g.a_cs = 1; g.a_bs = l;
+      g.B = Fs.p; g.b_rs = l; g.b_cs = 1; g.b_bs = 2 * (long long)ll;
+      g.C = Wp; g.c_rs = lw; g.c_cs = 1; g.c_bs = l;
       gemm(g, c.st);
     }
     CK(cudaMemcpyAsync(&herr, err.p, sizeof(double), cudaMemcpyDeviceToHost, c.st));
     read_status(c, "Kolmogorov-Nagumo integration");
     if (herr <= tol) break;                                    // (:235-237)
     if (iter == cap) { ++iter; break; }                        // (:238-241)
-    std::swap(Bc, Bp);
-    std::swap(Mc, Mp);
+    std::swap(Wc, Wp);
   }
   res.iterations = iter;
   res.error = herr;
   // Qbar = Qs M+  (:251)
   if (c.precision == kMixed) {
-    mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mp, qt, ldqt);
+    DBuf<double> Mt(nl);
+    copy2d<double, double>(Wp, lw, 1, Mt.p, l, 1, Nl, l, c.st);
+    mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mt.p, qt, ldqt);
   } else {
     DBuf<T> Mt(nl);
-    copy2d<double, T>(Mp, l, 1, Mt.p, l, 1, Nl, l, c.st);
+    copy2d<double, T>(Wp, lw, 1, Mt.p, l, 1, Nl, l, c.st);
     Gemm<T, T> g = gm<T>(m, l, Nl);
     g.A = qs; g.a_rs = ldq; g.a_cs = 1;
     g.B = Mt.p; g.b_rs = l; g.b_cs = 1;
