@@ -482,8 +482,13 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   done();
   // ---- orthogonalize
   progress("Orthogonalizing ............... ");
-  if (bo == "TS") orth_tsqr_dev<T>(c.sc, m, l, N, Y.p, Nl);
-  else orth_gramian_dev<T>(c.sc, m, l, N, Y.p, Nl);
+  if (bo == "TS") {
+    orth_tsqr_dev<T>(c.sc, m, l, N, Y.p, Nl);
+  } else {
+    // KN and WY form G = Qs' Qs anyway: they take over the second pass in the coordinates of G
+    c.sc.deferred_orth = (bi == "KN" || bi == "WY");
+    orth_gramian_dev<T>(c.sc, m, l, N, Y.p, Nl);
+  }
   tm.mark(2, st);
   sync();
   done();

@@ -177,6 +177,16 @@ __global__ void lincomb_kernel(double *out, const double *x, double a, const dou
   }
 }
 
+__global__ void copy_diag_blocks_kernel(const double *__restrict__ G, int Nl, int l, int N, double *__restrict__ out) {
+  const long long total = (long long)N * l * l;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long b = e / ((long long)l * l), r = e - b * l * l;
+    const long long i = r / l, j = r - i * l;
+    out[e] = G[(b * l + i) * Nl + b * l + j];
+  }
+}
+
 // d_i = num / (half * max(lambda_i, 0) + add)
 __global__ void recip_affine_kernel(const double *__restrict__ lam, int n, double num, double half, double add,
                                     double *__restrict__ d) {
@@ -221,6 +231,14 @@ void lincomb(double *out, const double *x, double a, const double *y, double b, 
   const long long total = rows * cols;
   const int grid = (int)std::min<long long>((total + 255) / 256, 8LL * Runtime::get().num_sms);
   lincomb_kernel<<<grid, 256, 0, st>>>(out, x, a, y, b, c, rows, cols);
+  KLAUNCHED();
+}
+
+void copy_diag_blocks(const double *G, int Nl, int l, int N, double *out, cudaStream_t st) {
+  const long long total = (long long)N * l * l;
+  if (total <= 0) return;
+  const int grid = (int)std::min<long long>((total + 255) / 256, 8LL * Runtime::get().num_sms);
+  copy_diag_blocks_kernel<<<grid, 256, 0, st>>>(G, Nl, l, N, out);
   KLAUNCHED();
 }
 

@@ -512,232 +512,6 @@ __global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
   }
 }
 
-// ------------------------------------------------------------------------------------------
-// Kolmogorov-Nagumo step by power series.
-//
-// With g(z) = 1/2 + (1/4 - z)^(1/2) = 1 - sum_{n>=1} Cat(n-1) z^n (Cat: Catalan numbers), the step
-// needs C = g(Z)^(1/2) and C^-1 = g(Z)^(-1/2).  Both are power series in Z with radius of
-// convergence 1/4 (coefficients from Miller's recurrence for powers of a series).  When
-// rho >= ||4 Z||_2 is small, as in all but the first Kolmogorov-Nagumo iterations, a truncated
-// series of degree d evaluated by the Paterson-Stockmeyer scheme (powers Z^2..Z^s by doubling, then
-// Horner in Z^s) needs ceil(log2 s) + d / s dependent products, against about 2 x 2 x 5 for the
-// two coupled Newton-Schulz square roots; the degree is the smallest whose tail bound
-// sum_{n>d} max(|c_n|, |d_n|) (rho / 4)^n is below the target.  When no degree up to the table
-// size reaches the target (rho close to 1), the step falls back to the Newton-Schulz iteration.
-
-__global__ void __launch_bounds__(kKnThreads) kn_series_kernel(KnStep a, KnSeries ser) {
-  const int l = a.l;
-  const size_t ll = (size_t)l * l;
-  // work: Z | P_1..P_8 | accC x2 | accCi x2 | BC_0..BC_7 | BI_0..BI_7 ; the Newton-Schulz fallback
-  // uses P_1..P_5
-  double *Zm = a.work, *P = Zm + ll, *AC = P + 8 * ll, *AI = AC + 2 * ll, *BC = AI + 2 * ll, *BI = BC + 8 * ll;
-  double *scal = a.work + (size_t)kKnWorkMatrices * ll;  // [0] method (degree, or -1: Newton-Schulz), [1] s, [2] k
-  const int nr = (l + 15) / 16, nt = nr * nr;
-  __shared__ double red[kKnThreads];
-
-  mm_tiles(l, nr, 0, nt, -1.0, a.Dc, a.Dc, 1.0, a.Dgc, 0.0, Zm);  // Z = Dgc - Dc Dc (:184-190)
-  if (!grid_barrier(a.bar, a.status)) return;
-  // P_1 = Zsym from the upper triangle (as syev 'U' reads Z)
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e / l), j = (int)(e % l);
-    P[e] = __ldcg(Zm + (size_t)min(i, j) * l + max(i, j));
-  }
-  if (blockIdx.x == 0) {
-    double f = 0.0;
-    for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
-      const int i = (int)(e / l), j = (int)(e % l);
-      const double z = __ldcg(Zm + (size_t)min(i, j) * l + max(i, j));
-      f += 16.0 * z * z;
-    }
-    red[threadIdx.x] = f;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-      if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-      __syncthreads();
-    }
-    const double fro = sqrt(red[0]);
-    __syncthreads();
-    double rmax = 0.0;
-    for (int i = threadIdx.x; i < l; i += blockDim.x) {
-      double rs = 0.0;
-      for (int j = 0; j < l; ++j) rs += fabs(4.0 * __ldcg(Zm + (size_t)min(i, j) * l + max(i, j)));
-      rmax = fmax(rmax, rs);
-    }
-    red[threadIdx.x] = rmax;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-      if (threadIdx.x < h) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + h]);
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      const double rho = fmin(fro, red[0]);
-      // smallest degree whose tail bound is below the target
-      int deg = -1;
-      if (rho < 0.9) {
-        const double x = 0.25 * rho;
-        double tail = 0.0, xn = 1.0;
-        double term[kSeriesLen];
-        for (int n = 0; n < kSeriesLen; ++n) {
-          term[n] = fmax(fabs(ser.c[n]), fabs(ser.d[n])) * xn;
-          xn *= x;
-        }
-        // remainder beyond the table: terms shrink at least by 4x / (1 - ...) ~ rho per degree
-        tail = term[kSeriesLen - 1] * rho / (1.0 - rho);
-        for (int n = kSeriesLen - 1; n >= 1; --n) {
-          if (tail > a.ns_target) break;
-          deg = n - 1;
-          tail += term[n];
-        }
-        if (tail <= a.ns_target) deg = 0;
-      }
-      int sb = 1;
-      if (deg >= 1) {  // block size: fewest dependent products, then the smallest
-        int best = 1 << 30;
-        for (int cand = 1; cand <= 8; ++cand) {
-          int lg = 0;
-          while ((1 << lg) < cand) ++lg;
-          const int cost = lg + deg / cand;
-          if (cost < best) { best = cost; sb = cand; }
-        }
-      }
-      scal[0] = (double)deg;
-      scal[1] = (double)sb;
-      scal[2] = (double)kn_ns_steps(rho, a.ns_target);
-    }
-  }
-  if (!grid_barrier(a.bar, a.status)) return;
-  const int deg = (int)__ldcg(scal);
-  const double *C = nullptr, *Ci = nullptr;
-  if (deg >= 0) {
-    const int sb = (int)__ldcg(scal + 1);
-    // powers P_2..P_sb by doubling: P_j = P_h P_(j-h), h the largest power of two below j
-    for (int h = 1; h < sb; h *= 2) {
-      const int hi = min(2 * h, sb);
-      for (int j = h + 1; j <= hi; ++j) {
-        const int slot = j - h - 1;  // distinct tile range per product of this phase
-        mm_tiles(l, nr, slot * nt, (slot + 1) * nt, 1.0, P + (h - 1) * ll, P + (j - h - 1) * ll, 0.0, nullptr, 0.0,
-                 P + (j - 1) * ll);
-      }
-      if (!grid_barrier(a.bar, a.status)) return;
-    }
-    // Paterson-Stockmeyer: B_i = sum_{t<sb} coef[i sb + t] Z^t (i = 0..q), then Horner in Z^sb:
-    // acc = B_q;  acc = acc Z^sb + B_i  (i = q-1 .. 0)
-    const int q = deg / sb;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-      const int i = (int)(e / l), j = (int)(e % l);
-      for (int b = 0; b <= q; ++b) {
-        double vc = (i == j) ? ser.c[b * sb] : 0.0, vd = (i == j) ? ser.d[b * sb] : 0.0;
-        for (int t = 1; t < sb && b * sb + t <= deg; ++t) {
-          const double p = __ldcg(P + (t - 1) * ll + e);
-          vc += ser.c[b * sb + t] * p;
-          vd += ser.d[b * sb + t] * p;
-        }
-        BC[b * ll + e] = vc;
-        BI[b * ll + e] = vd;
-      }
-    }
-    if (!grid_barrier(a.bar, a.status)) return;
-    const double *accC = BC + q * ll, *accI = BI + q * ll;
-    int cur = 0;
-    for (int i = q - 1; i >= 0; --i) {
-      mm_tiles(l, nr, 0, nt, 1.0, accC, P + (sb - 1) * ll, 1.0, BC + i * ll, 0.0, AC + cur * ll);
-      mm_tiles(l, nr, nt, 2 * nt, 1.0, accI, P + (sb - 1) * ll, 1.0, BI + i * ll, 0.0, AI + cur * ll);
-      if (!grid_barrier(a.bar, a.status)) return;
-      accC = AC + cur * ll;
-      accI = AI + cur * ll;
-      cur = 1 - cur;
-    }
-    C = accC;
-    Ci = accI;
-  } else {
-    // Newton-Schulz fallback (as kn_step_kernel): X = I - 4 Zsym; two coupled square roots
-    double *Y0 = P, *Y1 = P + ll, *Q0 = P + 2 * ll, *Q1 = P + 3 * ll, *T = P + 4 * ll;
-    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-      const int i = (int)(e / l), j = (int)(e % l);
-      Y0[e] = (i == j ? 1.0 : 0.0) - 4.0 * __ldcg(P + e);  // Y0 is P_1: each entry read, then written
-      Q0[e] = (i == j ? 1.0 : 0.0);
-    }
-    if (!grid_barrier(a.bar, a.status)) return;
-    double *Y = Y0, *Yn = Y1, *Q = Q0, *Qn = Q1;
-    for (int stage = 0; stage < 2; ++stage) {
-      const int k = (int)__ldcg(scal + 2);
-      for (int it = 0; it < k; ++it) {
-        mm_tiles(l, nr, 0, nt, 1.0, Q, Y, 0.0, nullptr, 0.0, T);
-        if (!grid_barrier(a.bar, a.status)) return;
-        mm_tiles(l, nr, 0, nt, -0.5, Y, T, 1.5, Y, 0.0, Yn);
-        mm_tiles(l, nr, nt, 2 * nt, -0.5, T, Q, 1.5, Q, 0.0, Qn);
-        if (!grid_barrier(a.bar, a.status)) return;
-        double *t1 = Y; Y = Yn; Yn = t1;
-        double *t2 = Q; Q = Qn; Qn = t2;
-      }
-      if (stage == 0) {
-        for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-          const int i = (int)(e / l), j = (int)(e % l);
-          T[e] = 0.5 * __ldcg(Y + e) + (i == j ? 0.5 : 0.0);
-        }
-        if (!grid_barrier(a.bar, a.status)) return;
-        for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-          const int i = (int)(e / l), j = (int)(e % l);
-          Y[e] = __ldcg(T + e);
-          Q[e] = (i == j ? 1.0 : 0.0);
-        }
-        if (blockIdx.x == 0) {
-          double f = 0.0;
-          for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
-            const int i = (int)(e / l), j = (int)(e % l);
-            const double d = (i == j ? 1.0 : 0.0) - __ldcg(T + e);
-            f += d * d;
-          }
-          red[threadIdx.x] = f;
-          __syncthreads();
-          for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-            if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-            __syncthreads();
-          }
-          if (threadIdx.x == 0) scal[2] = (double)kn_ns_steps(fmin(sqrt(red[0]), 0.5), a.ns_target);
-        }
-        if (!grid_barrier(a.bar, a.status)) return;
-      }
-    }
-    C = Y;
-    Ci = Q;
-  }
-  // F = C - Dc Cinv (:218); err = ||C - I||_F (:230-234)
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ll; e += (size_t)gridDim.x * blockDim.x) {
-    const double ci = __ldcg(Ci + e);
-    a.C[e] = __ldcg(C + e);
-    a.Cinv[e] = ci;
-    if (a.fstack) {
-      a.fstack[ll + e] = a.fstack_scale * ci;
-      a.fstack[3 * ll + e] = ci;
-    }
-  }
-  mm_tiles(l, nr, 0, nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.F);
-  if (a.fstack) {
-    mm_tiles(l, nr, nt, 2 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack);
-    mm_tiles(l, nr, 2 * nt, 3 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack + 2 * ll);
-  }
-  if (blockIdx.x == 0) {
-    double f = 0.0;
-    for (size_t e = threadIdx.x; e < ll; e += blockDim.x) {
-      const int i = (int)(e / l), j = (int)(e % l);
-      const double d = __ldcg(C + e) - (i == j ? 1.0 : 0.0);
-      f += d * d;
-    }
-    red[threadIdx.x] = f;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-      if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      const double err = sqrt(red[0]);
-      *a.err = err;
-      if (!(err == err)) atomicExch(a.status, kErrNumerical);
-    }
-  }
-}
-
 size_t eig_smem(int n, bool vs) {
   const int ne = n + (n & 1), np = ne / 2;
   const size_t npk = ((size_t)n * (n + 1) / 2 + 1) & ~(size_t)1;
@@ -774,47 +548,6 @@ void svd_jacobi_batched(int n, int batch, const double *B, double *U, double *s,
   if (smem > rt.smem_optin) fail(kErrUnsupported, "Jacobi SVD: l = %d exceeds on-chip capacity", n);
   CK(cudaFuncSetAttribute(svd_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   svd_jacobi_kernel<<<batch, kEigThreads, smem, st>>>(n, B, U, s, V, status);
-  KLAUNCHED();
-}
-
-// Coefficients of g(z)^(1/2) and g(z)^(-1/2), g(z) = 1 - sum_{n>=1} Cat(n-1) z^n: for h = f^alpha
-// with f_0 = 1, h_0 = 1 and h_n = (1/n) sum_{k=1..n} (alpha k - (n - k)) f_k h_(n-k) (J. C. P. Miller).
-static KnSeries make_series() {
-  KnSeries s;
-  double f[kSeriesLen], cat = 1.0;  // Cat(0) = 1, Cat(n) = Cat(n-1) 2 (2n - 1) / (n + 1)
-  f[0] = 1.0;
-  for (int n = 1; n < kSeriesLen; ++n) {
-    f[n] = -cat;
-    cat = cat * 2.0 * (2.0 * n - 1.0) / (n + 1.0);
-  }
-  const double alpha[2] = {0.5, -0.5};
-  double *out[2] = {s.c, s.d};
-  for (int w = 0; w < 2; ++w) {
-    double *h = out[w];
-    h[0] = 1.0;
-    for (int n = 1; n < kSeriesLen; ++n) {
-      double acc = 0.0;
-      for (int k = 1; k <= n; ++k) acc += (alpha[w] * k - (n - k)) * f[k] * h[n - k];
-      h[n] = acc / n;
-    }
-  }
-  return s;
-}
-
-void kn_step(const KnStep &a, cudaStream_t st) {
-  Runtime &rt = Runtime::get();
-  if (a.l > 160) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > 160", a.l);
-  static const KnSeries series = make_series();
-  const int nr = (a.l + 15) / 16;
-  int blocks = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kn_series_kernel, kKnThreads, 0));
-  // two CTAs per tile of one product: phases with more products take several tiles per CTA
-  int grid = std::min(2 * nr * nr, blocks * rt.num_sms);
-  grid = std::max(1, std::min(grid, rt.num_sms));
-  KnStep arg = a;
-  KnSeries ser = series;
-  void *args[] = {&arg, &ser};
-  CK(cudaLaunchCooperativeKernel((void *)kn_series_kernel, dim3(grid), dim3(kKnThreads), args, 0, st));
   KLAUNCHED();
 }
 

@@ -129,6 +129,8 @@ void dots(const DotJobs &jobs, double *out, cudaStream_t st);  // out[k] = value
 // out = a x + b y + c I  (rows x cols, contiguous; x or y may be null)
 void lincomb(double *out, const double *x, double a, const double *y, double b, double c, long long rows,
              long long cols, cudaStream_t st);
+// out[b] = the b-th l x l diagonal block of G (Nl x Nl row-major), b < N
+void copy_diag_blocks(const double *G, int Nl, int l, int N, double *out, cudaStream_t st);
 // d_i = num / (half max(lambda_i, 0) + add)
 void recip_affine(const double *lam, int n, double num, double half, double add, double *d, cudaStream_t st);
 

@@ -127,11 +127,47 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
 template <class T>
 void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy) {
   gramian_pass<T>(c, m, l, N, y, ldy, false);
-  if (c.precision == kMixed) gramian_pass<T>(c, m, l, N, y, ldy, true);
+  if (c.precision == kMixed && !c.deferred_orth) gramian_pass<T>(c, m, l, N, y, ldy, true);
   read_status(c, "Gramian orthogonalization");
 }
 
 // ------------------------------------------------------------------------------- integrate
+
+void coeff_orthonormalize(const StageCtx &c, int Nl, int l, int N, double *G, double *X) {
+  const size_t ll = (size_t)l * l;
+  DBuf<double> D(N * ll), G1((size_t)Nl * Nl);
+  copy_diag_blocks(G, Nl, l, N, D.p, c.st);
+  chol_inv_batched(l, N, D.p, 1.0, 0.0, 0.0, l * 0x1p-24, X, 1.0, kCholFactor, c.status, c.st);
+  {  // G1 = G diag(X_j)
+    Gemm<double, double> g = gm<double>(Nl, l, l);
+    g.batch = N;
+    g.A = G; g.a_rs = Nl; g.a_cs = 1; g.a_bs = l;
+    g.B = X; g.b_rs = l; g.b_cs = 1; g.b_bs = (long long)ll;
+    g.C = G1.p; g.c_rs = Nl; g.c_cs = 1; g.c_bs = l;
+    gemm(g, c.st);
+  }
+  {  // G = diag(X_i)' G1
+    Gemm<double, double> g = gm<double>(l, Nl, l);
+    g.batch = N;
+    g.A = X; g.a_rs = 1; g.a_cs = l; g.a_bs = (long long)ll;
+    g.B = G1.p; g.b_rs = Nl; g.b_cs = 1; g.b_bs = (long long)l * Nl;
+    g.C = G; g.c_rs = Nl; g.c_cs = 1; g.c_bs = (long long)l * Nl;
+    gemm(g, c.st);
+  }
+}
+
+void coeff_unorthonormalize(const StageCtx &c, int Nl, int l, int N, const double *X, const double *M, long long ldm,
+                            double *out) {
+  const size_t ll = (size_t)l * l;
+  Gemm<double, double> g = gm<double>(l, l, l);
+  g.batch = N;
+  g.A = X; g.a_rs = l; g.a_cs = 1; g.a_bs = (long long)ll;
+  g.B = M; g.b_rs = ldm; g.b_cs = 1; g.b_bs = (long long)l * ldm;
+  g.C = out; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
+  gemm(g, c.st);
+  (void)Nl;
+}
+
 //
 // Kolmogorov-Nagumo (reference @x@_integrate_kolmogorov_nagumo.c:153-266), carried in the
 // coordinates of Qs: with G = Qs' Qs (Nl x Nl), every m x l iterate is Qs * M for an Nl x l
@@ -157,6 +193,12 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.B = qs; g.b_rs = ldq; g.b_cs = 1;
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, c.st);
+  }
+  DBuf<double> Xo;  // deferred second orthogonalization pass, applied in the coordinates of G
+  const bool defer = (c.precision == kMixed && c.deferred_orth);
+  if (defer) {
+    Xo.alloc((size_t)N * ll);
+    coeff_orthonormalize(c, Nl, l, N, G.p, Xo.p);
   }
   // iterates W = [M | B | Bgc] (Nl x 3l, current and next), [Dc; Dgc], step outputs
   DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64), err(1);
@@ -219,7 +261,8 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   // Qbar = Qs M+  (:251)
   if (c.precision == kMixed) {
     DBuf<double> Mt(nl);
-    copy2d<double, double>(Wp, lw, 1, Mt.p, l, 1, Nl, l, c.st);
+    if (defer) coeff_unorthonormalize(c, Nl, l, N, Xo.p, Wp, lw, Mt.p);
+    else copy2d<double, double>(Wp, lw, 1, Mt.p, l, 1, Nl, l, c.st);
     mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mt.p, qt, ldqt);
   } else {
     DBuf<T> Mt(nl);

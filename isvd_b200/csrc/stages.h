@@ -15,6 +15,9 @@ struct StageCtx {
   int precision;   // kNative / kMixed
   int *status;     // device status word (zeroed by the caller)
   MixedCache *cache = nullptr;
+  // MIXED driver: the second (polar) pass of the Gramian orthogonalization is left to the
+  // integration, which re-orthonormalizes the blocks in the coordinates of G (coeff_orthonormalize)
+  bool deferred_orth = false;
 };
 
 struct IterResult {
@@ -59,6 +62,15 @@ template <class T>
 void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt);
 
 // Postprocessing.  s has l entries; ut (m x k, ldut), vt (n x k or n x l for TS, ldvt) when wanted.
+// MIXED driver, after a Gramian orthogonalization without its second pass: with R_i' R_i = G_ii
+// (Cholesky) and X = diag(R_i^-1), the blocks of Qs X are orthonormal with respect to G to FP64
+// rounding.  G (Nl x Nl, row-major) becomes X' G X in place; X (N blocks of l x l) is returned, and
+// a coefficient matrix M of Qs X is M' = X M for Qs (coeff_unorthonormalize).
+void coeff_orthonormalize(const StageCtx &c, int Nl, int l, int N, double *G, double *X);
+// out (Nl x l, ld l) = diag(X_i) M  for M with row stride ldm
+void coeff_unorthonormalize(const StageCtx &c, int Nl, int l, int N, const double *X, const double *M, long long ldm,
+                            double *out);
+
 // Z = A' Qbar (n x l, row-major, ld l) for A m x n stored per ordera.
 template <class T>
 void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,

@@ -142,6 +142,12 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, st);
   }
+  DBuf<double> Xo;  // deferred second orthogonalization pass, applied in the coordinates of G
+  const bool defer = (mixed && c.deferred_orth);
+  if (defer) {
+    Xo.alloc((size_t)N * ll);
+    coeff_orthonormalize(c, Nl, l, N, G.p, Xo.p);
+  }
   // out = G B / N in FP64 in both precision modes.  The iteration carries B by the recursion
   // B+ = Bc Fc + Bgc Fgc and never re-orthonormalizes, so the products must agree with one fixed G
   // to FP64 rounding: BF16x3 products (independent errors of ~1e-7 in every call) make Q drift off
@@ -258,7 +264,13 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   res.error = mu;
   // Qbar = Qs Mp
   if (mixed) {
-    mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mp, qt, ldqt);
+    if (defer) {
+      DBuf<double> Mt(nl);
+      coeff_unorthonormalize(c, Nl, l, N, Xo.p, Mp, l, Mt.p);
+      mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mt.p, qt, ldqt);
+    } else {
+      mixed_apply_coeff<T>(c, qp.P, m, Nl, l, qs, ldq, Mp, qt, ldqt);
+    }
   } else {
     DBuf<T> Mt(nl);
     copy2d<double, T>(Mp, l, 1, Mt.p, l, 1, Nl, l, st);
