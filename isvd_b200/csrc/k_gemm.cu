@@ -135,9 +135,16 @@ __global__ void splitk_reduce_kernel(const Gemm<T, Tout> g, const int splits, co
     const int b = (int)(e / MN);
     const long long r = e - (long long)b * MN;
     const int gm = (int)(r / g.N), gn = (int)(r - (long long)gm * g.N);
-    double s = 0.0;
     const T *p = partial + ((long long)b * splits) * MN + r;
-    for (int sp = 0; sp < splits; ++sp) s += (double)p[(long long)sp * MN];
+    // eight independent partial sums, so that eight loads are in flight
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int sp = 0;
+    for (; sp + 8 <= splits; sp += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += (double)p[(long long)(sp + u) * MN];
+    }
+    for (int u = 0; sp < splits; ++sp, ++u) acc[u] += (double)p[(long long)sp * MN];
+    const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     Tout *c = g.C + (long long)b * g.c_bs + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
     double v = g.alpha * s;
     if (g.beta != 0.0) v += g.beta * (double)(*c);

@@ -326,8 +326,17 @@ __global__ void umma_reduce_kernel(const KParams p) {
        e += (long long)gridDim.x * blockDim.x) {
     const long long b = e / MN, r = (e % MN) / p.N, c = e % p.N;
     if (p.upper && c < r) continue;
-    double s = 0.0;
-    for (int sp = 0; sp < p.splits; ++sp) s += (double)p.partial[((b * p.splits + sp) * p.M + r) * p.N + c];
+    // eight independent partial sums, so that eight loads are in flight
+    const float *q = p.partial + ((b * p.splits) * p.M + r) * p.N + c;
+    const long long stride = (long long)p.M * p.N;
+    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int sp = 0;
+    for (; sp + 8 <= p.splits; sp += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += (double)q[(sp + u) * stride];
+    }
+    for (int u = 0; sp < p.splits; ++sp, ++u) acc[u] += (double)q[sp * stride];
+    const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
     const long long off = b * p.c_step + r * p.c_rs + c * p.c_cs;
     if (p.c_double) ((double *)p.C)[off] = p.alpha * s;
     else ((float *)p.C)[off] = (float)(p.alpha * s);
