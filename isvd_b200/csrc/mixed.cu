@@ -19,7 +19,7 @@ void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, lon
                  cudaStream_t st) {
   const long long orows = transpose ? cols : rows, ocols = transpose ? rows : cols;
   const long long ld = plane_ld(ocols), rp = plane_rows(orows), ps = rp * ld;
-  pb.buf.alloc((size_t)np * ps);
+  pb.buf.ensure((size_t)np * ps);
   split_planes<T>(src, s_rs, 1, rows, cols, np, transpose, pb.buf.p, ld, ps, st);
   pb.P.ptr = pb.buf.p;
   pb.P.np = np;

@@ -8,6 +8,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace isvdb {
 
@@ -122,6 +123,33 @@ static bool g_profiling = false;
 
 bool profiling() { return g_profiling; }
 void set_profiling(bool on) { g_profiling = on; }
+
+unsigned long long count_kernel_nodes(cudaGraph_t g) {
+  size_t n = 0;
+  CK(cudaGraphGetNodes(g, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (n) CK(cudaGraphGetNodes(g, nodes.data(), &n));
+  unsigned long long k = 0;
+  for (size_t i = 0; i < n; ++i) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nodes[i], &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+GraphPair::GraphPair(cudaStream_t s) : st(s) {
+  const char *env = getenv("ISVD_GPU_GRAPHS");
+  const bool off = env && env[0] == '0';
+  // stream-ordered allocations inside the body go to the library stream: only that one is captured
+  usable = !off && s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread && !profiling() &&
+           s == Runtime::get().stream;
+}
+
+GraphPair::~GraphPair() {
+  for (int i = 0; i < 2; ++i)
+    if (exec[i]) cudaGraphExecDestroy(exec[i]);
+}
 void profile_add(const char *tag, double ms, double flops) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   ProfEntry &e = g_prof[tag];

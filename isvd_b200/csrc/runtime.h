@@ -76,6 +76,9 @@ struct DBuf {
   }
   ~DBuf() { release(); }
   void alloc(size_t count);
+  void ensure(size_t count) {  // keep the buffer when it already holds count elements
+    if (!p || n != count) alloc(count);
+  }
   void release();
   T *get() const { return p; }
   operator T *() const { return p; }
@@ -105,6 +108,44 @@ void sync();  // synchronise the library stream, converting errors into Error
 // Optional per-kernel timing (CUDA events on the launching stream), off by default.
 bool profiling();
 void set_profiling(bool on);
+
+unsigned long long count_kernel_nodes(cudaGraph_t g);
+
+// Two CUDA graphs for the two parities of a ping-pong loop body: captured from the body's
+// enqueues on first use and replayed afterwards.  Not used (the caller runs the body eagerly) on
+// the legacy default stream, while kernel timing is on, or with ISVD_GPU_GRAPHS=0.
+struct GraphPair {
+  cudaStream_t st;
+  bool usable;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  unsigned long long kernels[2] = {0, 0};  // kernel nodes per graph (added to the launch counter)
+  explicit GraphPair(cudaStream_t s);
+  ~GraphPair();
+  GraphPair(const GraphPair &) = delete;
+  GraphPair &operator=(const GraphPair &) = delete;
+  template <class F>
+  void run(int par, F &&body) {
+    if (!exec[par]) {
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        body();
+      } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(st, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamEndCapture(st, &g));
+      kernels[par] = count_kernel_nodes(g);
+      const cudaError_t e = cudaGraphInstantiate(&exec[par], g, 0);
+      cudaGraphDestroy(g);
+      CK(e);
+    }
+    CK(cudaGraphLaunch(exec[par], st));
+    g_launches.fetch_add(kernels[par]);
+  }
+};
 void profile_add(const char *tag, double ms, double flops);
 bool profile_get(const char *tag, double *ms, unsigned long long *count, double *flops);
 void profile_reset();

@@ -209,12 +209,11 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   const double invN = 1.0 / N;
   MixedGProduct gprod;  // MIXED: G's bf16 planes, reused by every iteration
   if (c.precision == kMixed) gprod.prepare(c, Nl, G.p);
-  IterResult res;
-  double herr = 0.0;
-  const int cap = maxit > 0 ? maxit : 1000000;
-  int iter = 1;
-  for (;; ++iter) {
-    double *Bc = Wc + l, *Bgc = Wc + 2 * l;
+  // One iteration: W(next) from W(cur).  After two eager iterations (which size every buffer and
+  // set every kernel attribute) the iteration is captured as one CUDA graph per parity of the
+  // ping-pong buffers, so that an iteration costs one graph launch plus the host read of err.
+  auto iteration = [&](double *Wcur, double *Wnext) {
+    double *Bc = Wcur + l, *Bgc = Wcur + 2 * l;
     if (c.precision == kMixed) {  // Bgc = G Bc / N   (:174-177)
       gprod.apply(c, l, Bc, lw, invN, Bgc, lw);
     } else {
@@ -245,11 +244,21 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     {  // [M+ | B+] = [Mc Bc] [F; C^-1 / N] , [Bc Bgc] [F; C^-1]   (:221-226), one batched product
       Gemm<double, double> g = gm<double>(Nl, l, 2 * l);
       g.batch = 2;
-      g.A = Wc; g.a_rs = lw; g.a_cs = 1; g.a_bs = l;
+      g.A = Wcur; g.a_rs = lw; g.a_cs = 1; g.a_bs = l;
       g.B = Fs.p; g.b_rs = l; g.b_cs = 1; g.b_bs = 2 * (long long)ll;
-      g.C = Wp; g.c_rs = lw; g.c_cs = 1; g.c_bs = l;
+      g.C = Wnext; g.c_rs = lw; g.c_cs = 1; g.c_bs = l;
       gemm(g, c.st);
     }
+  };
+  GraphPair graphs(c.st);
+  IterResult res;
+  double herr = 0.0;
+  const int cap = maxit > 0 ? maxit : 1000000;
+  int iter = 1;
+  for (;; ++iter) {
+    const int par = iter & 1;
+    if (graphs.usable && iter > 2) graphs.run(par, [&] { iteration(Wc, Wp); });
+    else iteration(Wc, Wp);
     CK(cudaMemcpyAsync(&herr, err.p, sizeof(double), cudaMemcpyDeviceToHost, c.st));
     read_status(c, "Kolmogorov-Nagumo integration");
     if (herr <= tol) break;                                    // (:235-237)
