@@ -98,6 +98,37 @@ void isvd_gpu_profile_enable( int on );
 void isvd_gpu_profile_reset( void );
 int  isvd_gpu_profile_get( const char *tag, double *ms, unsigned long long *launches, double *flops );
 
+/* ---------------------------------------------------------------- truncated-SVD adjoint
+ * Gradient of a scalar loss L(U, s, V) with respect to A, where A ~ U diag(s) V' are the k leading
+ * singular triplets of A (m x n; s descending, distinct, and s_k > s_(k+1)).  No counterpart in the
+ * reference.  Inputs: A stored per ordera ('R' / 'C', leading dimension lda); s (k); U as ut and V
+ * as vt, row-major m x k and n x k (the layout of isvd_?Isvd's ut / vt outputs, leading dimensions
+ * >= k); the cotangents ds = dL/ds (k), dut = dL/dU (m x k), dvt = dL/dV (n x k), each may be NULL
+ * (zero).  Output: da = dL/dA (m x n, stored per ordera, leading dimension ldda).
+ *   dA = U J V' + Lam S V' + U Lam' Aperp + U S Gam' + Aperp Gam V',   Aperp = (I - UU') A (I - VV'),
+ *   J = diag(ds) + (F o (U'dU - dU'U)) S + S (F o (V'dV - dV'V)),  F_ij = 1 / (s_j^2 - s_i^2),
+ *   Lam S^2 - Aperp Aperp' Lam = (I - UU') dU,   Gam S^2 - Aperp' Aperp Gam = (I - VV') dV,
+ * the last two solved column by column by conjugate gradients (at most cg_iters iterations each,
+ * relative residual tol); cg_iters = 0 uses Lam = (I - UU') dU S^-2 (exact when rank(A) = k).
+ * *iterations (may be NULL) receives the CG iterations used.  Buffers may be host or device memory.
+ * Returns an ISVD_GPU_* status. */
+int isvd_sSvdAdjoint(
+    const isvd_int_t m, const isvd_int_t n, const isvd_int_t k, const char ordera,
+    const isvd_s_val_t *a, const isvd_int_t lda, const isvd_s_val_t *s,
+    const isvd_s_val_t *ut, const isvd_int_t ldut, const isvd_s_val_t *vt, const isvd_int_t ldvt,
+    const isvd_s_val_t *ds, const isvd_s_val_t *dut, const isvd_int_t lddut,
+    const isvd_s_val_t *dvt, const isvd_int_t lddvt, isvd_s_val_t *da, const isvd_int_t ldda,
+    const int cg_iters, const double tol, int *iterations
+);
+int isvd_dSvdAdjoint(
+    const isvd_int_t m, const isvd_int_t n, const isvd_int_t k, const char ordera,
+    const isvd_d_val_t *a, const isvd_int_t lda, const isvd_d_val_t *s,
+    const isvd_d_val_t *ut, const isvd_int_t ldut, const isvd_d_val_t *vt, const isvd_int_t ldvt,
+    const isvd_d_val_t *ds, const isvd_d_val_t *dut, const isvd_int_t lddut,
+    const isvd_d_val_t *dvt, const isvd_int_t lddvt, isvd_d_val_t *da, const isvd_int_t ldda,
+    const int cg_iters, const double tol, int *iterations
+);
+
 /* ---------------------------------------------------------------- no device allocation
  * Kolmogorov-Nagumo integration in FP64 that allocates no device memory: no cudaMalloc or
  * cudaFree, no stream-ordered pool, no allocating library routine.  It has no counterpart in the

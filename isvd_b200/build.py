@@ -20,7 +20,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libisvd_gpu_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-Xcompiler", "-fvisibility=hidden",
+FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-Xcompiler", "-fvisibility=hidden,-fvisibility-inlines-hidden",
                 "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include"),
                 "-I" + os.path.join(REPO, "include", "mpi_shim"), "-I" + CSRC]
 
@@ -33,6 +33,11 @@ def _newest_header():
 
 def build(force=False, verbose=False, extra=()):
     os.makedirs(OBJ, exist_ok=True)
+    # a change of compiler flags rebuilds everything
+    stamp = os.path.join(OBJ, "flags.txt")
+    flags = " ".join([NVCC] + FLAGS + list(extra))
+    if not os.path.exists(stamp) or open(stamp).read() != flags:
+        force = True
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     hdr = _newest_header()
 
@@ -58,6 +63,8 @@ def build(force=False, verbose=False, extra=()):
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))
+    with open(stamp, "w") as fh:
+        fh.write(flags)
     return LIB
 
 

@@ -569,6 +569,51 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
 }  // namespace
 
 // ============================================================================ exported C ABI
+namespace {
+
+// Adjoint of the truncated SVD (isvd/b200.h).
+template <class T>
+int adjoint_api(isvd_int_t m, isvd_int_t n, isvd_int_t k, char ordera, const T *a, isvd_int_t lda, const T *s,
+                const T *ut, isvd_int_t ldut, const T *vt, isvd_int_t ldvt, const T *ds, const T *dut,
+                isvd_int_t lddut, const T *dvt, isvd_int_t lddvt, T *da, isvd_int_t ldda, int cg_iters, double tol,
+                int *iterations) {
+  int its = 0;
+  const int st = api_call([&] {
+    const char ordera_ = arg2char("ORDERA", ordera, "CR");
+    REQUIRE(m > 0 && n > 0 && k > 0 && k <= m && k <= n);
+    REQUIRE(a != nullptr && s != nullptr && ut != nullptr && vt != nullptr && da != nullptr);
+    REQUIRE(ordera_ == 'R' ? (lda >= n && ldda >= n) : (lda >= m && ldda >= m));
+    REQUIRE(ldut >= k && ldvt >= k);
+    if (dut) REQUIRE(lddut >= k);
+    if (dvt) REQUIRE(lddvt >= k);
+    REQUIRE(cg_iters >= 0 && tol >= 0);
+    Ctx c(kNative);
+    cudaStream_t sst = c.sc.st;
+    View<T> A, S, U, V, dS, dU, dV, dA;
+    if (ordera_ == 'R') {
+      A.bind(a, n, m, lda, true, sst);
+      dA.bind(da, n, m, ldda, false, sst);
+    } else {
+      A.bind(a, m, n, lda, true, sst);
+      dA.bind(da, m, n, ldda, false, sst);
+    }
+    S.bind(s, k, 1, k, true, sst);
+    U.bind(ut, k, m, ldut, true, sst);
+    V.bind(vt, k, n, ldvt, true, sst);
+    if (ds) dS.bind(ds, k, 1, k, true, sst);
+    if (dut) dU.bind(dut, k, m, lddut, true, sst);
+    if (dvt) dV.bind(dvt, k, n, lddvt, true, sst);
+    its = svd_adjoint_dev<T>(c.sc, m, n, k, ordera_, A.d, lda, U.d, ldut, S.d, V.d, ldvt, dut ? dU.d : nullptr, lddut,
+                             ds ? dS.d : nullptr, dvt ? dV.d : nullptr, lddvt, dA.d, ldda, cg_iters, tol);
+    dA.back(sst);
+    sync();
+  });
+  if (iterations) *iterations = its;
+  return st;
+}
+
+}  // namespace
+
 #pragma GCC visibility push(default)
 extern "C" {
 
@@ -804,6 +849,26 @@ int isvd_dIntegrateKolmogorovNagumo_noalloc(const isvd_Param param, const isvd_d
     if (retc > ++ri) retv[ri] = (double)r.iterations;
     if (retc > ++ri) retv[ri] = r.error;
   });
+}
+
+int isvd_sSvdAdjoint(const isvd_int_t m, const isvd_int_t n, const isvd_int_t k, const char ordera,
+                     const isvd_s_val_t *a, const isvd_int_t lda, const isvd_s_val_t *s, const isvd_s_val_t *ut,
+                     const isvd_int_t ldut, const isvd_s_val_t *vt, const isvd_int_t ldvt, const isvd_s_val_t *ds,
+                     const isvd_s_val_t *dut, const isvd_int_t lddut, const isvd_s_val_t *dvt,
+                     const isvd_int_t lddvt, isvd_s_val_t *da, const isvd_int_t ldda, const int cg_iters,
+                     const double tol, int *iterations) {
+  return adjoint_api<float>(m, n, k, ordera, a, lda, s, ut, ldut, vt, ldvt, ds, dut, lddut, dvt, lddvt, da, ldda,
+                            cg_iters, tol, iterations);
+}
+
+int isvd_dSvdAdjoint(const isvd_int_t m, const isvd_int_t n, const isvd_int_t k, const char ordera,
+                     const isvd_d_val_t *a, const isvd_int_t lda, const isvd_d_val_t *s, const isvd_d_val_t *ut,
+                     const isvd_int_t ldut, const isvd_d_val_t *vt, const isvd_int_t ldvt, const isvd_d_val_t *ds,
+                     const isvd_d_val_t *dut, const isvd_int_t lddut, const isvd_d_val_t *dvt,
+                     const isvd_int_t lddvt, isvd_d_val_t *da, const isvd_int_t ldda, const int cg_iters,
+                     const double tol, int *iterations) {
+  return adjoint_api<double>(m, n, k, ordera, a, lda, s, ut, ldut, vt, ldvt, ds, dut, lddut, dvt, lddvt, da, ldda,
+                             cg_iters, tol, iterations);
 }
 
 }  // extern "C"

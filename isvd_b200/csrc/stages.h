@@ -71,6 +71,15 @@ void coeff_orthonormalize(const StageCtx &c, int Nl, int l, int N, double *G, do
 void coeff_unorthonormalize(const StageCtx &c, int Nl, int l, int N, const double *X, const double *M, long long ldm,
                             double *out);
 
+// Adjoint of the truncated SVD A ~ U diag(s) V' (adjoint.cu): dA from dU (m x k), ds (k), dV (n x k),
+// any of them null.  A and dA stored per ordera; U, V, dU, dV row-major.  cg_iters bounds the
+// conjugate-gradient iterations of the orthogonal-complement terms (0: rank-k formula).  Returns
+// the iterations used (both complement systems).
+template <class T>
+int svd_adjoint_dev(const StageCtx &c, int m, int n, int k, char ordera, const T *a, long long lda, const T *u,
+                    long long ldu, const T *s, const T *v, long long ldv, const T *du, long long lddu, const T *ds,
+                    const T *dv, long long lddv, T *da, long long ldda, int cg_iters, double tol);
+
 // Z = A' Qbar (n x l, row-major, ld l) for A m x n stored per ordera.
 template <class T>
 void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
