@@ -98,6 +98,42 @@ void isvd_gpu_profile_enable( int on );
 void isvd_gpu_profile_reset( void );
 int  isvd_gpu_profile_get( const char *tag, double *ms, unsigned long long *launches, double *flops );
 
+/* ---------------------------------------------------------------- batched solves
+ * Many independent matrices of uneven sizes and ranks solved together (no counterpart in the
+ * reference): GP / GR / KN / GR with one MPI rank, products in the element type on CUDA cores and
+ * FP64 l x l steps, every stage as grouped launches over all matrices.  A batch fixes the shapes
+ * (matrix i: m[i] x n[i], rank k[i], oversampling p[i], l = k + p <= 96 and l <= min(m, n); N sketches
+ * each) and owns the workspace; NULL on failure (see isvd_gpu_get_last_error).
+ * isvd_?BatchIsvd solves every matrix: a[i] (row-major, lda[i] >= n[i]), s[i] (l values), ut[i]
+ * (m[i] x l, ldut[i] >= l, k[i] valid columns), vt[i] (n[i] x l, ldvt[i] >= l), all device memory;
+ * seed[i] draws the Gaussian test matrix as isvd_?Isvd with that seed; argv / argc: the
+ * Kolmogorov-Nagumo arguments {maxit, tol} (defaults 256, 1e-4).  Each matrix stops at its own
+ * convergence; iterations[i] and errors[i] (may be NULL) receive the KN iteration count (maxit + 1
+ * when exhausted) and error.  The work before and after the iterations is captured as CUDA graphs
+ * on the second solve with the same buffers and replayed by later ones.  Returns an ISVD_GPU_* status. */
+typedef struct isvd_gpu_batch isvd_gpu_batch;
+isvd_gpu_batch *isvd_sBatchCreate(
+    const isvd_int_t count, const isvd_int_t *m, const isvd_int_t *n, const isvd_int_t *k, const isvd_int_t *p,
+    const isvd_int_t N
+);
+isvd_gpu_batch *isvd_dBatchCreate(
+    const isvd_int_t count, const isvd_int_t *m, const isvd_int_t *n, const isvd_int_t *k, const isvd_int_t *p,
+    const isvd_int_t N
+);
+int isvd_sBatchIsvd(
+    isvd_gpu_batch *batch, const isvd_s_val_t *const *a, const isvd_int_t *lda, isvd_s_val_t *const *s,
+    isvd_s_val_t *const *ut, const isvd_int_t *ldut, isvd_s_val_t *const *vt, const isvd_int_t *ldvt,
+    const isvd_int_t *seed, const isvd_s_val_t *argv, const isvd_int_t argc, isvd_int_t *iterations,
+    isvd_s_val_t *errors
+);
+int isvd_dBatchIsvd(
+    isvd_gpu_batch *batch, const isvd_d_val_t *const *a, const isvd_int_t *lda, isvd_d_val_t *const *s,
+    isvd_d_val_t *const *ut, const isvd_int_t *ldut, isvd_d_val_t *const *vt, const isvd_int_t *ldvt,
+    const isvd_int_t *seed, const isvd_d_val_t *argv, const isvd_int_t argc, isvd_int_t *iterations,
+    isvd_d_val_t *errors
+);
+void isvd_gpu_batch_destroy( isvd_gpu_batch *batch );
+
 /* ---------------------------------------------------------------- truncated-SVD adjoint
  * Gradient of a scalar loss L(U, s, V) with respect to A, where A ~ U diag(s) V' are the k leading
  * singular triplets of A (m x n; s descending, distinct, and s_k > s_(k+1)).  No counterpart in the

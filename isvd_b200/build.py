@@ -59,7 +59,12 @@ def build(force=False, verbose=False, extra=()):
         results = list(ex.map(compile_one, srcs))
     objs = [o for o, _ in results]
     if force or any(c for _, c in results) or not os.path.exists(LIB):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda"]
+        # export the C ABI only (isvd_*); template code instantiated from the C++ standard library
+        # would otherwise be exported with default visibility
+        vmap = os.path.join(OBJ, "exports.map")
+        with open(vmap, "w") as fh:
+            fh.write("{ global: isvd_*; local: *; };\n")
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcuda", "-Xlinker", "--version-script=" + vmap]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s%s" % (r.stdout, r.stderr))

@@ -1,0 +1,613 @@
+// Batched iSVD: many independent matrices of uneven sizes and ranks (GP / GR / KN / GR, one MPI
+// rank, products in the matrices' own type on CUDA cores, FP64 l x l steps).
+//
+// Every stage runs as grouped launches over all matrices instead of one launch per matrix:
+//   * products: one persistent GEMM kernel walks a list of (product, output tile) work items --
+//     the sketches, Gram matrices, applies, G = Qs'Qs products and Kolmogorov-Nagumo coefficient
+//     products of every matrix in one launch.  Its tile shape is chosen per product list by
+//     measurement on first use (every candidate computes the same result in the same order; the
+//     fastest is kept and remembered by a signature of the list);
+//   * small dense steps: the Jacobi eigensolver with one CTA per l x l matrix of its own size, and
+//     the Kolmogorov-Nagumo step with one thread-block cluster per matrix;
+//   * the Kolmogorov-Nagumo iterations of all matrices advance together; a matrix leaves the
+//     active set at its own convergence test, so its iteration count and error are those of a
+//     single solve.
+// A plan holds the workspace and the device-side work lists of one batch shape.  The work before
+// and after the iterations is captured as two CUDA graphs on the second solve with the same
+// buffers (the first one runs eagerly and measures the tile shapes) and replayed afterwards.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "batched.h"
+#include "kernels.h"
+#include "runtime.h"
+
+namespace isvdb {
+namespace {
+
+// ------------------------------------------------------------------------- grouped GEMM
+struct GProd {  // C = alpha A B + beta C, A M x K, B K x N (element strides), C M x N
+  int M, N, K;
+  const void *A;
+  long long a_rs, a_cs;
+  const void *B;
+  long long b_rs, b_cs;
+  void *C;
+  long long c_rs, c_cs;
+  double alpha, beta;
+  int tile0, tn;  // first work item of this product, output tiles along N
+};
+
+constexpr int kGThreads = 256;
+
+template <class T, class Tout, int BM, int BN>
+__global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restrict__ prods, int nprod, int total) {
+  constexpr int BK = 16, TM = BM / 16, TN = BN / 16;
+  constexpr int LA = BM * BK / kGThreads, LB = BK * BN / kGThreads;
+  __shared__ T As[BK][BM + 1];
+  __shared__ T Bs[BK][BN + 1];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    int lo = 0, hi = nprod - 1;  // the product owning work item t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prods[mid].tile0 <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GProd g = prods[lo];
+    const int tt = t - g.tile0, m0 = (tt / g.tn) * BM, n0 = (tt % g.tn) * BN;
+    const T *__restrict__ A = static_cast<const T *>(g.A);
+    const T *__restrict__ B = static_cast<const T *>(g.B);
+    const bool akc = (g.a_cs == 1), bnc = (g.b_cs == 1);
+    T acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+    T ra[LA], rb[LB];
+    auto load = [&](int k0) {
+#pragma unroll
+      for (int r = 0; r < LA; ++r) {
+        const int e = tid + r * kGThreads;
+        const int mm = akc ? e / BK : e % BM, kk = akc ? e % BK : e / BM;
+        const int gm = m0 + mm, gk = k0 + kk;
+        ra[r] = (gm < g.M && gk < g.K) ? A[(long long)gm * g.a_rs + (long long)gk * g.a_cs] : T(0);
+      }
+#pragma unroll
+      for (int r = 0; r < LB; ++r) {
+        const int e = tid + r * kGThreads;
+        const int nn = bnc ? e % BN : e / BK, kk = bnc ? e / BN : e % BK;
+        const int gn = n0 + nn, gk = k0 + kk;
+        rb[r] = (gn < g.N && gk < g.K) ? B[(long long)gk * g.b_rs + (long long)gn * g.b_cs] : T(0);
+      }
+    };
+    auto store = [&]() {
+#pragma unroll
+      for (int r = 0; r < LA; ++r) {
+        const int e = tid + r * kGThreads;
+        const int mm = akc ? e / BK : e % BM, kk = akc ? e % BK : e / BM;
+        As[kk][mm] = ra[r];
+      }
+#pragma unroll
+      for (int r = 0; r < LB; ++r) {
+        const int e = tid + r * kGThreads;
+        const int nn = bnc ? e % BN : e / BK, kk = bnc ? e / BN : e % BK;
+        Bs[kk][nn] = rb[r];
+      }
+    };
+    if (g.K > 0) load(0);
+    for (int k0 = 0; k0 < g.K; k0 += BK) {
+      store();
+      __syncthreads();
+      if (k0 + BK < g.K) load(k0 + BK);
+#pragma unroll
+      for (int kk = 0; kk < BK; ++kk) {
+        T av[TM], bv[TN];
+#pragma unroll
+        for (int i = 0; i < TM; ++i) av[i] = As[kk][ty + 16 * i];
+#pragma unroll
+        for (int j = 0; j < TN; ++j) bv[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < TM; ++i)
+#pragma unroll
+          for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+      }
+      __syncthreads();
+    }
+    Tout *__restrict__ C = static_cast<Tout *>(g.C);
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gm = m0 + ty + 16 * i;
+      if (gm >= g.M) continue;
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const int gn = n0 + tx + 16 * j;
+        if (gn >= g.N) continue;
+        Tout *c = C + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+        double v = g.alpha * (double)acc[i][j];
+        if (g.beta != 0.0) v += g.beta * (double)(*c);
+        *c = (Tout)v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- grouped elementwise
+struct GMap {  // dst(r, c) = f(src(r, c), w[c]) over rows x cols
+  const void *src;
+  long long s_rs, s_cs;
+  void *dst;
+  long long d_rs, d_cs;
+  int rows, cols;
+  const double *w;
+  int mode;
+};
+enum { kMapCopy = 0, kMapInvSqrt = 1, kMapSqrt = 2, kMapIdentity = 3 };
+
+template <class Ts, class Td>
+__global__ void gmap_kernel(const GMap *__restrict__ maps) {
+  const GMap g = maps[blockIdx.y];
+  const long long total = (long long)g.rows * g.cols;
+  const Ts *src = static_cast<const Ts *>(g.src);
+  Td *dst = static_cast<Td *>(g.dst);
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long r = e / g.cols, c = e - r * g.cols;
+    double v;
+    if (g.mode == kMapIdentity) {
+      v = (r == c) ? 1.0 : 0.0;
+    } else {
+      const double x = (double)src[r * g.s_rs + c * g.s_cs];
+      v = g.mode == kMapInvSqrt ? x / sqrt(g.w[c]) : g.mode == kMapSqrt ? sqrt(x) : x;
+    }
+    dst[r * g.d_rs + c * g.d_cs] = (Td)v;
+  }
+}
+
+// ----------------------------------------------------------------------- device lists
+template <class X>
+struct DevList {
+  DBuf<X> d;
+  int count = 0;
+  void upload(const std::vector<X> &h, cudaStream_t st) {
+    count = (int)h.size();
+    d.ensure(std::max<size_t>(1, h.size()));
+    if (!h.empty()) CK(cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice, st));
+  }
+};
+
+constexpr int kConfigs = 3;
+constexpr int kBM[kConfigs] = {64, 128, 128}, kBN[kConfigs] = {64, 64, 128};
+std::map<std::string, int> g_tuned;  // product-list signature -> tile shape
+
+// A grouped product list: host descriptors, the device copy for the chosen tile shape.
+template <class T, class Tout>
+struct GemmList {
+  std::vector<GProd> host;
+  DevList<GProd> dev;
+  int config = -1, total = 0, uploaded = -1;
+
+  void clear() {
+    host.clear();
+    uploaded = -1;
+  }
+  std::string signature() const {
+    int bm = 0, bn = 0, bk = 0;
+    for (const auto &g : host) {
+      bm = std::max(bm, g.M);
+      bn = std::max(bn, g.N);
+      bk = std::max(bk, g.K);
+    }
+    auto lg = [](int v) {
+      int b = 0;
+      while ((1 << b) < v) ++b;
+      return b;
+    };
+    return std::to_string(sizeof(T)) + std::to_string(sizeof(Tout)) + ":" + std::to_string(host.size()) + ":" +
+           std::to_string(lg(bm)) + "," + std::to_string(lg(bn)) + "," + std::to_string(lg(bk));
+  }
+  void finalize(int cfg, cudaStream_t st) {  // work items for tile shape cfg, uploaded
+    int tot = 0;
+    for (auto &g : host) {
+      g.tn = (g.N + kBN[cfg] - 1) / kBN[cfg];
+      g.tile0 = tot;
+      tot += ((g.M + kBM[cfg] - 1) / kBM[cfg]) * g.tn;
+    }
+    total = tot;
+    dev.upload(host, st);
+    uploaded = cfg;
+  }
+  void launch(int cfg, cudaStream_t st) {  // kernels only (capturable)
+    if (host.empty() || total == 0) return;
+    const int grid = std::max(1, std::min(total, 4 * Runtime::get().num_sms));
+    switch (cfg) {
+      case 0: ggemm_kernel<T, Tout, 64, 64><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
+      case 1: ggemm_kernel<T, Tout, 128, 64><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
+      default: ggemm_kernel<T, Tout, 128, 128><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
+    }
+    KLAUNCHED();
+  }
+  // Choose the tile shape (measuring every candidate on first sight of the signature when all
+  // products overwrite their outputs) and upload the work items.  May run the products.
+  void prepare(cudaStream_t st, bool may_measure) {
+    if (host.empty()) return;
+    if (config < 0) {
+      const std::string key = signature();
+      auto it = g_tuned.find(key);
+      bool idempotent = true;
+      for (const auto &g : host) idempotent = idempotent && g.beta == 0.0;
+      if (it != g_tuned.end()) {
+        config = it->second;
+      } else if (may_measure && idempotent) {
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        float best = 1e30f;
+        int bestc = 0;
+        for (int cfg = 0; cfg < kConfigs; ++cfg) {
+          finalize(cfg, st);
+          CK(cudaEventRecord(e0, st));
+          launch(cfg, st);
+          CK(cudaEventRecord(e1, st));
+          CK(cudaEventSynchronize(e1));
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          if (ms < best) {
+            best = ms;
+            bestc = cfg;
+          }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        config = bestc;
+        g_tuned[key] = bestc;
+      } else {
+        config = 0;
+      }
+    }
+    if (uploaded != config) finalize(config, st);
+  }
+  void run(cudaStream_t st, bool may_measure) {
+    prepare(st, may_measure);
+    launch(config, st);
+  }
+};
+
+template <class Ts, class Td>
+struct MapList {
+  std::vector<GMap> host;
+  DevList<GMap> dev;
+  int gx = 1;
+  void prepare(cudaStream_t st) {
+    dev.upload(host, st);
+    long long mx = 1;
+    for (const auto &g : host) mx = std::max<long long>(mx, (long long)g.rows * g.cols);
+    gx = (int)std::min<long long>((mx + 255) / 256, 64);
+  }
+  void launch(cudaStream_t st) {
+    if (host.empty()) return;
+    gmap_kernel<Ts, Td><<<dim3(gx, (unsigned)host.size()), 256, 0, st>>>(dev.d.p);
+    KLAUNCHED();
+  }
+};
+
+inline GProd prod(int M, int N, int K, const void *A, long long a_rs, long long a_cs, const void *B, long long b_rs,
+                  long long b_cs, void *C, long long c_rs, long long c_cs, double alpha = 1.0) {
+  GProd g;
+  g.M = M; g.N = N; g.K = K;
+  g.A = A; g.a_rs = a_rs; g.a_cs = a_cs;
+  g.B = B; g.b_rs = b_rs; g.b_cs = b_cs;
+  g.C = C; g.c_rs = c_rs; g.c_cs = c_cs;
+  g.alpha = alpha; g.beta = 0.0;
+  g.tile0 = 0; g.tn = 1;
+  return g;
+}
+
+inline GMap gm(const void *src, long long s_rs, long long s_cs, void *dst, long long d_rs, long long d_cs, int rows,
+               int cols, int mode, const double *w = nullptr) {
+  GMap g;
+  g.src = src; g.s_rs = s_rs; g.s_cs = s_cs;
+  g.dst = dst; g.d_rs = d_rs; g.d_cs = d_cs;
+  g.rows = rows; g.cols = cols; g.w = w; g.mode = mode;
+  return g;
+}
+
+// ---------------------------------------------------------------------------- the plan
+template <class T>
+struct Plan : BatchPlan {
+  int count = 0, N = 0, max_l = 0;
+  std::vector<int> m, n, k, l, Nl;
+  struct Mat {  // workspace of one matrix
+    DBuf<T> om, y, qs, wp, mt, qbar, z, wk, vk;
+    DBuf<double> wg, vg, lam, G, W, DD, C, Ci, F, Fs, work, wz, vz, lz;
+  };
+  std::vector<std::unique_ptr<Mat>> mats;
+  DBuf<double> errs;
+  DBuf<int> status;
+  // bound user buffers
+  std::vector<const T *> a;
+  std::vector<long long> lda, ldut, ldvt;
+  std::vector<T *> s, ut, vt;
+  std::vector<unsigned long long> seeds;
+  bool bound = false;
+  int solves = 0;
+  // work lists
+  GemmList<T, T> sketch, apply, qbar_l, proj, ul, vl;
+  GemmList<T, double> gram, gfull, wzl;
+  GemmList<double, double> l1, l2, l4;
+  MapList<double, T> m_scale, m_mt, m_s, m_wk, m_vk;
+  MapList<double, double> m_init;
+  DevList<EigDesc> eig1, eig2;
+  DevList<KnStep> steps;
+  // graphs of the work before and after the iterations
+  cudaGraphExec_t pre = nullptr, post = nullptr;
+  unsigned long long pre_k = 0, post_k = 0;
+
+  ~Plan() override { drop_graphs(); }
+  void drop_graphs() {
+    if (pre) cudaGraphExecDestroy(pre);
+    if (post) cudaGraphExecDestroy(post);
+    pre = post = nullptr;
+  }
+};
+
+template <class T>
+void build_lists(Plan<T> &P, cudaStream_t st) {
+  const int B = P.count, N = P.N;
+  P.sketch.clear(); P.apply.clear(); P.qbar_l.clear(); P.proj.clear(); P.ul.clear(); P.vl.clear();
+  P.gram.clear(); P.gfull.clear(); P.wzl.clear();
+  P.m_scale.host.clear(); P.m_s.host.clear(); P.m_wk.host.clear(); P.m_vk.host.clear(); P.m_init.host.clear();
+  std::vector<EigDesc> e1, e2;
+  for (int b = 0; b < B; ++b) {
+    auto &M = *P.mats[b];
+    const int m = P.m[b], n = P.n[b], k = P.k[b], l = P.l[b], Nl = P.Nl[b];
+    const size_t ll = (size_t)l * l;
+    P.sketch.host.push_back(prod(m, Nl, n, P.a[b], P.lda[b], 1, M.om.p, Nl, 1, M.y.p, Nl, 1));
+    for (int i = 0; i < N; ++i) {
+      P.gram.host.push_back(prod(l, l, m, M.y.p + i * l, 1, Nl, M.y.p + i * l, Nl, 1, M.wg.p + i * ll, l, 1));
+      e1.push_back(EigDesc{l, M.wg.p + i * ll, M.vg.p + i * ll, M.lam.p + (size_t)i * l});
+      P.m_scale.host.push_back(gm(M.vg.p + i * ll, l, 1, M.wp.p + i * ll, l, 1, l, l, kMapInvSqrt, M.lam.p + i * l));
+      P.apply.host.push_back(prod(m, l, l, M.y.p + i * l, Nl, 1, M.wp.p + i * ll, l, 1, M.qs.p + i * l, Nl, 1));
+    }
+    P.gfull.host.push_back(prod(Nl, Nl, m, M.qs.p, 1, Nl, M.qs.p, Nl, 1, M.G.p, Nl, 1));
+    // iterate [M | B | Bgc] in W[0]: Bc = G[:, 0:l], M = [I; 0]
+    P.m_init.host.push_back(gm(M.G.p, Nl, 1, M.W.p + l, 3 * l, 1, Nl, l, kMapCopy));
+    P.m_init.host.push_back(gm(nullptr, 0, 0, M.W.p, 3 * l, 1, Nl, l, kMapIdentity));
+    // after the iterations: Qbar = Qs M, Z = A' Qbar, W = Z'Z, eig, s, U, V
+    P.qbar_l.host.push_back(prod(m, l, Nl, M.qs.p, Nl, 1, M.mt.p, l, 1, M.qbar.p, l, 1));
+    P.proj.host.push_back(prod(n, l, m, P.a[b], 1, P.lda[b], M.qbar.p, l, 1, M.z.p, l, 1));
+    P.wzl.host.push_back(prod(l, l, n, M.z.p, 1, l, M.z.p, l, 1, M.wz.p, l, 1));
+    e2.push_back(EigDesc{l, M.wz.p, M.vz.p, M.lz.p});
+    P.m_s.host.push_back(gm(M.lz.p, 1, 0, P.s[b], 1, 0, l, 1, kMapSqrt));
+    P.m_wk.host.push_back(gm(M.vz.p, l, 1, M.wk.p, k, 1, l, k, kMapCopy));
+    P.m_vk.host.push_back(gm(M.vz.p, l, 1, M.vk.p, k, 1, l, k, kMapInvSqrt, M.lz.p));
+    P.ul.host.push_back(prod(m, k, l, M.qbar.p, l, 1, M.wk.p, k, 1, P.ut[b], P.ldut[b], 1));
+    P.vl.host.push_back(prod(n, k, l, M.z.p, l, 1, M.vk.p, k, 1, P.vt[b], P.ldvt[b], 1));
+  }
+  P.eig1.upload(e1, st);
+  P.eig2.upload(e2, st);
+  P.m_scale.prepare(st); P.m_s.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
+}
+
+template <class T>
+void run_pre(Plan<T> &P, cudaStream_t st, bool measure) {
+  for (int b = 0; b < P.count; ++b)
+    rng_gaussian<T>(P.mats[b]->om.p, P.n[b], P.Nl[b], P.Nl[b], P.seeds[b], 0, st);
+  P.sketch.run(st, measure);
+  P.gram.run(st, measure);
+  sym_eig_grouped(P.eig1.d.p, P.eig1.count, P.max_l, +1, true, P.status.p, st);
+  P.m_scale.launch(st);
+  P.apply.run(st, measure);
+  P.gfull.run(st, measure);
+  P.m_init.launch(st);
+}
+
+template <class T>
+void run_post(Plan<T> &P, cudaStream_t st, bool measure) {
+  P.qbar_l.run(st, measure);
+  P.proj.run(st, measure);
+  P.wzl.run(st, measure);
+  sym_eig_grouped(P.eig2.d.p, P.eig2.count, P.max_l, +1, true, P.status.p, st);
+  P.m_s.launch(st);
+  P.m_wk.launch(st);
+  P.m_vk.launch(st);
+  P.ul.run(st, measure);
+  P.vl.run(st, measure);
+}
+
+// Runs body eagerly (first solve, which measures tile shapes), or captures it once and replays it.
+template <class F>
+void graphed(cudaGraphExec_t &exec, unsigned long long &nk, bool capture, cudaStream_t st, F &&body) {
+  if (!capture) {
+    body();
+    return;
+  }
+  if (!exec) {
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(st, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamEndCapture(st, &g));
+    nk = count_kernel_nodes(g);
+    const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+  }
+  CK(cudaGraphLaunch(exec, st));
+  g_launches.fetch_add(nk);
+}
+
+}  // namespace
+
+int plan_count(const BatchPlan *plan) {
+  return plan->elem == 4 ? static_cast<const Plan<float> *>(plan)->count : static_cast<const Plan<double> *>(plan)->count;
+}
+
+template <class T>
+BatchPlan *batch_plan_create(int count, const int *m, const int *n, const int *k, const int *p, int N) {
+  if (count <= 0) fail(kErrArgument, "batched iSVD: count = %d", count);
+  if (N <= 0) fail(kErrArgument, "batched iSVD: N = %d", N);
+  std::unique_ptr<Plan<T>> P(new Plan<T>());
+  P->elem = sizeof(T);
+  P->count = count;
+  P->N = N;
+  P->mats.resize(count);
+  for (int b = 0; b < count; ++b) {
+    const int l = k[b] + p[b], Nl = N * l;
+    if (m[b] <= 0 || n[b] <= 0 || k[b] <= 0 || p[b] < 0 || l > n[b] || l > m[b])
+      fail(kErrArgument, "batched iSVD: matrix %d: m = %d, n = %d, k = %d, p = %d", b, m[b], n[b], k[b], p[b]);
+    if (l > 96) fail(kErrUnsupported, "batched iSVD: matrix %d: l = %d > 96", b, l);
+    P->m.push_back(m[b]); P->n.push_back(n[b]); P->k.push_back(k[b]); P->l.push_back(l); P->Nl.push_back(Nl);
+    P->max_l = std::max(P->max_l, l);
+    auto M = std::make_unique<typename Plan<T>::Mat>();
+    const size_t ll = (size_t)l * l, nl = (size_t)Nl * l;
+    M->om.alloc((size_t)n[b] * Nl);
+    M->y.alloc((size_t)m[b] * Nl);
+    M->qs.alloc((size_t)m[b] * Nl);
+    M->wp.alloc(N * ll);
+    M->mt.alloc(nl);
+    M->qbar.alloc((size_t)m[b] * l);
+    M->z.alloc((size_t)n[b] * l);
+    M->wk.alloc((size_t)l * k[b]);
+    M->vk.alloc((size_t)l * k[b]);
+    M->wg.alloc(N * ll); M->vg.alloc(N * ll); M->lam.alloc((size_t)N * l);
+    M->G.alloc((size_t)Nl * Nl);
+    M->W.alloc(6 * nl);
+    M->DD.alloc(2 * ll); M->C.alloc(ll); M->Ci.alloc(ll); M->F.alloc(ll); M->Fs.alloc(4 * ll);
+    M->work.alloc(kKnWorkMatrices * ll + 64);
+    M->wz.alloc(ll); M->vz.alloc(ll); M->lz.alloc(l);
+    P->mats[b] = std::move(M);
+  }
+  P->errs.alloc(count);
+  P->status.alloc(1);
+  return P.release();
+}
+
+template <class T>
+void batch_solve(BatchPlan *plan, const T *const *a, const long long *lda, T *const *s, T *const *ut,
+                 const long long *ldut, T *const *vt, const long long *ldvt, const unsigned long long *seeds, int maxit,
+                 double tol, int *iters, double *errs) {
+  if (!plan || plan->elem != (int)sizeof(T)) fail(kErrArgument, "batched iSVD: plan of another element type");
+  Plan<T> &P = *static_cast<Plan<T> *>(plan);
+  Runtime &rt = Runtime::get();
+  cudaStream_t st = rt.stream;
+  const int B = P.count, N = P.N;
+  // bind the caller's buffers; a change rebuilds the work lists and the graphs
+  bool same = P.bound;
+  for (int b = 0; b < B && same; ++b)
+    same = P.a[b] == a[b] && P.lda[b] == lda[b] && P.s[b] == s[b] && P.ut[b] == ut[b] && P.ldut[b] == ldut[b] &&
+           P.vt[b] == vt[b] && P.ldvt[b] == ldvt[b] && P.seeds[b] == seeds[b];
+  if (!same) {
+    for (int b = 0; b < B; ++b) {
+      if (lda[b] < P.n[b] || ldut[b] < P.l[b] || ldvt[b] < P.l[b])
+        fail(kErrArgument, "batched iSVD: matrix %d: leading dimension too small", b);
+      if (!is_device_pointer(a[b]) || !is_device_pointer(s[b]) || !is_device_pointer(ut[b]) ||
+          !is_device_pointer(vt[b]))
+        fail(kErrArgument, "batched iSVD: matrix %d: a, s, ut and vt must be device memory", b);
+    }
+    P.a.assign(a, a + B); P.lda.assign(lda, lda + B); P.s.assign(s, s + B); P.ut.assign(ut, ut + B);
+    P.ldut.assign(ldut, ldut + B); P.vt.assign(vt, vt + B); P.ldvt.assign(ldvt, ldvt + B);
+    P.seeds.assign(seeds, seeds + B);
+    P.drop_graphs();
+    build_lists(P, st);
+    P.bound = true;
+    P.solves = 0;
+  }
+  const bool capture = P.solves > 0 && st != nullptr && !profiling();
+  CK(cudaMemsetAsync(P.status.p, 0, sizeof(int), st));
+  graphed(P.pre, P.pre_k, capture, st, [&] { run_pre(P, st, !capture); });
+
+  // ---- Kolmogorov-Nagumo iterations of the active matrices (reference :153-266)
+  const double invN = 1.0 / N;
+  const int cap = maxit > 0 ? maxit : 1000000;
+  std::vector<int> active(B), cur(B, 0), it_of(B, 0);
+  for (int b = 0; b < B; ++b) active[b] = b;
+  std::vector<double> herr(B, 0.0);
+  std::vector<KnStep> hsteps;
+  for (int iter = 1; !active.empty(); ++iter) {
+    P.l1.clear(); P.l2.clear(); P.l4.clear();
+    hsteps.clear();
+    for (int b : active) {
+      auto &M = *P.mats[b];
+      const int l = P.l[b], Nl = P.Nl[b];
+      const size_t ll = (size_t)l * l, nl3 = (size_t)Nl * 3 * l;
+      double *Wc = M.W.p + cur[b] * nl3, *Wn = M.W.p + (1 - cur[b]) * nl3;
+      const long long lw = 3LL * l;
+      P.l1.host.push_back(prod(Nl, l, Nl, M.G.p, Nl, 1, Wc + l, lw, 1, Wc + 2 * l, lw, 1, invN));
+      P.l2.host.push_back(prod(l, l, Nl, Wc + l, 1, lw, Wc + l, lw, 1, M.DD.p, l, 1, invN));
+      P.l2.host.push_back(prod(l, l, Nl, Wc + l, 1, lw, Wc + 2 * l, lw, 1, M.DD.p + ll, l, 1, invN));
+      P.l4.host.push_back(prod(Nl, l, 2 * l, Wc, lw, 1, M.Fs.p, l, 1, Wn, lw, 1));
+      P.l4.host.push_back(prod(Nl, l, 2 * l, Wc + l, lw, 1, M.Fs.p + 2 * ll, l, 1, Wn + l, lw, 1));
+      KnStep s;
+      s.l = l; s.Dc = M.DD.p; s.Dgc = M.DD.p + ll; s.C = M.C.p; s.Cinv = M.Ci.p; s.F = M.F.p;
+      s.err = P.errs.p + b; s.work = M.work.p; s.status = P.status.p; s.bar = nullptr;
+      s.ns_target = 1e-18;
+      s.fstack = M.Fs.p; s.fstack_scale = invN;
+      hsteps.push_back(s);
+    }
+    P.l1.run(st, true);
+    P.l2.run(st, true);
+    P.steps.upload(hsteps, st);
+    kn_step_grouped(P.steps.d.p, (int)hsteps.size(), P.max_l, st);
+    P.l4.run(st, true);
+    int hstatus = 0;
+    CK(cudaMemcpyAsync(herr.data(), P.errs.p, B * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&hstatus, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hstatus) fail(kErrNumerical, "batched iSVD: small dense solver reported status %d", hstatus);
+    std::vector<int> next;
+    for (int b : active) {
+      cur[b] = 1 - cur[b];  // the iterate just written
+      if (herr[b] <= tol) {                 // (:235-237)
+        it_of[b] = iter;
+      } else if (iter == cap) {             // (:238-241)
+        it_of[b] = iter + 1;
+      } else {
+        next.push_back(b);
+      }
+    }
+    active.swap(next);
+  }
+  // M of each matrix (in its final iterate) to the element type
+  {
+    MapList<double, T> mt;
+    for (int b = 0; b < B; ++b) {
+      auto &M = *P.mats[b];
+      const size_t nl3 = (size_t)P.Nl[b] * 3 * P.l[b];
+      mt.host.push_back(gm(M.W.p + cur[b] * nl3, 3LL * P.l[b], 1, M.mt.p, P.l[b], 1, P.Nl[b], P.l[b], kMapCopy));
+    }
+    mt.prepare(st);
+    mt.launch(st);
+    graphed(P.post, P.post_k, capture, st, [&] { run_post(P, st, !capture); });
+    int hstatus = 0;
+    CK(cudaMemcpyAsync(&hstatus, P.status.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (hstatus) fail(kErrNumerical, "batched iSVD: small dense solver reported status %d", hstatus);
+  }
+  for (int b = 0; b < B; ++b) {
+    if (iters) iters[b] = it_of[b];
+    if (errs) errs[b] = herr[b];
+  }
+  ++P.solves;
+}
+
+template BatchPlan *batch_plan_create<float>(int, const int *, const int *, const int *, const int *, int);
+template BatchPlan *batch_plan_create<double>(int, const int *, const int *, const int *, const int *, int);
+template void batch_solve<float>(BatchPlan *, const float *const *, const long long *, float *const *, float *const *,
+                                 const long long *, float *const *, const long long *, const unsigned long long *, int,
+                                 double, int *, double *);
+template void batch_solve<double>(BatchPlan *, const double *const *, const long long *, double *const *,
+                                  double *const *, const long long *, double *const *, const long long *,
+                                  const unsigned long long *, int, double, int *, double *);
+
+}  // namespace isvdb

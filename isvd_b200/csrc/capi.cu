@@ -10,7 +10,9 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
+#include "batched.h"
 #include "kernels.h"
 #include "mixed.h"
 #include "runtime.h"
@@ -571,6 +573,52 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
 // ============================================================================ exported C ABI
 namespace {
 
+// Batched iSVD (isvd/b200.h).
+template <class T>
+isvd_gpu_batch *batch_create_api(isvd_int_t count, const isvd_int_t *m, const isvd_int_t *n, const isvd_int_t *k,
+                                 const isvd_int_t *p, isvd_int_t N) {
+  BatchPlan *plan = nullptr;
+  api_call([&] {
+    REQUIRE(count > 0 && m && n && k && p && N > 0);
+    std::vector<int> mm(count), nn(count), kk(count), pp(count);
+    for (isvd_int_t b = 0; b < count; ++b) {
+      mm[b] = (int)m[b]; nn[b] = (int)n[b]; kk[b] = (int)k[b]; pp[b] = (int)p[b];
+    }
+    plan = batch_plan_create<T>((int)count, mm.data(), nn.data(), kk.data(), pp.data(), (int)N);
+  });
+  return reinterpret_cast<isvd_gpu_batch *>(plan);
+}
+
+template <class T>
+int batch_isvd_api(isvd_gpu_batch *batch, const T *const *a, const isvd_int_t *lda, T *const *s, T *const *ut,
+                   const isvd_int_t *ldut, T *const *vt, const isvd_int_t *ldvt, const isvd_int_t *seed, const T *argv,
+                   isvd_int_t argc, isvd_int_t *iterations, T *errors) {
+  return api_call([&] {
+    REQUIRE(batch != nullptr && a && lda && s && ut && ldut && vt && ldvt && seed);
+    if (argc > 0) REQUIRE(argv != nullptr);
+    BatchPlan *plan = reinterpret_cast<BatchPlan *>(batch);
+    if (plan->elem != (int)sizeof(T)) fail(kErrArgument, "batched iSVD: plan created for another element type");
+    int ai = -1;
+    const int maxit = (argc > ++ai) ? (int)argv[ai] : 256;
+    const double tol = (argc > ++ai) ? (double)argv[ai] : 1e-4;
+    REQUIRE(maxit >= 0 && tol >= 0);
+    const int count = plan_count(plan);
+    std::vector<long long> la(count), lu(count), lv(count);
+    std::vector<unsigned long long> sd(count);
+    for (int b = 0; b < count; ++b) {
+      la[b] = lda[b]; lu[b] = ldut[b]; lv[b] = ldvt[b];
+      sd[b] = (unsigned long long)(uint32_t)seed[b];  // as the single-solve driver
+    }
+    std::vector<int> it(count);
+    std::vector<double> er(count);
+    batch_solve<T>(plan, a, la.data(), s, ut, lu.data(), vt, lv.data(), sd.data(), maxit, tol, it.data(), er.data());
+    for (int b = 0; b < count; ++b) {
+      if (iterations) iterations[b] = it[b];
+      if (errors) errors[b] = (T)er[b];
+    }
+  });
+}
+
 // Adjoint of the truncated SVD (isvd/b200.h).
 template <class T>
 int adjoint_api(isvd_int_t m, isvd_int_t n, isvd_int_t k, char ordera, const T *a, isvd_int_t lda, const T *s,
@@ -848,6 +896,37 @@ int isvd_dIntegrateKolmogorovNagumo_noalloc(const isvd_Param param, const isvd_d
     int ri = -1;
     if (retc > ++ri) retv[ri] = (double)r.iterations;
     if (retc > ++ri) retv[ri] = r.error;
+  });
+}
+
+isvd_gpu_batch *isvd_sBatchCreate(const isvd_int_t count, const isvd_int_t *m, const isvd_int_t *n,
+                                  const isvd_int_t *k, const isvd_int_t *p, const isvd_int_t N) {
+  return batch_create_api<float>(count, m, n, k, p, N);
+}
+
+isvd_gpu_batch *isvd_dBatchCreate(const isvd_int_t count, const isvd_int_t *m, const isvd_int_t *n,
+                                  const isvd_int_t *k, const isvd_int_t *p, const isvd_int_t N) {
+  return batch_create_api<double>(count, m, n, k, p, N);
+}
+
+int isvd_sBatchIsvd(isvd_gpu_batch *batch, const isvd_s_val_t *const *a, const isvd_int_t *lda,
+                    isvd_s_val_t *const *s, isvd_s_val_t *const *ut, const isvd_int_t *ldut, isvd_s_val_t *const *vt,
+                    const isvd_int_t *ldvt, const isvd_int_t *seed, const isvd_s_val_t *argv, const isvd_int_t argc,
+                    isvd_int_t *iterations, isvd_s_val_t *errors) {
+  return batch_isvd_api<float>(batch, a, lda, s, ut, ldut, vt, ldvt, seed, argv, argc, iterations, errors);
+}
+
+int isvd_dBatchIsvd(isvd_gpu_batch *batch, const isvd_d_val_t *const *a, const isvd_int_t *lda,
+                    isvd_d_val_t *const *s, isvd_d_val_t *const *ut, const isvd_int_t *ldut, isvd_d_val_t *const *vt,
+                    const isvd_int_t *ldvt, const isvd_int_t *seed, const isvd_d_val_t *argv, const isvd_int_t argc,
+                    isvd_int_t *iterations, isvd_d_val_t *errors) {
+  return batch_isvd_api<double>(batch, a, lda, s, ut, ldut, vt, ldvt, seed, argv, argc, iterations, errors);
+}
+
+void isvd_gpu_batch_destroy(isvd_gpu_batch *batch) {
+  api_call([&] {
+    delete reinterpret_cast<BatchPlan *>(batch);
+    sync();
   });
 }
 

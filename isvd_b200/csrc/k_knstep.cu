@@ -150,7 +150,7 @@ __device__ int ks_block_size(int deg) {
   return sb;
 }
 
-__global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_kernel(KnStep a, KnSeries ser) {
+__device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries &ser) {
   extern __shared__ double sm[];
   __shared__ double red[kKsThreads / 32];
   __shared__ int plan[3];  // degree (-1: Newton-Schulz), block size, Newton-Schulz steps
@@ -289,6 +289,14 @@ __global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_kernel(KnStep a, KnS
   }
 }
 
+__global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_kernel(KnStep a, KnSeries ser) { kn_cluster_body(a, ser); }
+
+// One cluster per step of steps[] (grid = count x cluster size): many independent problems.
+__global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_grouped_kernel(const KnStep *steps, KnSeries ser) {
+  const KnStep a = steps[blockIdx.x / cg::this_cluster().num_blocks()];
+  kn_cluster_body(a, ser);
+}
+
 // Coefficients of g(z)^(1/2) and g(z)^(-1/2), g(z) = 1 - sum_{n>=1} Cat(n-1) z^n: for h = f^alpha
 // with f_0 = 1, h_0 = 1 and h_n = (1/n) sum_{k=1..n} (alpha k - (n - k)) f_k h_(n-k).
 KnSeries make_series() {
@@ -350,6 +358,37 @@ int choose_cluster_size(const KnStep &a, cudaStream_t st) {
 }
 
 }  // namespace
+
+void kn_step_grouped(const KnStep *steps, int count, int max_l, cudaStream_t st) {
+  if (count <= 0) return;
+  if (max_l > kKsMaxL) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > %d", max_l, kKsMaxL);
+  KnStep probe;
+  probe.l = max_l;
+  int cs = choose_cluster_size(probe, st);
+  if (cs == 0) fail(kErrUnsupported, "grouped Kolmogorov-Nagumo step: no thread-block cluster launch on this device");
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKsSmem));
+    attr = true;
+  }
+  cs = std::min(cs, 8);  // many clusters run side by side: eight CTAs each
+  static const KnSeries series = make_series();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(count * cs);
+  cfg.blockDim = dim3(kKsThreads);
+  cfg.dynamicSmemBytes = kKsSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cs;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, kn_cluster_grouped_kernel, steps, series));
+  KLAUNCHED();
+}
 
 void kn_step(const KnStep &a, cudaStream_t st) {
   if (a.l > kKsMaxL) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > %d", a.l, kKsMaxL);

@@ -53,15 +53,17 @@ __device__ __forceinline__ int pk(int i, int j, int n) {
   return i * n - (i * (i - 1)) / 2 + (j - i);
 }
 
+// One CTA per matrix: batch b at Ag + b n^2 (uniform n), or, with desc, the matrix desc[b] (its own n).
 template <bool VS>
 __global__ void __launch_bounds__(kEigThreads)
-    sym_eig_kernel(int n, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg, int order,
-                   bool absval, double *__restrict__ scratch, int *status) {
+    sym_eig_kernel(int n_uniform, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg,
+                   int order, bool absval, double *__restrict__ scratch, int *status, const EigDesc *desc) {
   extern __shared__ double sm[];
   const int b = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
-  const double *A0 = Ag + (size_t)b * n * n;
-  double *V = Vg + (size_t)b * n * n;
-  double *w = wg + (size_t)b * n;
+  const int n = desc ? desc[b].n : n_uniform;
+  const double *A0 = desc ? desc[b].A : Ag + (size_t)b * n * n;
+  double *V = desc ? desc[b].V : Vg + (size_t)b * n * n;
+  double *w = desc ? desc[b].w : wg + (size_t)b * n;
   const int ne = n + (n & 1), np = ne / 2;
   const int npk = n * (n + 1) / 2;
   double *A = sm;                                                           // packed upper triangle
@@ -528,7 +530,7 @@ void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, in
   const size_t smem_vs = eig_smem(n, true);
   if (smem_vs <= rt.smem_optin) {
     CK(cudaFuncSetAttribute(sym_eig_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_vs));
-    sym_eig_kernel<true><<<batch, kEigThreads, smem_vs, st>>>(n, A, V, w, order, absval, nullptr, status);
+    sym_eig_kernel<true><<<batch, kEigThreads, smem_vs, st>>>(n, A, V, w, order, absval, nullptr, status, nullptr);
     KLAUNCHED();
     return;
   }
@@ -536,7 +538,20 @@ void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, in
   if (smem > rt.smem_optin) fail(kErrUnsupported, "symmetric eigensolver: l = %d exceeds on-chip capacity", n);
   DBuf<double> scratch((size_t)batch * n * n);
   CK(cudaFuncSetAttribute(sym_eig_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  sym_eig_kernel<false><<<batch, kEigThreads, smem, st>>>(n, A, V, w, order, absval, scratch.p, status);
+  sym_eig_kernel<false><<<batch, kEigThreads, smem, st>>>(n, A, V, w, order, absval, scratch.p, status,
+                                                            nullptr);
+  KLAUNCHED();
+}
+
+void sym_eig_grouped(const EigDesc *desc, int count, int max_n, int order, bool absval, int *status,
+                     cudaStream_t st) {
+  if (count <= 0 || max_n <= 0) return;
+  const size_t smem = eig_smem(max_n, true);
+  if (smem > Runtime::get().smem_optin)
+    fail(kErrUnsupported, "symmetric eigensolver: l = %d exceeds on-chip capacity", max_n);
+  CK(cudaFuncSetAttribute(sym_eig_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  sym_eig_kernel<true><<<count, kEigThreads, smem, st>>>(0, nullptr, nullptr, nullptr, order, absval, nullptr, status,
+                                                         desc);
   KLAUNCHED();
 }
 

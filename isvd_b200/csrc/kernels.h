@@ -61,6 +61,14 @@ void scale_cols_batched(const Ts *src, long long lds, Td *dst, long long ldd, lo
 // A: batch x (n x n) row-major (only read), V: batch x (n x n) row-major eigenvectors (columns),
 // w: batch x n eigenvalues.  order > 0: sort by |lambda| descending (gesvd of a PSD matrix);
 // order < 0: ascending lambda (syev).  absval: return |lambda| in w.
+struct EigDesc {  // one matrix of a grouped eigensolve: n x n row-major A -> V (columns), w
+  int n;
+  const double *A;
+  double *V, *w;
+};
+// As sym_eig_batched for count matrices of different sizes (desc in device memory; max_n >= every n).
+void sym_eig_grouped(const EigDesc *desc, int count, int max_n, int order, bool absval, int *status,
+                     cudaStream_t st);
 void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, int order, bool absval,
                      int *status, cudaStream_t st);
 
@@ -90,6 +98,8 @@ struct KnSeries {  // power-series coefficients of C(Z) and C(Z)^-1 (k_small.cu)
   double c[kSeriesLen], d[kSeriesLen];
 };
 void kn_step(const KnStep &a, cudaStream_t st);
+// count independent steps (steps in device memory, each with its own buffers; max_l >= every l)
+void kn_step_grouped(const KnStep *steps, int count, int max_l, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_chol.cu
 enum CholMode { kCholFactor = 0, kCholInverse = 1 };
