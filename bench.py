@@ -197,6 +197,101 @@ def config_dict(w):
 
 
 # ------------------------------------------------------------------------------ B200 arm
+BATCH = dict(count=256, m=(512, 8192), n=(256, 4096), k=(8, 16, 32, 64), N=8, noise=1e-4, seed=4)
+
+
+def batch_main(args):
+    """Batched uneven solves: 256 FP32 matrices, m log-uniform in [512, 8192], n log-uniform in
+    [256, 4096] with n <= m, each rank 4k with a geometric spectrum (1 .. 1e-3) plus noise, k in
+    {8, 16, 32, 64}, p = k/2, N = 8, GP / GR / KN / GR.  One line: the batch (isvd_sBatchIsvd, inputs
+    resident, device-timed over K solves after W warm-up solves) beside the same 256 matrices solved
+    one after another through isvd_sIsvd_ex (NATIVE FP32, one pass)."""
+    import torch
+    import isvd_b200
+    from isvd_b200.capi import c_int_t
+    dev = torch.device("cuda", 0)
+    lib = isvd_b200.load()
+    rng = np.random.default_rng(BATCH["seed"])
+    gen = torch.Generator(device=dev).manual_seed(BATCH["seed"])
+    mats = []
+    for _ in range(BATCH["count"]):
+        m = int(np.exp(rng.uniform(np.log(BATCH["m"][0]), np.log(BATCH["m"][1]))))
+        n = int(np.exp(rng.uniform(np.log(BATCH["n"][0]), np.log(min(m, BATCH["n"][1])))))
+        k = int(rng.choice(BATCH["k"]))
+        p = k // 2
+        r = min(n, 4 * k)
+        u = torch.linalg.qr(torch.randn(m, r, device=dev, generator=gen))[0]
+        v = torch.linalg.qr(torch.randn(n, r, device=dev, generator=gen))[0]
+        sig = torch.logspace(0, -3, r, device=dev)
+        a = ((u * sig) @ v.T + BATCH["noise"] * torch.randn(m, n, device=dev, generator=gen)).contiguous()
+        l = k + p
+        mats.append(dict(m=m, n=n, k=k, p=p, a=a, s=torch.zeros(l, device=dev), ut=torch.zeros((m, l), device=dev),
+                         vt=torch.zeros((n, l), device=dev)))
+    torch.cuda.synchronize()
+    B, N = len(mats), BATCH["N"]
+    vp = ctypes.c_void_p
+    arr = lambda vals, ct=c_int_t: (ct * len(vals))(*vals)
+    create = lib.lib.isvd_sBatchCreate
+    create.argtypes = [c_int_t, vp, vp, vp, vp, c_int_t]
+    create.restype = vp
+    solve_b = lib.lib.isvd_sBatchIsvd
+    solve_b.argtypes = [vp] * 10 + [c_int_t, vp, vp]
+    solve_b.restype = ctypes.c_int
+    batch = create(B, arr([d["m"] for d in mats]), arr([d["n"] for d in mats]), arr([d["k"] for d in mats]),
+                   arr([d["p"] for d in mats]), N)
+    assert batch, lib.last_error()
+    seeds = [11 + i for i in range(B)]
+    argv = np.asarray([256, 1e-4], dtype=np.float32)
+    its = arr([0] * B)
+    call = lambda: solve_b(batch, arr([d["a"].data_ptr() for d in mats], vp), arr([d["n"] for d in mats]),
+                           arr([d["s"].data_ptr() for d in mats], vp), arr([d["ut"].data_ptr() for d in mats], vp),
+                           arr([d["ut"].shape[1] for d in mats]), arr([d["vt"].data_ptr() for d in mats], vp),
+                           arr([d["vt"].shape[1] for d in mats]), arr(seeds), argv.ctypes.data, 2, its, None)
+    for _ in range(max(3, args.warmup)):
+        assert call() == 0, lib.last_error()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = lib.lib.isvd_gpu_kernel_launch_count()
+    e0.record()
+    for _ in range(args.steps):
+        assert call() == 0, lib.last_error()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = (lib.lib.isvd_gpu_kernel_launch_count() - l0) // args.steps
+    ms_batch = e0.elapsed_time(e1) / args.steps
+    s_batch = [d["s"].clone() for d in mats]
+    it_batch = list(its)
+    # the same matrices, one single solve each
+    e0.record()
+    it_seq = []
+    for i, d in enumerate(mats):
+        prm = lib.create_param(d["m"], d["n"], d["k"], d["p"], N)
+        l = d["k"] + d["p"]
+        retv, _, st = lib.isvd("s", prm, ("GP", "GR", "KN", "GR"), d["a"], d["n"], d["s"], d["ut"], l, d["vt"], l,
+                               seed=seeds[i], argv=[None, None, [256, 1e-4], None], retc=(0, 0, 2, 0), precision=0)
+        assert st == 0, lib.last_error()
+        it_seq.append(int(retv[2][0]))
+    e1.record()
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    err = max(float(((s_batch[i] - d["s"]).abs().max() / d["s"].abs().max()).item()) for i, d in enumerate(mats))
+    lib.lib.isvd_gpu_batch_destroy(ctypes.c_void_p(batch))
+    out = {
+        "metric": "batched iSVD matrices/s (256 uneven FP32 matrices)", "value": B / (ms_batch / 1e3),
+        "unit": "matrix/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+        "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "fp32 (fp64 l x l)", "data": "synthetic",
+        "config": {"workload": "256 matrices, m log-uniform [512, 8192], n log-uniform [256, 4096] (n <= m), "
+                               "rank 4k geometric 1..1e-3 + 1e-4 noise, k in {8,16,32,64}, p = k/2, N = 8, GP/GR/KN/GR",
+                   "total_elements": int(sum(d["m"] * d["n"] for d in mats)), "seed": BATCH["seed"]},
+        "gpu_launches": int(launches),
+        "sequential": {"ms": ms_seq, "value": B / (ms_seq / 1e3), "path": "isvd_sIsvd_ex per matrix, NATIVE FP32"},
+        "speedup_vs_sequential": ms_seq / ms_batch,
+        "sigma_rel_diff_max": err,
+        "kn_iterations_equal": sum(int(a == b) for a, b in zip(it_batch, it_seq)),
+    }
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -209,7 +304,11 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--single", action="store_true",
                     help="one MIXED solve and its stage times, nothing else (for ncu launch lists / captures)")
+    ap.add_argument("--batched", action="store_true",
+                    help="the batched-solves workload (256 uneven matrices) instead of the single large solve")
     args = ap.parse_args()
+    if args.batched:
+        return batch_main(args)
     w = WORKLOADS[args.size]
     if args.impl == "reference":
         return reference_arm(args, w)
