@@ -105,6 +105,56 @@ __global__ void __launch_bounds__(kCholThreads)
   }
 }
 
+// out = out_scale A^-1 for A = alpha W + shift I (upper triangle of W, n x n, one CTA per matrix) by
+// the sweep operator (Goodnight, "A tutorial on the SWEEP operator", Amer. Statist. 33 (1979)):
+// sweeping pivot k maps a_kk -> -1/a_kk, a_ik -> a_ik/a_kk, a_ij -> a_ij - a_ik a_kj / a_kk; after
+// all pivots the matrix is -A^-1.  For a symmetric positive definite A the pivots are the Cholesky
+// pivots (Schur-complement diagonals), so the elimination needs no pivoting; one pivot that is not
+// above piv_rel times its starting diagonal value sets *status = kStatusNotPD.  Symmetry halves the
+// per-pivot reads: row k equals column k.
+constexpr int kSwThreads = 1024;
+
+__global__ void __launch_bounds__(kSwThreads)
+    spd_inverse_kernel(int n, const double *__restrict__ W, double alpha, double shift, double piv_rel,
+                       double *__restrict__ out, double out_scale, int *status) {
+  extern __shared__ double sm[];
+  const int ld = n + 1, tid = threadIdx.x;
+  double *A = sm, *col = sm + (size_t)n * ld, *diag0 = col + n;
+  const double *w = W + (size_t)blockIdx.x * n * n;
+  const int tx = tid & 31, ty = tid >> 5;  // element (ty + 32 a, tx + 32 b)
+  for (int i = ty; i < n; i += 32)
+    for (int j = tx; j < n; j += 32) {
+      const double v = alpha * ((i <= j) ? w[(size_t)i * n + j] : w[(size_t)j * n + i]) + (i == j ? shift : 0.0);
+      A[i * ld + j] = v;
+      if (i == j) diag0[i] = v;
+    }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    for (int i = tid; i < n; i += kSwThreads) col[i] = A[i * ld + k];
+    __syncthreads();
+    const double d = col[k];
+    if (!(d > piv_rel * diag0[k]) || !(d > 0.0) || !(d < INFINITY)) {  // same decision in every thread
+      if (tid == 0) atomicExch(status, kStatusNotPD);
+      return;
+    }
+    const double inv = 1.0 / d;
+    for (int i = ty; i < n; i += 32) {
+      const double ci = col[i];
+      for (int j = tx; j < n; j += 32) {
+        double v;
+        if (i == k) v = (j == k) ? -inv : col[j] * inv;
+        else if (j == k) v = ci * inv;
+        else v = A[i * ld + j] - ci * col[j] * inv;
+        A[i * ld + j] = v;
+      }
+    }
+    __syncthreads();
+  }
+  double *o = out + (size_t)blockIdx.x * n * n;
+  for (int i = ty; i < n; i += 32)
+    for (int j = tx; j < n; j += 32) o[(size_t)i * n + j] = -out_scale * A[i * ld + j];
+}
+
 // Householder sign rule.  P = Qtop X is the top n x n block of the next Q factor (positive-
 // diagonal convention).  A Householder QR (LAPACK geqrf / gelqf) of the same matrix returns
 // Q diag(s) with s_j = -sign(pivot_j) of the LU factorization of P - diag(s) carried out with
@@ -144,23 +194,35 @@ __global__ void __launch_bounds__(kCholThreads)
   for (int e = tid; e < n * n; e += nt) x[e] *= sg[e % n];
 }
 
-constexpr int kDotThreads = 1024;
+constexpr int kDotThreads = 256;
+constexpr int kDotBlocks = 64;  // CTAs per job; partial sums combined in a fixed order
 
-__global__ void __launch_bounds__(kDotThreads) dots_kernel(DotJobs jobs, double *__restrict__ out) {
+// Partial sums: CTA (x, job) sums the entries x, x + kDotBlocks, ... (in units of its thread count).
+__global__ void __launch_bounds__(kDotThreads) dots_kernel(DotJobs jobs, double *__restrict__ partial) {
   __shared__ double red[kDotThreads / 32];
-  const DotJob jb = jobs.job[blockIdx.x];
+  const DotJob jb = jobs.job[blockIdx.y];
+  const long long stride = (long long)gridDim.x * blockDim.x;
   double v = 0.0;
   if (jb.trace) {
-    for (long long i = threadIdx.x; i < jb.n; i += blockDim.x) v += jb.a[i * jb.n + i];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < jb.n; i += stride) v += jb.a[i * jb.n + i];
   } else {
-    for (long long i = threadIdx.x; i < jb.n; i += blockDim.x) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < jb.n; i += stride) {
       const double x = jb.a[i] - (jb.b ? jb.b[i] : 0.0);
       const double y = jb.c[i] - (jb.d ? jb.d[i] : 0.0);
       v += x * y;
     }
   }
   v = block_sum(v, red);
-  if (threadIdx.x == 0) out[blockIdx.x] = v;
+  if (threadIdx.x == 0) partial[blockIdx.y * gridDim.x + blockIdx.x] = v;
+}
+
+__global__ void dots_final_kernel(const double *__restrict__ partial, int nblocks, int count, double *__restrict__ out) {
+  const int j = threadIdx.x;
+  if (j < count) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[j * nblocks + b];
+    out[j] = s;
+  }
 }
 
 // (out may alias x or y: each entry is read and written by the same thread)
@@ -200,6 +262,14 @@ size_t chol_smem(int n) { return ((size_t)n * (n + 1) + n) * sizeof(double); }
 void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
                       double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st) {
   if (n <= 0 || batch <= 0) return;
+  if (mode == kCholInverse && shift_rel == 0.0) {  // the full inverse: sweep operator, fewer dependent steps
+    const size_t smem = ((size_t)n * (n + 1) + 2 * n) * sizeof(double);
+    if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "SPD inverse: l = %d exceeds on-chip capacity", n);
+    CK(cudaFuncSetAttribute(spd_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    spd_inverse_kernel<<<batch, kSwThreads, smem, st>>>(n, W, alpha, shift_abs, piv_rel, out, out_scale, status);
+    KLAUNCHED();
+    return;
+  }
   const size_t smem = chol_smem(n);
   if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "Cholesky: l = %d exceeds on-chip capacity", n);
   CK(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -221,7 +291,10 @@ void hh_sign_batched(int n, int batch, const T *Q, long long q_ld, long long q_b
 void dots(const DotJobs &jobs, double *out, cudaStream_t st) {
   if (jobs.count <= 0) return;
   if (jobs.count > kMaxDotJobs) fail(kErrArgument, "dots: %d jobs > %d", jobs.count, kMaxDotJobs);
-  dots_kernel<<<jobs.count, kDotThreads, 0, st>>>(jobs, out);
+  DBuf<double> partial((size_t)kDotBlocks * jobs.count);
+  dots_kernel<<<dim3(kDotBlocks, jobs.count), kDotThreads, 0, st>>>(jobs, partial.p);
+  KLAUNCHED();
+  dots_final_kernel<<<1, 32, 0, st>>>(partial.p, kDotBlocks, jobs.count, out);
   KLAUNCHED();
 }
 

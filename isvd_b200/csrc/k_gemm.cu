@@ -248,10 +248,13 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
   const bool b_nc = (g.b_cs == 1);
   if (!a_kc && g.a_rs != 1) fail(kErrArgument, "gemm: operand A has no unit stride");
   if (!b_nc && g.b_rs != 1) fail(kErrArgument, "gemm: operand B has no unit stride");
-  // 128 x 128 tiles when they fill the GPU; otherwise 64 x 64 tiles (4x more CTAs)
+  // 128 x 128 tiles when they fill the GPU, or when a long inner dimension lets split-K fill it
+  // (8 x 8 register blocks: half the shared-memory reads per FMA of 64 x 64 tiles); otherwise
+  // 64 x 64 tiles (4x more CTAs)
   const long long tiles128 = (long long)((g.M + 127) / 128) * ((g.N + 127) / 128) * g.batch;
   const int sms = Runtime::get().num_sms;
-  if (g.M <= 64 || g.N <= 64 || tiles128 < 2LL * sms)
+  const bool long_k = g.splits <= 0 && (long long)g.K >= 2048 && tiles128 * (g.K / 1024) >= 2LL * sms;
+  if (g.M <= 64 || g.N <= 64 || (tiles128 < 2LL * sms && !long_k))
     launch<T, Tout, 64, 64, 16>(g, a_kc, b_nc, st);
   else
     launch<T, Tout, 128, 128, 16>(g, a_kc, b_nc, st);
