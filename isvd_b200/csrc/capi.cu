@@ -489,7 +489,12 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   } else {
     // KN and WY form G = Qs' Qs anyway: they take over the second pass in the coordinates of G
     c.sc.deferred_orth = (bi == "KN" || bi == "WY");
+    // KN, WY and HR are equivariant under Q_i -> Q_i R_i and GR / SY postprocessing is invariant,
+    // so the blocks' bases are free: Cholesky factors instead of eigendecompositions.  (The TS
+    // postprocessing of the reference depends on the basis of Qbar, so it keeps the eigenbasis.)
+    c.sc.chol_basis = (bp != "TS");
     orth_gramian_dev<T>(c.sc, m, l, N, Y.p, Nl);
+    c.sc.chol_basis = false;
   }
   tm.mark(2, st);
   sync();

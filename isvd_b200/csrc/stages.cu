@@ -85,10 +85,27 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
     g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
     gemm(g, c.st);
   }
-  // eig(W_i) = W_i S_i^2 W_i'  (gesvd 'O' of the PSD Gram: |lambda| descending, :88-91)
-  sym_eig_batched(l, N, W.p, V.p, w.p, +1, true, c.status, c.st);
   DBuf<T> Wp(N * ll);
-  if (!polar) {
+  bool done = false;
+  if (c.chol_basis) {
+    // F = R^-1 with R'R = W_i (Cholesky): another orthonormal basis of span(Y_i), for callers
+    // whose result does not depend on the basis; falls back to the eigenbasis when W_i is too
+    // ill-conditioned for a Cholesky factor
+    DBuf<int> bad(1);
+    CK(cudaMemsetAsync(bad.p, 0, sizeof(int), c.st));
+    chol_inv_batched(l, N, W.p, 1.0, 0.0, 0.0, l * 0x1p-52, V.p, 1.0, kCholFactor, bad.p, c.st);
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, bad.p, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaStreamSynchronize(c.st));
+    if (!h) {
+      copy2d<double, T>(V.p, l, 1, Wp.p, l, 1, (long long)N * l, l, c.st);
+      done = true;
+    }
+  }
+  // eig(W_i) = W_i S_i^2 W_i'  (gesvd 'O' of the PSD Gram: |lambda| descending, :88-91)
+  if (!done) sym_eig_batched(l, N, W.p, V.p, w.p, +1, true, c.status, c.st);
+  if (done) {
+  } else if (!polar) {
     // W_i / S_i with S = sqrt(s)  (:94)
     scale_cols_batched<double, T>(V.p, l, Wp.p, l, (long long)N * l, l, l, w.p, kScaleInvSqrt, c.st);
   } else {

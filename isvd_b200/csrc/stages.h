@@ -18,6 +18,9 @@ struct StageCtx {
   // MIXED driver: the second (polar) pass of the Gramian orthogonalization is left to the
   // integration, which re-orthonormalizes the blocks in the coordinates of G (coeff_orthonormalize)
   bool deferred_orth = false;
+  // Gramian orthogonalization may return any orthonormal basis of each span(Y_i) (Cholesky factor
+  // instead of the eigenbasis): set by the driver when the rest of the pipeline is basis-invariant
+  bool chol_basis = false;
 };
 
 struct IterResult {
