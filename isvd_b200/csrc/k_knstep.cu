@@ -35,21 +35,26 @@ namespace {
 constexpr int kKsThreads = 1024;  // one output of a 32 x 32 tile per thread
 constexpr int kKsMaxL = 160;
 constexpr int kAld = kKsMaxL + 1;  // shared-memory row stride of the A tile (32 x l)
-constexpr int kBld = 33;           // shared-memory row stride of the B tile (l x 32)
+constexpr int kBld = 34;           // shared-memory row stride of the B tile (l x 32; even: 16-byte pairs)
 constexpr int kKsPer = (32 * kKsMaxL + kKsThreads - 1) / kKsThreads;
 
 struct Ks {
   int l, nr, cs, rank;
-  double *As, *Bs;
+  double *As, *Bs, *part;
 };
 
 // C = alpha A B + beta Cin + diag I on the 32 x 32 output tiles [tile_begin, tile_end) of a phase
 // (tiles numbered across the products of the phase); CTA r takes the tiles t = r mod cs.
 // Row-major l x l operands; every load goes through L2 (__ldcg), as they are written by other CTAs.
+// Inner loop: four quarters of the inner dimension x 256 threads, each with a 2 x 2 output block
+// (three shared-memory loads per four FMAs); the quarters' partial sums meet in shared memory and
+// are added in a fixed order.
 __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, const double *A, const double *B,
                       double beta, const double *Cin, double diag, double *C) {
   const int l = k.l, tid = threadIdx.x;
-  const int ty = tid >> 5, tx = tid & 31;  // output (ty, tx) of the tile
+  const int ty = tid >> 5, tx = tid & 31;                    // output (ty, tx) of the tile in the epilogue
+  const int qk = tid >> 8, bi = (tid & 255) >> 4, bj = tid & 15;  // quarter, 2 x 2 block of the inner loop
+  const int kq = (l + 3) >> 2, kb = qk * kq, ke = min(l, kb + kq);
   const int first = tile_begin + (((k.rank - tile_begin) % k.cs) + k.cs) % k.cs;
   for (int t = first; t < tile_end; t += k.cs) {
     const int tt = t - tile_begin;
@@ -62,8 +67,8 @@ __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, c
       const int e = tid + u * kKsThreads;
       const int r = e / l, kk = e - r * l;  // A tile: 32 rows x l
       ra[u] = (e < 32 * l && i0 + r < l) ? __ldcg(A + (size_t)(i0 + r) * l + kk) : 0.0;
-      const int kb = e >> 5, cb = e & 31;   // B tile: l rows x 32
-      rb[u] = (e < 32 * l && j0 + cb < l) ? __ldcg(B + (size_t)kb * l + j0 + cb) : 0.0;
+      const int kr = e >> 5, cb = e & 31;   // B tile: l rows x 32
+      rb[u] = (e < 32 * l && j0 + cb < l) ? __ldcg(B + (size_t)kr * l + j0 + cb) : 0.0;
     }
     __syncthreads();  // the previous tile's shared memory reads are done
 #pragma unroll
@@ -76,16 +81,26 @@ __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, c
       }
     }
     __syncthreads();
-    double acc0 = 0.0, acc1 = 0.0;  // two chains over even / odd k
-    const double *ar = k.As + ty * kAld;
-    const double *br = k.Bs + tx;
-    int kk = 0;
-    for (; kk + 1 < l; kk += 2) {
-      acc0 = fma(ar[kk], br[kk * kBld], acc0);
-      acc1 = fma(ar[kk + 1], br[(kk + 1) * kBld], acc1);
+    double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
+    const double *a0 = k.As + (2 * bi) * kAld, *a1 = a0 + kAld;
+    const double *bp = k.Bs + 2 * bj;
+    for (int kk = kb; kk < ke; ++kk) {
+      const double x0 = a0[kk], x1 = a1[kk];
+      const double2 y = *reinterpret_cast<const double2 *>(bp + kk * kBld);
+      c00 = fma(x0, y.x, c00);
+      c01 = fma(x0, y.y, c01);
+      c10 = fma(x1, y.x, c10);
+      c11 = fma(x1, y.y, c11);
     }
-    if (kk < l) acc0 = fma(ar[kk], br[kk * kBld], acc0);
-    if (i < l && j < l) C[(size_t)i * l + j] = alpha * (acc0 + acc1) + beta * cin + (i == j ? diag : 0.0);
+    double *part = k.part + qk * 1024;  // 32 x 32 partial sums of this quarter
+    part[(2 * bi) * 32 + 2 * bj] = c00;
+    part[(2 * bi) * 32 + 2 * bj + 1] = c01;
+    part[(2 * bi + 1) * 32 + 2 * bj] = c10;
+    part[(2 * bi + 1) * 32 + 2 * bj + 1] = c11;
+    __syncthreads();
+    const int o = ty * 32 + tx;
+    const double acc = (k.part[o] + k.part[1024 + o]) + (k.part[2048 + o] + k.part[3072 + o]);
+    if (i < l && j < l) C[(size_t)i * l + j] = alpha * acc + beta * cin + (i == j ? diag : 0.0);
   }
 }
 
@@ -157,7 +172,8 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
   cg::cluster_group cluster = cg::this_cluster();
   const int l = a.l;
   const size_t ll = (size_t)l * l;
-  Ks k{l, (l + 31) / 32, (int)cluster.num_blocks(), (int)cluster.block_rank(), sm, sm + 32 * kAld};
+  Ks k{l, (l + 31) / 32, (int)cluster.num_blocks(), (int)cluster.block_rank(), sm, sm + 32 * kAld,
+         sm + 32 * kAld + kKsMaxL * kBld};
   const int nt = k.nr * k.nr;
   const int gtid = k.rank * kKsThreads + threadIdx.x, gstride = k.cs * kKsThreads;
   // work: Z | P_1..P_8 | accC x2 | accCi x2 | BC_0..BC_7 | BI_0..BI_7 (Newton-Schulz: P_1..P_5), then
@@ -321,7 +337,7 @@ KnSeries make_series() {
   return s;
 }
 
-constexpr size_t kKsSmem = (size_t)(32 * kAld + kKsMaxL * kBld) * sizeof(double);
+constexpr size_t kKsSmem = (size_t)(32 * kAld + kKsMaxL * kBld + 4 * 1024) * sizeof(double);
 int g_cluster_size = -1;  // -1: not decided yet; 0: no cluster launch possible
 
 int choose_cluster_size(const KnStep &a, cudaStream_t st) {
