@@ -31,8 +31,9 @@ void isvd_gpu_clear_error( void );
 
 /* ---------------------------------------------------------------- precision */
 #define ISVD_GPU_PRECISION_NATIVE   0  /* products in the routine's own type (FP64 for isvd_d*, FP32 for isvd_s*) */
-#define ISVD_GPU_PRECISION_MIXED    1  /* BF16x3 split products on tcgen05 tensor cores, FP32 accumulation;
-                                          l x l steps (eigensolves, inverse square roots, small SVDs) in FP64 */
+#define ISVD_GPU_PRECISION_MIXED    1  /* bf16 split products (2 or 3 planes per operand) on tcgen05 tensor
+                                          cores, FP32 accumulation; l x l steps (eigensolves, inverse square
+                                          roots, small SVDs) in FP64 */
 
 /* Process-wide default precision.  Initial value: ISVD_GPU_PRECISION_NATIVE, or the value
  * of the environment variable ISVD_GPU_PRECISION ("native" / "mixed") at first use. */

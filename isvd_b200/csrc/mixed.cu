@@ -2,7 +2,13 @@
 // the large dimensions; FP64 for every l x l step (done by the callers in stages.cu).
 //
 // Plane counts per product (relative error of one product term, before FP32 accumulation):
-//   sketch       A: 3 planes (exact for FP32 A)  x  Omega: 1 exact bf16 plane, or 3 when passed in
+//   sketch       A: 2 planes (16 significant bits; ISVD_GPU_SKETCH_PLANES=3 keeps FP32 A exact)
+//                x  Omega: 1 exact bf16 plane, or 3 when passed in.  Two planes leave a relative
+//                error of at most 2^-17 per element of A (TF32 keeps 2^-11); its effect on each
+//                entry of Y = A Omega averages over the n-long inner products to about that of an
+//                FP32 GEMM's own rounding at n ~ 1e4, and the sketch only fixes the subspace, whose
+//                Rayleigh-Ritz values (the postprocess) move by the square of a subspace
+//                perturbation.
 //   block Gram   Y': 3 x 3 planes, 6 products  (W feeds the orthogonalizing eigensolve)
 //   G = Qs' Qs   2 x 2 planes, 3 products      (errors average over the m-long inner products)
 //   Z = A' Qbar  Qbar': 2 planes x A: 2 planes, 3 products
@@ -60,7 +66,17 @@ static long long panel_rows(long long m, long long n, size_t elem) {
   return std::min<long long>(p, m);
 }
 
-// Sketch Y = A Omega with A processed in row panels: each panel is split into A's three bf16 planes
+// bf16 planes of A used by the sketch (2, or 3 with ISVD_GPU_SKETCH_PLANES=3); the postprocess
+// reads the first two.
+static int sketch_planes() {
+  static const int np = [] {
+    const char *e = getenv("ISVD_GPU_SKETCH_PLANES");
+    return (e && atoi(e) == 3) ? 3 : 2;
+  }();
+  return np;
+}
+
+// Sketch Y = A Omega with A processed in row panels: each panel is split into A's bf16 planes
 // (kept for the postprocess) and multiplied by Omega' on the tensor cores.  When A is in host
 // memory, panel p + 1 is copied to the device on the copy stream while panel p is split and
 // multiplied, so that the PCIe transfer overlaps the tensor-core work (the reference streams A in
@@ -74,12 +90,13 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
   const long long ld = plane_ld(n), rp = plane_rows(m), ps = rp * ld;
   MixedCache local;
   MixedCache *mc = c.cache ? c.cache : &local;
-  mc->buf.alloc((size_t)3 * ps);
-  for (int q = 0; q < 3; ++q)  // zero rows [m, rp): TMA boxes of the last tile read them
+  const int na = sketch_planes();
+  mc->buf.alloc((size_t)na * ps);
+  for (int q = 0; q < na; ++q)  // zero rows [m, rp): TMA boxes of the last tile read them
     if (rp > m)
       CK(cudaMemsetAsync(mc->buf.p + (size_t)q * ps + (size_t)m * ld, 0, (size_t)(rp - m) * ld * 2, c.st));
   Planes all;
-  all.ptr = mc->buf.p; all.np = 3; all.rows = m; all.cols = n; all.ld = ld; all.plane_stride = ps;
+  all.ptr = mc->buf.p; all.np = na; all.rows = m; all.cols = n; all.ld = ld; all.plane_stride = ps;
   PlaneBuf om;
   if (!omega) {
     const long long old = plane_ld(n), orp = plane_rows(Nl);
@@ -107,8 +124,8 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     const long long rows = std::min<long long>(P, m - r0);
     __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
     if (a_dev) {
-      if (ordera == 'R') split_rows<T>(a + r0 * lda, lda, 1, rows, n, 3, false, dst, ld, ps, c.st);
-      else split_rows<T>(a + r0, lda, 1, n, rows, 3, true, dst, ld, ps, c.st);  // A' rows r0.. as n x rows
+      if (ordera == 'R') split_rows<T>(a + r0 * lda, lda, 1, rows, n, na, false, dst, ld, ps, c.st);
+      else split_rows<T>(a + r0, lda, 1, n, rows, na, true, dst, ld, ps, c.st);  // A' rows r0.. as n x rows
     } else {
       const int b = p & 1;
       if (p >= 2) CK(cudaStreamWaitEvent(rt.copy_stream, consumed[b], 0));
@@ -121,8 +138,8 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
       }
       CK(cudaEventRecord(copied[b], rt.copy_stream));
       CK(cudaStreamWaitEvent(c.st, copied[b], 0));
-      if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, 3, false, dst, ld, ps, c.st);
-      else split_rows<T>(stage[b].p, rows, 1, n, rows, 3, true, dst, ld, ps, c.st);
+      if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, na, false, dst, ld, ps, c.st);
+      else split_rows<T>(stage[b].p, rows, 1, n, rows, na, true, dst, ld, ps, c.st);
       CK(cudaEventRecord(consumed[b], c.st));
     }
     Planes ap = all;
@@ -131,7 +148,7 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     UmmaGemm g;
     g.M = (int)rows; g.N = Nl; g.K = n;
     g.A = ap; g.B = om.P;
-    set_products(g, 3, om.P.np);
+    set_products(g, na, om.P.np);
     g.C = y + r0 * ldy; g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
     g.status = c.status;
     g.tag = "sketch";

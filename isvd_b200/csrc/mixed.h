@@ -1,4 +1,4 @@
-// MIXED precision engine: BF16x3 split products on tcgen05 tensor cores with FP32 accumulation.
+// MIXED precision engine: bf16 split products on tcgen05 tensor cores with FP32 accumulation.
 // Each FP32/FP64 operand x is split into bf16 pieces x = x0 + x1 + x2 (+ residual); a product
 // keeps the piece pairs whose combined magnitude is above the FP32 rounding level.
 #pragma once
@@ -42,7 +42,8 @@ struct MixedCache {
 };
 
 // Y = A * Omega (m x Nl, row-major ldy).  omega == nullptr: Omega is drawn exactly in bf16
-// (Philox + Box-Muller, rounded), so only A is split (3 products).  Otherwise Omega is split too.
+// (Philox + Box-Muller, rounded), so only A is split (2 products, one per A plane).  Otherwise
+// Omega is split too.
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                   long long ldom, uint64_t seed, T *y, long long ldy);

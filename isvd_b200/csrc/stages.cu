@@ -1,6 +1,6 @@
 // Device-level iSVD stages (one MPI rank).  NATIVE precision: products in the stage's type on
 // CUDA cores; l x l steps in FP64.  MIXED precision routes the large products to the tcgen05
-// BF16x3 engine (mixed.cu).
+// bf16 split-product engine (mixed.cu).
 #include <cmath>
 #include <vector>
 

@@ -53,7 +53,7 @@ constexpr double unit_roundoff() {
 //   pass 0: W = Y'Y,  R'R = W + s I with s = (sqrt(rows) + l + 1) u trace(W),  Y := Y R^-1
 //   pass 1, 2: the same without shift (CholeskyQR2 on the now well-conditioned panels); the last
 //   R^-1 carries the Householder column signs.
-// MIXED precision takes the Gram matrices and products from the BF16x3 tensor-core engine.
+// MIXED precision takes the Gram matrices and products from the bf16 split-product tensor-core engine.
 template <class T>
 void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long long ldy) {
   const int Nl = N * l;

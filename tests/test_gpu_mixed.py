@@ -1,4 +1,4 @@
-"""MIXED precision (BF16x3 planes on tcgen05 tensor cores, FP32 accumulation, FP64 l x l steps)
+"""MIXED precision (bf16 split planes on tcgen05 tensor cores, FP32 accumulation, FP64 l x l steps)
 against FP64: every stage on the reference goldens, and end to end against the FP64 path with
 the same Omega.  Tolerance: singular values within 1e-5 relative, largest principal angle of U
 and V within 1e-4 (the mixed-precision bar); products within FP32 rounding (1e-6 relative)."""

@@ -158,7 +158,7 @@ def test_driver_qr_wy_matches_reference(lib, reflib, oracle, algs):
 
 @pytest.mark.parametrize("algs", [("GP", "TS", "WY", "GR"), ("GP", "TS", "KN", "TS")])
 def test_driver_qr_wy_mixed(lib, oracle, algs):
-    """MIXED precision (BF16x3 tensor-core products) against the FP64 path on FP32 input."""
+    """MIXED precision (bf16 split tensor-core products) against the FP64 path on FP32 input."""
     m, n, k, p, N = 4000, 2000, 16, 16, 8
     l = k + p
     a = lowrank(m, n, 600, 0.99, 1e-5, seed=33).astype(np.float32)
