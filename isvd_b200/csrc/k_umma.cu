@@ -29,7 +29,9 @@ constexpr int BM = 128;
 constexpr int kThreads = 320;
 constexpr int kEpiWarps = 8;
 constexpr int kChunkK = 128;  // K depth of one tensor-memory accumulation chunk
-constexpr long long kWaitLimit = 1LL << 23;
+constexpr long long kWaitLimit = 1LL << 23;       // iterations of an unsuspended poll (drains)
+constexpr unsigned long long kWaitNs = 4000000000ull;  // wall-clock bound of one pipeline wait
+constexpr uint32_t kSuspendNs = 1000000;             // suspension cap of one try_wait
 
 struct KParams {
   int M, N, K;
@@ -46,6 +48,8 @@ struct KParams {
   float *partial;
   int upper;  // only tiles intersecting the upper triangle (symmetric output)
   int *status;
+  int chunk_kb;   // k-blocks per tensor-memory accumulation chunk
+  int stage_out;  // epilogue stages its rows through shared memory (C rows contiguous)
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -65,13 +69,30 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait; false on expiry or when another role has aborted.
+// try_wait that suspends the thread (up to kSuspendNs) until the phase completes, so that waiting
+// warps take no issue slots from the MMA and TMA threads that share their sub-partition.
+__device__ __forceinline__ bool mbar_try_susp(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity), "r"(kSuspendNs)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Bounded wait (kWaitNs of wall clock); false on expiry or when another role has aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
-  for (long long i = 0; i < kWaitLimit; ++i) {
-    if (mbar_try(bar, parity)) return true;
-    if ((i & 255) == 255 && *abort_flag) return false;
+  if (mbar_try_susp(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_susp(bar, parity)) return true;
+    if (*abort_flag || global_ns() - t0 > kWaitNs) return false;
   }
-  return false;
 }
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
@@ -108,6 +129,27 @@ __device__ __forceinline__ void umma_commit(uint64_t *bar) {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// 32 consecutive columns of this warp's 32 lanes; completes at the caller's tmem_wait().
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   uint32_t r[8];
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
@@ -125,7 +167,6 @@ struct Cfg {
   static constexpr uint32_t A_LAYOUT = (BK == 64) ? 2u : 4u;   // SWIZZLE_128B / SWIZZLE_64B
   static constexpr uint32_t A_SBO = (BK == 64) ? 1024u : 512u;  // 8 rows of BK bf16
   static constexpr int TMEM_COLS = (2 * BN <= 64) ? 64 : (2 * BN <= 128) ? 128 : (2 * BN <= 256) ? 256 : 512;
-  static constexpr int CHUNK = (kChunkK / BK) > 0 ? (kChunkK / BK) : 1;  // k-blocks per chunk
   static constexpr int HALF = BN / 2;                                      // columns per epilogue warp
 };
 
@@ -178,10 +219,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------------- TMA producer
     const int a_row = (int)(b * p.a_mn_step) + m0;
     const int b_row = (int)(b * p.b_mn_step) + n0;
-    int issued = 0;
+    int issued = 0, s = 0;
+    uint32_t ph = 1;  // parity of the empty phase to wait for (first pass: none)
     for (int kb = 0; kb < nkb; ++kb) {
-      const int s = kb % stages;
-      if (kb >= stages && !mbar_wait(&empty[s], ((kb / stages) & 1) ^ 1, abort_flag)) {
+      if (kb >= stages && !mbar_try(&empty[s], ph) && !mbar_wait(&empty[s], ph, abort_flag)) {
         *abort_flag = 1;
         break;
       }
@@ -209,6 +250,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       ++issued;
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+      }
     }
     // Drain: every issued load has landed before the CTA can exit (bounded).
     for (int kb = max(0, issued - stages); kb < issued; ++kb) {
@@ -219,12 +264,27 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // ---------------------------------------------------------------- MMA issuer
+    // The tensor core queues about one MMA ahead of this thread, so everything between two MMAs
+    // stalls the pipe: descriptors are precomputed (start-address field + byte offset / 16),
+    // stage and chunk positions are counters, and the full-barrier wait tries once inline first.
     const uint32_t idesc = idesc_bf16(BM, BN, AMN, BMN);
-    int chunk = 0;
-    uint32_t tacc = tmem;
-    bool first = true;
+    const uint64_t dA = AMN ? sdesc(0, BK * 128, 1024, 2u) : sdesc(0, 16, C::A_SBO, C::A_LAYOUT);
+    const uint64_t dB = BMN ? sdesc(0, BK * 128, 1024, 2u) : sdesc(0, 16, C::A_SBO, C::A_LAYOUT);
+    constexpr uint32_t kStepA = AMN ? 2048 / 16 : 32 / 16;  // one K = 16 step, in 16-byte units
+    constexpr uint32_t kStepB = BMN ? 2048 / 16 : 32 / 16;
+    const int nprod = p.nprod;
+    uint32_t aoff[8], boff[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      aoff[i] = (i < nprod) ? (uint32_t)(p.pa[i] * C::A_TILE) >> 4 : 0u;
+      boff[i] = (i < nprod) ? (uint32_t)(p.na * C::A_TILE + p.pb[i] * C::B_TILE) >> 4 : 0u;
+    }
+    const uint32_t smem16 = su32(smem) >> 4, stage16 = (uint32_t)stage_bytes >> 4;
+    const int chunk_kb = p.chunk_kb;
+    int chunk = 0, cleft = 0, s = 0;
+    uint32_t ph = 0, tacc = tmem, accf = 0;
     for (int kb = 0; kb < nkb; ++kb) {
-      if (kb % C::CHUNK == 0) {
+      if (cleft == 0) {
         const int b2 = chunk & 1;
         if (chunk >= 2 && !mbar_wait(&tempty[b2], ((chunk >> 1) & 1) ^ 1, abort_flag)) {
           *abort_flag = 1;
@@ -232,32 +292,35 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         tc_fence_after();
         tacc = tmem + (uint32_t)(b2 * BN);
-        first = true;
+        accf = 0;
+        cleft = chunk_kb;
       }
-      const int s = kb % stages;
-      if (!mbar_wait(&full[s], (kb / stages) & 1, abort_flag)) {
+      if (!mbar_try(&full[s], ph) && !mbar_wait(&full[s], ph, abort_flag)) {
         *abort_flag = 1;
         break;
       }
       tc_fence_after();
-      const uint32_t st = su32(smem + (size_t)s * stage_bytes);
-      for (int i = 0; i < p.nprod; ++i) {
-        const uint32_t a_base = st + p.pa[i] * C::A_TILE;
-        const uint32_t b_base = st + p.na * C::A_TILE + p.pb[i] * C::B_TILE;
+      const uint64_t so = (uint64_t)(smem16 + (uint32_t)s * stage16);
 #pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk) {
-          const uint64_t da = AMN ? sdesc(a_base + kk * 2048, BK * 128, 1024, 2u)
-                                  : sdesc(a_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
-          const uint64_t db = BMN ? sdesc(b_base + kk * 2048, BK * 128, 1024, 2u)
-                                  : sdesc(b_base + kk * 32, 16, C::A_SBO, C::A_LAYOUT);
-          umma_bf16(tacc, da, db, idesc, first ? 0u : 1u);
-          first = false;
+      for (int i = 0; i < 8; ++i) {
+        if (i < nprod) {
+          const uint64_t da = dA + so + aoff[i], db = dB + so + boff[i];
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            umma_bf16(tacc, da + kk * kStepA, db + kk * kStepB, idesc, accf);
+            accf = 1u;
+          }
         }
       }
       umma_commit(&empty[s]);
-      if (kb % C::CHUNK == C::CHUNK - 1 || kb == nkb - 1) {
+      if (--cleft == 0 || kb == nkb - 1) {
         umma_commit(&tfull[chunk & 1]);  // arrives when this chunk's MMAs have completed
         ++chunk;
+        cleft = 0;
+      }
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
       }
     }
   } else if (warp >= 2) {
@@ -265,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;                 // TMEM lane quarter accessible to this warp
     const int h = (warp - 2) >> 2;          // column half
     const int row = q * 32 + lane;
-    const int nchunks = (nkb + C::CHUNK - 1) / C::CHUNK;
+    const int nchunks = (nkb + p.chunk_kb - 1) / p.chunk_kb;
     float acc[C::HALF];
 #pragma unroll
     for (int j = 0; j < C::HALF; ++j) acc[j] = 0.f;
@@ -282,18 +345,44 @@ __global__ void __launch_bounds__(kThreads, 1)
       tc_fence_after();
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b2 * BN + h * C::HALF);
 #pragma unroll
-      for (int j = 0; j < C::HALF; j += 8) {
-        float v[8];
-        tmem_ld8(tbase + (uint32_t)j, v);
+      for (int j = 0; j < C::HALF; j += 16) {
+        uint32_t v[16];
+        tmem_ld16(tbase + (uint32_t)j, v);
+        tmem_wait();
 #pragma unroll
-        for (int i = 0; i < 8; ++i) acc[j + i] += v[i];
+        for (int i = 0; i < 16; ++i) acc[j + i] += __uint_as_float(v[i]);
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(&tempty[b2])) : "memory");
     }
     const int gm = m0 + row;
-    if (ok && gm < p.M) {
+    if (ok && p.stage_out) {
+      // every MMA has completed (last tfull), so every load has landed and the pipeline buffers
+      // are free: each warp transposes its 32 x HALF block through them and writes whole rows
+      constexpr int SROW = C::HALF + 1;
+      float *stg = (float *)smem + (size_t)(warp - 2) * 32 * SROW;
+#pragma unroll
+      for (int j = 0; j < C::HALF; ++j) stg[lane * SROW + j] = acc[j];
+      __syncwarp();
+      for (int r = 0; r < 32; ++r) {
+        const int gr = m0 + q * 32 + r;
+        if (gr >= p.M) break;
+#pragma unroll
+        for (int t = 0; t < C::HALF / 32; ++t) {
+          const int gn = n0 + h * C::HALF + t * 32 + lane;
+          if (gn >= p.N || (p.upper && gn < gr)) continue;
+          const float v = stg[r * SROW + t * 32 + lane];
+          if (p.splits == 1) {
+            const long long off = (long long)b * p.c_step + (long long)gr * p.c_rs + (long long)gn * p.c_cs;
+            if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)v;
+            else ((float *)p.C)[off] = (float)(p.alpha * (double)v);
+          } else {
+            p.partial[(((long long)b * p.splits + split) * p.M + gr) * p.N + gn] = v;
+          }
+        }
+      }
+    } else if (ok && gm < p.M) {
       const bool upper_tile = p.upper != 0;
 #pragma unroll
       for (int j = 0; j < C::HALF; ++j) {
@@ -315,6 +404,292 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)C::TMEM_COLS));
+  }
+}
+
+// ------------------------------------------------------------------ CTA-pair (cta_group::2) GEMM
+// K-major A and B, no batch / split-K / triangle.  The two CTAs of a cluster compute one 256 x 256
+// tile: CTA r (rank in the pair) stages A rows [m0 + 128 r, +128) and B rows [n0 + 128 r, +128) of
+// every plane in its own shared memory, and CTA 0 issues tcgen05.mma.cta_group::2 (M = 256), which
+// reads the A half and both B halves of each CTA.  Each SM thus stages half a B tile per k-block
+// instead of a whole one: shared-memory traffic per MMA drops from A + B to A + B/2 (the one-CTA
+// kernel spends about a quarter of its time with the tensor pipe waiting on shared memory).
+// Barriers: full[s] lives in CTA 0 and receives the bytes of both CTAs' loads; empty[s] and
+// tfull[b] exist in both CTAs and receive one tcgen05.commit each from CTA 0; tempty[b] lives in
+// CTA 0 and counts the epilogue warps of both CTAs (remote arrivals from CTA 1).  The epilogue
+// stages each warp's 32 x 128 FP32 block through the (then idle) pipeline buffers, so the final
+// store writes whole 128-byte rows.
+__device__ __forceinline__ uint32_t cluster_ctarank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// shared::cluster address of the variable at shared::cta address `saddr` in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t mapa_shared(uint32_t saddr, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 "
+      "%0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(su32(bar)), "r"(parity), "r"(kSuspendNs)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *bar, uint32_t parity, volatile int *abort_flag) {
+  if (mbar_try_cluster(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_cluster(bar, parity)) return true;
+    if (*abort_flag || global_ns() - t0 > kWaitNs) return false;
+  }
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar_cluster) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+// TMA load into this CTA's shared memory whose completion is counted on a barrier of either CTA of
+// the pair (bar_cluster: a shared::cluster address); no multicast.
+__device__ __forceinline__ void tma_load_3d_pair(void *dst, const CUtensorMap *map, uint32_t bar_cluster, int x,
+                                                 int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+      "%5}], [%2];" ::"r"(su32(dst)),
+      "l"((uint64_t)map), "r"(bar_cluster), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                               uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::
+          "r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+// Arrives on the barrier at shared::cluster address bar_cluster once this thread's earlier
+// cta_group::2 MMAs have completed.
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar_cluster) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar_cluster)
+               : "memory");
+}
+
+template <int BK>
+__global__ void __launch_bounds__(kThreads, 1)
+    umma_pair_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                     const KParams p, const int stages) {
+  constexpr int HT = BM * BK * 2;  // bytes of one 128-row plane tile (A, or half of B)
+  constexpr uint32_t LAYOUT = (BK == 64) ? 2u : 4u;
+  constexpr uint32_t SBO = (BK == 64) ? 1024u : 512u;
+  const int CHUNK = p.chunk_kb;
+  constexpr int BN2 = 256;         // tile columns (both halves of B)
+  constexpr int HALF = BN2 / 2;    // columns per epilogue warp
+  constexpr int TMEM_COLS = 512;   // two 256-column accumulators
+  constexpr int SROW = HALF + 1;   // staging row stride (floats), conflict-free both ways
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const int stage_bytes = (p.na + p.nb) * HT;
+  uint64_t *full = (uint64_t *)(smem + (size_t)stages * stage_bytes);
+  uint64_t *empty = full + stages;
+  uint64_t *tfull = empty + stages;
+  uint64_t *tempty = tfull + 2;
+  uint64_t *mdone = tempty + 2;
+  uint32_t *tslot = (uint32_t *)(mdone + 1);
+  volatile int *abort_flag = (volatile int *)(tslot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_ctarank();
+  const int nt = blockIdx.x >> 1, pt = blockIdx.y;
+  const int m0 = pt * (2 * BM) + (int)rank * BM, n0 = nt * BN2;
+  const int nkb = p.total_kb;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b2 = 0; b2 < 2; ++b2) {
+      mbar_init(&tfull[b2], 1);
+      mbar_init(&tempty[b2], 2 * kEpiWarps);
+    }
+    mbar_init(mdone, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(tslot)),
+                 "r"((uint32_t)TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  cluster_sync_all();  // barriers of CTA 0 initialised before CTA 1 loads into them
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+
+  if (warp == 0 && lane == 0) {
+    // ---------------------------------------------------------------- TMA producer (both CTAs)
+    const int b_row = n0 + (int)rank * BM;
+    const uint32_t full0 = mapa_shared(su32(full), 0);  // CTA 0's full barriers
+    int issued = 0, s = 0;
+    uint32_t ph = 1;
+    for (int kb = 0; kb < nkb; ++kb) {
+      if (kb >= stages && !mbar_try(&empty[s], ph) && !mbar_wait(&empty[s], ph, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      uint8_t *st = smem + (size_t)s * stage_bytes;
+      const uint32_t fb = full0 + 8u * (uint32_t)s;
+      if (rank == 0) mbar_expect_tx(&full[s], (uint32_t)(2 * stage_bytes));
+      const int k0 = kb * BK;
+      for (int q = 0; q < p.na; ++q) tma_load_3d_pair(st + q * HT, &mapA, fb, k0, m0, q);
+      for (int q = 0; q < p.nb; ++q) tma_load_3d_pair(st + (p.na + q) * HT, &mapB, fb, k0, b_row, q);
+      ++issued;
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+      }
+    }
+    // Drain (CTA 0 holds the barriers): every issued load has landed before the pair can exit.
+    if (rank == 0) {
+      for (int kb = max(0, issued - stages); kb < issued; ++kb) {
+        const int s = kb % stages;
+        long long i = 0;
+        while (!mbar_try(&full[s], (kb / stages) & 1) && ++i < kWaitLimit) {
+        }
+      }
+    }
+  } else if (warp == 1 && lane == 0 && rank == 0) {
+    // ---------------------------------------------------------------- MMA issuer (CTA 0)
+    const uint32_t idesc = idesc_bf16(2 * BM, BN2, false, false);
+    const uint64_t d0 = sdesc(0, 16, SBO, LAYOUT);
+    const int nprod = p.nprod;
+    uint32_t aoff[8], boff[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      aoff[i] = (i < nprod) ? (uint32_t)(p.pa[i] * HT) >> 4 : 0u;
+      boff[i] = (i < nprod) ? (uint32_t)((p.na + p.pb[i]) * HT) >> 4 : 0u;
+    }
+    const uint32_t smem16 = su32(smem) >> 4, stage16 = (uint32_t)stage_bytes >> 4;
+    // shared::cluster addresses of both CTAs' barrier arrays (each CTA's window is contiguous)
+    const uint32_t empty0 = mapa_shared(su32(empty), 0), empty1 = mapa_shared(su32(empty), 1);
+    const uint32_t tfull0 = mapa_shared(su32(tfull), 0), tfull1 = mapa_shared(su32(tfull), 1);
+    int chunk = 0, cleft = 0, s = 0;
+    uint32_t ph = 0, tacc = tmem, accf = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      if (cleft == 0) {
+        const int b2 = chunk & 1;
+        if (chunk >= 2 && !mbar_wait_cluster(&tempty[b2], ((chunk >> 1) & 1) ^ 1, abort_flag)) {
+          *abort_flag = 1;
+          break;
+        }
+        tc_fence_after();
+        tacc = tmem + (uint32_t)(b2 * BN2);
+        accf = 0;
+        cleft = CHUNK;
+      }
+      if (!mbar_try(&full[s], ph) && !mbar_wait(&full[s], ph, abort_flag)) {
+        *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint64_t so = (uint64_t)(smem16 + (uint32_t)s * stage16);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        if (i < nprod) {
+          const uint64_t da = d0 + so + aoff[i], db = d0 + so + boff[i];
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            umma_bf16_pair(tacc, da + kk * 2, db + kk * 2, idesc, accf);
+            accf = 1u;
+          }
+        }
+      }
+      umma_commit_pair(empty0 + 8u * (uint32_t)s);
+      umma_commit_pair(empty1 + 8u * (uint32_t)s);
+      if (--cleft == 0 || kb == nkb - 1) {
+        const int b2 = chunk & 1;
+        umma_commit_pair(tfull0 + 8u * (uint32_t)b2);
+        umma_commit_pair(tfull1 + 8u * (uint32_t)b2);
+        ++chunk;
+        cleft = 0;
+      }
+      if (++s == stages) {
+        s = 0;
+        ph ^= 1u;
+      }
+    }
+    // every MMA (they write both CTAs' tensor memory) has completed before the pair frees it
+    umma_commit_pair(mapa_shared(su32(mdone), 0));
+    long long i = 0;
+    while (!mbar_try(mdone, 0) && ++i < kWaitLimit) {
+    }
+  } else if (warp >= 2) {
+    // ---------------------------------------------------------------- epilogue (both CTAs)
+    const int q = warp & 3;
+    const int h = (warp - 2) >> 2;
+    const int nchunks = (nkb + CHUNK - 1) / CHUNK;
+    float acc[HALF];
+#pragma unroll
+    for (int j = 0; j < HALF; ++j) acc[j] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      const int b2 = c & 1;
+      int okw = 0;
+      if (lane == 0) okw = mbar_wait(&tfull[b2], (c >> 1) & 1, abort_flag) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
+      if (!ok) {
+        if (lane == 0) *abort_flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b2 * BN2 + h * HALF);
+#pragma unroll
+      for (int j = 0; j < HALF; j += 32) {
+        uint32_t v[32];
+        tmem_ld32(tbase + (uint32_t)j, v);
+        tmem_wait();
+#pragma unroll
+        for (int i = 0; i < 32; ++i) acc[j + i] += __uint_as_float(v[i]);
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_remote(mapa_shared(su32(&tempty[b2]), 0));
+    }
+    if (ok) {
+      // all MMAs have completed (last tfull), so every load has landed: the pipeline buffers are free
+      float *stg = (float *)smem + (size_t)(warp - 2) * 32 * SROW;
+#pragma unroll
+      for (int j = 0; j < HALF; ++j) stg[lane * SROW + j] = acc[j];
+      __syncwarp();
+      const int gn0 = n0 + h * HALF;
+      for (int r = 0; r < 32; ++r) {
+        const int gm = m0 + q * 32 + r;
+        if (gm >= p.M) break;
+#pragma unroll
+        for (int t = 0; t < HALF / 32; ++t) {
+          const int gn = gn0 + t * 32 + lane;
+          if (gn < p.N) {
+            const float v = stg[r * SROW + t * 32 + lane];
+            const long long off = (long long)gm * p.c_rs + (long long)gn * p.c_cs;
+            if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)v;
+            else ((float *)p.C)[off] = (float)(p.alpha * (double)v);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (*abort_flag && threadIdx.x == 0) atomicExch(p.status, (int)kErrTimeout);
+  tc_fence_before();
+  cluster_sync_all();  // CTA 0's MMAs are complete before either CTA frees tensor memory
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)TMEM_COLS));
   }
 }
 
@@ -511,6 +886,13 @@ CUtensorMap make_map(const Planes &P, int bx, int by, CUtensorMapSwizzle sw) {
   return m;
 }
 
+// k-blocks per accumulation chunk: chunk_k deep (0: kChunkK; ISVD_UMMA_CHUNK_K overrides)
+int chunk_kblocks(int bk, int chunk_k) {
+  int ck = chunk_k > 0 ? chunk_k : kChunkK;
+  if (const char *e = getenv("ISVD_UMMA_CHUNK_K")) ck = std::max(bk, atoi(e));
+  return std::max(1, ck / bk);
+}
+
 template <int BN, int BK, bool AMN, bool BMN>
 void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   using C = Cfg<BN, BK, AMN, BMN>;
@@ -558,6 +940,10 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   const int stage_bytes = g.A.np * C::A_TILE + g.B.np * C::B_TILE;
   const int budget = (int)rt.smem_optin - 1024 - 256;
   int stages = std::min(8, budget / stage_bytes);
+  p.chunk_kb = chunk_kblocks(BK, g.chunk_k);
+  // rows of C contiguous (or a split-K partial): stage the epilogue through shared memory when the
+  // pipeline buffers can hold the 8 warps' 32 x (BN/2 + 1) blocks
+  p.stage_out = ((p.splits > 1 || g.c_cs == 1) && stages * stage_bytes >= 8 * 32 * (C::HALF + 1) * 4) ? 1 : 0;
   if (stages < 2) fail(kErrUnsupported, "tcgen05 GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
   static_assert(kThreads == 64 + 32 * kEpiWarps, "warp roles");
@@ -586,6 +972,69 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
     const int blocks = (int)std::min<long long>((total + 255) / 256, 16LL * rt.num_sms);
     umma_reduce_kernel<<<blocks, 256, 0, st>>>(p);
     KLAUNCHED();
+  }
+}
+
+// Pair kernel: K-major A and B, one batch, no split-K, no triangle; grid (2 x N tiles, M pairs),
+// clusters of two CTAs along x.
+template <int BK>
+void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
+  Runtime &rt = Runtime::get();
+  KParams p;
+  memset(&p, 0, sizeof(p));
+  p.M = g.M; p.N = g.N; p.K = g.K;
+  p.na = g.A.np; p.nb = g.B.np; p.nprod = g.nprod;
+  for (int i = 0; i < g.nprod; ++i) { p.pa[i] = g.pa[i]; p.pb[i] = g.pb[i]; }
+  p.batch = 1; p.splits = 1;
+  p.C = g.C; p.c_double = g.c_double;
+  p.c_rs = g.c_rs; p.c_cs = g.c_cs;
+  p.alpha = g.alpha;
+  p.status = status;
+  p.total_kb = (g.K + BK - 1) / BK;
+  p.kbps = p.total_kb;
+  p.chunk_kb = chunk_kblocks(BK, g.chunk_k);
+  const CUtensorMapSwizzle sw = (BK == 64) ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+  CUtensorMap ma = make_map(g.A, BK, BM, sw);
+  CUtensorMap mb = make_map(g.B, BK, BM, sw);  // 128-row halves of the 256-row B tile
+  const int stage_bytes = (g.A.np + g.B.np) * BM * BK * 2;
+  const int budget = (int)rt.smem_optin - 1024 - 256;
+  const int stages = std::min(8, budget / stage_bytes);
+  // the epilogue stages 8 warps x 32 rows x 129 floats in the pipeline buffers
+  if (stages < 2 || stages * stage_bytes < 8 * 32 * 129 * 4)
+    fail(kErrUnsupported, "tcgen05 pair GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
+  const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
+  auto kern = umma_pair_kernel<BK>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int gx = (g.N + 255) / 256, gy = (g.M + 2 * BM - 1) / (2 * BM);
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned)(2 * gx), (unsigned)gy, 1);
+  cfg.blockDim = dim3(kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 2;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (profiling()) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st));
+  }
+  CK(cudaLaunchKernelEx(&cfg, kern, ma, mb, p, stages));
+  KLAUNCHED();
+  if (profiling()) {
+    CK(cudaEventRecord(e1, st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    profile_add(g.tag, ms, 2.0 * g.M * (double)g.N * g.K * g.nprod);
   }
 }
 
@@ -659,6 +1108,25 @@ void rng_gaussian_bf16_t(__nv_bfloat16 *dst, long long n, long long Nl, long lon
   KLAUNCHED();
 }
 
+// The CTA-pair kernel serves K-major products with enough 256 x 256 tiles to fill the GPU when
+// ISVD_UMMA_PAIR=1 (ISVD_UMMA_PAIR_BK=32 selects 32-deep k-blocks).  Off by default: on the
+// sketch shape it measures 2 % slower than the one-CTA kernel, whose tensor pipe is not limited by
+// shared-memory bandwidth once its issue loop is tight.
+static bool pair_ok(const UmmaGemm &g) {
+  const char *e = getenv("ISVD_UMMA_PAIR");
+  if (!e || atoi(e) == 0) return false;
+  const long long tiles = (long long)((g.N + 255) / 256) * ((g.M + 255) / 256);
+  return tiles >= Runtime::get().num_sms / 2 && g.K >= 1024;
+}
+static bool bk32_forced() {
+  const char *e = getenv("ISVD_UMMA_BK");
+  return e && atoi(e) == 32;
+}
+static int pair_bk() {
+  const char *e = getenv("ISVD_UMMA_PAIR_BK");
+  return (e && atoi(e) == 32) ? 32 : 64;
+}
+
 void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
   if (g.nprod < 1 || g.nprod > 8) fail(kErrArgument, "tcgen05 GEMM: 1..8 plane products");
@@ -678,7 +1146,10 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
     launch_t<128, 64, false, true>(g, st, status);
   } else if (small_n) {
     launch_t<128, 64, false, false>(g, st, status);
-  } else if (3 * stage64 <= (int)rt.smem_optin - 2048) {
+  } else if (g.batch == 1 && g.splits <= 0 && !g.upper && pair_ok(g)) {
+    if (pair_bk() == 32) launch_pair<32>(g, st, status);
+    else launch_pair<64>(g, st, status);
+  } else if (3 * stage64 <= (int)rt.smem_optin - 2048 && !bk32_forced()) {
     launch_t<256, 64, false, false>(g, st, status);
   } else {
     launch_t<256, 32, false, false>(g, st, status);

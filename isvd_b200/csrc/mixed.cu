@@ -119,39 +119,52 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     CK(cudaEventRecord(ready, c.st));  // staging buffers allocated on the compute stream
     CK(cudaStreamWaitEvent(rt.copy_stream, ready, 0));
   }
-  int p = 0;
-  for (long long r0 = 0; r0 < m; r0 += P, ++p) {
-    const long long rows = std::min<long long>(P, m - r0);
-    __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
-    if (a_dev) {
+  UmmaGemm g;
+  g.N = Nl; g.K = n;
+  g.B = om.P;
+  set_products(g, na, om.P.np);
+  g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
+  g.status = c.status;
+  g.chunk_k = 512;  // 5e-7 relative tensor-core chain error per chunk, below the 2^-17 split level
+  g.tag = "sketch";
+  if (a_dev) {
+    // A on the device: split every row, then one launch over all m rows (no per-panel wave tail)
+    for (long long r0 = 0; r0 < m; r0 += P) {
+      const long long rows = std::min<long long>(P, m - r0);
+      __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
       if (ordera == 'R') split_rows<T>(a + r0 * lda, lda, 1, rows, n, na, false, dst, ld, ps, c.st);
       else split_rows<T>(a + r0, lda, 1, n, rows, na, true, dst, ld, ps, c.st);  // A' rows r0.. as n x rows
-    } else {
-      const int b = p & 1;
-      if (p >= 2) CK(cudaStreamWaitEvent(rt.copy_stream, consumed[b], 0));
-      if (ordera == 'R') {
-        CK(cudaMemcpy2DAsync(stage[b].p, n * sizeof(T), a + r0 * lda, lda * sizeof(T), n * sizeof(T), rows,
-                             cudaMemcpyHostToDevice, rt.copy_stream));
-      } else {
-        CK(cudaMemcpy2DAsync(stage[b].p, rows * sizeof(T), a + r0, lda * sizeof(T), rows * sizeof(T), n,
-                             cudaMemcpyHostToDevice, rt.copy_stream));
-      }
-      CK(cudaEventRecord(copied[b], rt.copy_stream));
-      CK(cudaStreamWaitEvent(c.st, copied[b], 0));
-      if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, na, false, dst, ld, ps, c.st);
-      else split_rows<T>(stage[b].p, rows, 1, n, rows, na, true, dst, ld, ps, c.st);
-      CK(cudaEventRecord(consumed[b], c.st));
     }
+    g.M = m;
+    g.A = all;
+    g.C = y;
+    umma_gemm(g, c.st);
+  }
+  int p = 0;
+  for (long long r0 = 0; r0 < m && !a_dev; r0 += P, ++p) {
+    // A in host memory: panel p + 1 is copied while panel p is split and multiplied
+    const long long rows = std::min<long long>(P, m - r0);
+    __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
+    const int b = p & 1;
+    if (p >= 2) CK(cudaStreamWaitEvent(rt.copy_stream, consumed[b], 0));
+    if (ordera == 'R') {
+      CK(cudaMemcpy2DAsync(stage[b].p, n * sizeof(T), a + r0 * lda, lda * sizeof(T), n * sizeof(T), rows,
+                           cudaMemcpyHostToDevice, rt.copy_stream));
+    } else {
+      CK(cudaMemcpy2DAsync(stage[b].p, rows * sizeof(T), a + r0, lda * sizeof(T), rows * sizeof(T), n,
+                           cudaMemcpyHostToDevice, rt.copy_stream));
+    }
+    CK(cudaEventRecord(copied[b], rt.copy_stream));
+    CK(cudaStreamWaitEvent(c.st, copied[b], 0));
+    if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, na, false, dst, ld, ps, c.st);
+    else split_rows<T>(stage[b].p, rows, 1, n, rows, na, true, dst, ld, ps, c.st);
+    CK(cudaEventRecord(consumed[b], c.st));
     Planes ap = all;
     ap.ptr = dst;
     ap.rows = rows;
-    UmmaGemm g;
-    g.M = (int)rows; g.N = Nl; g.K = n;
-    g.A = ap; g.B = om.P;
-    set_products(g, na, om.P.np);
-    g.C = y + r0 * ldy; g.c_double = is_double<T>(); g.c_rs = ldy; g.c_cs = 1;
-    g.status = c.status;
-    g.tag = "sketch";
+    g.M = (int)rows;
+    g.A = ap;
+    g.C = y + r0 * ldy;
     umma_gemm(g, c.st);
   }
   if (!a_dev) {

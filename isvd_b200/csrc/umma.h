@@ -41,6 +41,7 @@ struct UmmaGemm {
   double alpha = 1.0;
   int splits = 0;      // split-K (0: automatic); partial sums are added in FP64
   bool upper = false;  // symmetric output: only tiles touching the upper triangle, j >= i written
+  int chunk_k = 0;     // K depth of one tensor-memory accumulation chunk (0: 128)
   const char *tag = "gemm";  // name under which launches are recorded when profiling is enabled
   int *status = nullptr;     // device status word: set, the call returns without a host synchronisation
 };

@@ -29,7 +29,7 @@ def lowrank(m, n, rank, decay, noise, seed):
 @pytest.mark.parametrize("ordera", [b"R", b"C"])
 @pytest.mark.parametrize("shape", [(101, 1001, 132), (1000, 777, 300), (300, 2000, 512)])
 def test_mixed_sketch_omega(lib, x, ordera, shape):
-    """Y = A Omega with A and Omega both split into 3 planes (6 products): FP32-level accuracy
+    """Y = A Omega with A split into 2 planes and Omega into 3 (5 products): FP32-level accuracy
     (the FP32 tensor-core accumulation bounds it, as it bounds an FP32 GEMM: ~1e-6 relative at
     K = 1e3..2e4), across M/N/K tails and both storage orders of A."""
     m, n, nl = shape
@@ -45,6 +45,29 @@ def test_mixed_sketch_omega(lib, x, ordera, shape):
     ref = a.astype(np.float64) @ om.astype(np.float64)
     err = np.abs(y - ref).max() / np.abs(ref).max()
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("bk", ["64", "32"])
+def test_mixed_sketch_cta_pair(lib, monkeypatch, bk):
+    """A sketch large enough for the CTA-pair kernel (ISVD_UMMA_PAIR=1; 80 tiles of 256 x 256; M, N
+    and K tails): the same products as the one-CTA kernel (ISVD_UMMA_PAIR=0) to FP32 rounding, and
+    the FP64 product to the sketch's bar."""
+    m, n, nl = 4000, 1500, 1200
+    rng = np.random.default_rng(8)
+    a = rng.standard_normal((m, n)).astype(np.float32)
+    om = rng.standard_normal((n, nl)).astype(np.float32)
+    prm = lib.create_param(m, n, nl, 0, 1)
+    monkeypatch.setenv("ISVD_UMMA_PAIR", "1")
+    monkeypatch.setenv("ISVD_UMMA_PAIR_BK", bk)
+    y2 = np.zeros((m, nl), np.float32)
+    lib.sketch_omega("s", prm, a, n, om, nl, y2, nl)
+    monkeypatch.setenv("ISVD_UMMA_PAIR", "0")
+    y1 = np.zeros((m, nl), np.float32)
+    lib.sketch_omega("s", prm, a, n, om, nl, y1, nl)
+    ref = a.astype(np.float64) @ om.astype(np.float64)
+    scale = np.abs(ref).max()
+    assert np.abs(y2 - y1).max() < 1e-6 * scale
+    assert np.abs(y2 - ref).max() < 1e-5 * scale
 
 
 def test_mixed_sketch_internal_omega_matches_native(lib):
