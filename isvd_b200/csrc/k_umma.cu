@@ -752,24 +752,57 @@ __device__ __forceinline__ uint4 pack8(const __nv_bfloat16 *v) {
   return u;
 }
 
-// Non-transposed: plane(r, c) for r < rows_pad, c < ld (zero outside rows x cols); each thread
-// converts 8 consecutive columns and writes one 16-byte vector per plane.
+// Pieces of an FP32 value in FP32 arithmetic: x - bf16(x) is exact in FP32 (the rounding error of
+// an 8-bit rounding of a 24-bit significand), and so is the next remainder.
+__device__ __forceinline__ void split3f(float x, __nv_bfloat16 *o) {
+  const __nv_bfloat16 h0 = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h0);
+  const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(h1);
+  o[0] = h0;
+  o[1] = h1;
+  o[2] = __float2bfloat16_rn(r2);
+}
+
+// Non-transposed: plane(r, c) for r < rows_pad, c < ld (zero outside rows x cols).  Grid: x over
+// 8-column groups of a row (one 16-byte vector per plane per thread), y striding over rows; rows
+// with unit column stride and 16-byte aligned starts are read as vectors.
 template <class T>
 __global__ void split_kernel(const T *__restrict__ src, long long s_rs, long long s_cs, long long rows,
                              long long cols, long long rows_pad, int np, __nv_bfloat16 *__restrict__ dst,
                              long long ld, long long ps) {
-  const long long gpr = ld / 8;
-  const long long total = rows_pad * gpr;
-  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < total;
-       g += (long long)gridDim.x * blockDim.x) {
-    const long long r = g / gpr, c0 = (g - r * gpr) * 8;
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long c0 = 8LL * g;
+  if (c0 >= ld) return;
+  for (long long r = blockIdx.y; r < rows_pad; r += gridDim.y) {
+    T x[8];
+    const T *row = src + r * s_rs;
+    if (r < rows && c0 + 8 <= cols && s_cs == 1 && ((uintptr_t)(row + c0) & 15) == 0) {
+      if (sizeof(T) == 4) {
+        const float4 u = __ldg((const float4 *)(row + c0)), v = __ldg((const float4 *)(row + c0) + 1);
+        x[0] = (T)u.x; x[1] = (T)u.y; x[2] = (T)u.z; x[3] = (T)u.w;
+        x[4] = (T)v.x; x[5] = (T)v.y; x[6] = (T)v.z; x[7] = (T)v.w;
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const double2 u = __ldg((const double2 *)(row + c0) + i);
+          x[2 * i] = (T)u.x;
+          x[2 * i + 1] = (T)u.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const long long c = c0 + i;
+        x[i] = (r < rows && c < cols) ? src[r * s_rs + c * s_cs] : T(0);
+      }
+    }
     __nv_bfloat16 o[3][8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      const long long c = c0 + i;
-      const T x = (r < rows && c < cols) ? src[r * s_rs + c * s_cs] : T(0);
       __nv_bfloat16 t[3];
-      split3<T>(x, t, 3);
+      if (sizeof(T) == 4) split3f((float)x[i], t);
+      else split3<T>(x[i], t, 3);
 #pragma unroll
       for (int q = 0; q < 3; ++q) o[q][i] = t[q];
     }
@@ -1043,15 +1076,13 @@ void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
 template <class T>
 void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np,
                   bool transpose, __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st) {
-  Runtime &rt = Runtime::get();
   const long long out_rows = transpose ? cols : rows;
   const long long rows_pad = plane_stride / ld;
   if (rows_pad < out_rows || ld < (transpose ? rows : cols)) fail(kErrArgument, "split_planes: plane too small");
   if (!transpose) {
     if (ld % 8) fail(kErrArgument, "split_planes: ld must be a multiple of 8");
-    const long long total = rows_pad * (ld / 8);
-    const int blocks = (int)std::min<long long>((total + 255) / 256, 32LL * rt.num_sms);
-    split_kernel<T><<<blocks, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows_pad, np, dst, ld, plane_stride);
+    const dim3 grid((unsigned)((ld / 8 + 255) / 256), (unsigned)std::min<long long>(rows_pad, 65535));
+    split_kernel<T><<<grid, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows_pad, np, dst, ld, plane_stride);
     KLAUNCHED();
   } else {
     // zero the padding (rows beyond cols, columns beyond rows), then transpose-split
@@ -1073,13 +1104,11 @@ void split_planes(const T *src, long long s_rs, long long s_cs, long long rows, 
 template <class T>
 void split_rows(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np, bool transpose,
                 __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st) {
-  Runtime &rt = Runtime::get();
   if (ld % 8) fail(kErrArgument, "split_rows: ld must be a multiple of 8");
   if (!transpose) {
     if (ld < cols) fail(kErrArgument, "split_rows: plane too narrow");
-    const long long total = rows * (ld / 8);
-    const int blocks = (int)std::min<long long>((total + 255) / 256, 32LL * rt.num_sms);
-    split_kernel<T><<<blocks, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows, np, dst, ld, plane_stride);
+    const dim3 grid((unsigned)((ld / 8 + 255) / 256), (unsigned)std::min<long long>(std::max(rows, 1LL), 65535));
+    split_kernel<T><<<grid, 256, 0, st>>>(src, s_rs, s_cs, rows, cols, rows, np, dst, ld, plane_stride);
     KLAUNCHED();
   } else {
     // output rows = cols of src, output columns = rows of src; the grid covers ld when
