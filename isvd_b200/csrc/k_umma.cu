@@ -478,10 +478,13 @@ __device__ __forceinline__ void umma_commit_pair(uint32_t bar_cluster) {
                : "memory");
 }
 
-template <int BK>
+// MN: both operands MN-major (stored K x M and K x N, M / N contiguous; BK = 64 only), e.g. the
+// Gram matrix Q'Q of a row-major Q; `upper` then skips pairs strictly below the diagonal.
+template <int BK, bool MN>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_pair_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                      const KParams p, const int stages) {
+  static_assert(!MN || BK == 64, "MN-major pair tiles use 64-deep k-blocks");
   constexpr int HT = BM * BK * 2;  // bytes of one 128-row plane tile (A, or half of B)
   constexpr uint32_t LAYOUT = (BK == 64) ? 2u : 4u;
   constexpr uint32_t SBO = (BK == 64) ? 1024u : 512u;
@@ -506,6 +509,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int nt = blockIdx.x >> 1, pt = blockIdx.y;
   const int m0 = pt * (2 * BM) + (int)rank * BM, n0 = nt * BN2;
   const int nkb = p.total_kb;
+  if (p.upper && n0 + BN2 <= pt * (2 * BM)) return;  // both CTAs: pair strictly below the diagonal
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < stages; ++s) {
@@ -546,8 +550,17 @@ __global__ void __launch_bounds__(kThreads, 1)
       const uint32_t fb = full0 + 8u * (uint32_t)s;
       if (rank == 0) mbar_expect_tx(&full[s], (uint32_t)(2 * stage_bytes));
       const int k0 = kb * BK;
-      for (int q = 0; q < p.na; ++q) tma_load_3d_pair(st + q * HT, &mapA, fb, k0, m0, q);
-      for (int q = 0; q < p.nb; ++q) tma_load_3d_pair(st + (p.na + q) * HT, &mapB, fb, k0, b_row, q);
+      if (!MN) {
+        for (int q = 0; q < p.na; ++q) tma_load_3d_pair(st + q * HT, &mapA, fb, k0, m0, q);
+        for (int q = 0; q < p.nb; ++q) tma_load_3d_pair(st + (p.na + q) * HT, &mapB, fb, k0, b_row, q);
+      } else {
+        // two 64-wide MN atoms of BK K-rows each per 128-row half
+        for (int q = 0; q < p.na; ++q)
+          for (int j = 0; j < 2; ++j) tma_load_3d_pair(st + q * HT + j * (BK * 128), &mapA, fb, m0 + 64 * j, k0, q);
+        for (int q = 0; q < p.nb; ++q)
+          for (int j = 0; j < 2; ++j)
+            tma_load_3d_pair(st + (p.na + q) * HT + j * (BK * 128), &mapB, fb, b_row + 64 * j, k0, q);
+      }
       ++issued;
       if (++s == stages) {
         s = 0;
@@ -565,8 +578,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1 && lane == 0 && rank == 0) {
     // ---------------------------------------------------------------- MMA issuer (CTA 0)
-    const uint32_t idesc = idesc_bf16(2 * BM, BN2, false, false);
-    const uint64_t d0 = sdesc(0, 16, SBO, LAYOUT);
+    const uint32_t idesc = idesc_bf16(2 * BM, BN2, MN, MN);
+    const uint64_t d0 = MN ? sdesc(0, BK * 128, 1024, 2u) : sdesc(0, 16, SBO, LAYOUT);
+    constexpr uint32_t kStep = MN ? 2048 / 16 : 32 / 16;  // one K = 16 step, in 16-byte units
     const int nprod = p.nprod;
     uint32_t aoff[8], boff[8];
 #pragma unroll
@@ -604,7 +618,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           const uint64_t da = d0 + so + aoff[i], db = d0 + so + boff[i];
 #pragma unroll
           for (int kk = 0; kk < BK / 16; ++kk) {
-            umma_bf16_pair(tacc, da + kk * 2, db + kk * 2, idesc, accf);
+            umma_bf16_pair(tacc, da + kk * kStep, db + kk * kStep, idesc, accf);
             accf = 1u;
           }
         }
@@ -673,7 +687,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int t = 0; t < HALF / 32; ++t) {
           const int gn = gn0 + t * 32 + lane;
-          if (gn < p.N) {
+          if (gn < p.N && !(p.upper && gn < gm)) {
             const float v = stg[r * SROW + t * 32 + lane];
             const long long off = (long long)gm * p.c_rs + (long long)gn * p.c_cs;
             if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)v;
@@ -1010,7 +1024,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
 
 // Pair kernel: K-major A and B, one batch, no split-K, no triangle; grid (2 x N tiles, M pairs),
 // clusters of two CTAs along x.
-template <int BK>
+template <int BK, bool MN>
 void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
   Runtime &rt = Runtime::get();
   KParams p;
@@ -1022,13 +1036,15 @@ void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.C = g.C; p.c_double = g.c_double;
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
+  p.upper = g.upper ? 1 : 0;
   p.status = status;
   p.total_kb = (g.K + BK - 1) / BK;
   p.kbps = p.total_kb;
   p.chunk_kb = chunk_kblocks(BK, g.chunk_k);
   const CUtensorMapSwizzle sw = (BK == 64) ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
-  CUtensorMap ma = make_map(g.A, BK, BM, sw);
-  CUtensorMap mb = make_map(g.B, BK, BM, sw);  // 128-row halves of the 256-row B tile
+  CUtensorMap ma = MN ? make_map(g.A, 64, BK, CU_TENSOR_MAP_SWIZZLE_128B) : make_map(g.A, BK, BM, sw);
+  // 128-row halves of the 256-row B tile
+  CUtensorMap mb = MN ? make_map(g.B, 64, BK, CU_TENSOR_MAP_SWIZZLE_128B) : make_map(g.B, BK, BM, sw);
   const int stage_bytes = (g.A.np + g.B.np) * BM * BK * 2;
   const int budget = (int)rt.smem_optin - 1024 - 256;
   const int stages = std::min(8, budget / stage_bytes);
@@ -1036,7 +1052,7 @@ void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
   if (stages < 2 || stages * stage_bytes < 8 * 32 * 129 * 4)
     fail(kErrUnsupported, "tcgen05 pair GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
-  auto kern = umma_pair_kernel<BK>;
+  auto kern = umma_pair_kernel<BK, MN>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const int gx = (g.N + 255) / 256, gy = (g.M + 2 * BM - 1) / (2 * BM);
   cudaLaunchConfig_t cfg;
@@ -1147,6 +1163,15 @@ static bool pair_ok(const UmmaGemm &g) {
   const long long tiles = (long long)((g.N + 255) / 256) * ((g.M + 255) / 256);
   return tiles >= Runtime::get().num_sms / 2 && g.K >= 1024;
 }
+// MN-major pairs (Gram matrices Q'Q of row-major panels; ISVD_UMMA_PAIR_MN=0 turns them off): each
+// SM stages half of the B tile, which halves the L2 traffic of these shared-operand products (the
+// config-2 Gram Qs'Qs, 4096 x 4096 x 200000 as 2 x 2 planes: 13.3 -> 8.0 ms).
+static bool pair_mn_ok(const UmmaGemm &g) {
+  const char *e = getenv("ISVD_UMMA_PAIR_MN");
+  if (e && atoi(e) == 0) return false;
+  const long long tiles = (long long)((g.N + 255) / 256) * ((g.M + 255) / 256);
+  return tiles >= Runtime::get().num_sms / 2 && g.K >= 1024 && g.A.np + g.B.np <= 4;
+}
 static bool bk32_forced() {
   const char *e = getenv("ISVD_UMMA_BK");
   return e && atoi(e) == 32;
@@ -1168,7 +1193,8 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   const int stage64 = g.A.np * BM * 64 * 2 + g.B.np * 256 * 64 * 2;
   const bool small_n = g.N <= 128;
   if (amn && bmn) {
-    launch_t<128, 64, true, true>(g, st, status);
+    if (g.batch == 1 && g.splits <= 0 && pair_mn_ok(g)) launch_pair<64, true>(g, st, status);
+    else launch_t<128, 64, true, true>(g, st, status);
   } else if (amn) {
     fail(kErrUnsupported, "tcgen05 GEMM: MN-major A needs MN-major B");
   } else if (bmn) {
@@ -1176,8 +1202,8 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   } else if (small_n) {
     launch_t<128, 64, false, false>(g, st, status);
   } else if (g.batch == 1 && g.splits <= 0 && !g.upper && pair_ok(g)) {
-    if (pair_bk() == 32) launch_pair<32>(g, st, status);
-    else launch_pair<64>(g, st, status);
+    if (pair_bk() == 32) launch_pair<32, false>(g, st, status);
+    else launch_pair<64, false>(g, st, status);
   } else if (3 * stage64 <= (int)rt.smem_optin - 2048 && !bk32_forced()) {
     launch_t<256, 64, false, false>(g, st, status);
   } else {

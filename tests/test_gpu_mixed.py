@@ -70,6 +70,35 @@ def test_mixed_sketch_cta_pair(lib, monkeypatch, bk):
     assert np.abs(y2 - ref).max() < 1e-5 * scale
 
 
+def test_mixed_kn_gram_cta_pair(lib, monkeypatch):
+    """KN at N l = 4096 (the Gram matrix Qs'Qs has 136 upper 256 x 256 tiles): with the Gram on
+    the MN-major CTA-pair kernel (the default), the same iteration count and Qbar as with the
+    one-CTA kernel (ISVD_UMMA_PAIR_MN=0)."""
+    torch = pytest.importorskip("torch")
+    m, l, Nn = 6000, 128, 32
+    g = torch.Generator(device="cuda").manual_seed(3)
+    base = torch.linalg.qr(torch.randn(m, l, device="cuda", dtype=torch.float64, generator=g))[0]
+    blocks = []
+    for _ in range(Nn):  # perturbed copies of one subspace, re-orthonormalised
+        blocks.append(torch.linalg.qr(base + 0.05 * torch.randn(m, l, device="cuda", dtype=torch.float64,
+                                                                 generator=g))[0])
+    qs = torch.cat(blocks, dim=1).float().contiguous()
+    prm = lib.create_param(m, m, l, 0, Nn)
+
+    def run():
+        qt = torch.zeros((m, l), device="cuda")
+        torch.cuda.synchronize()
+        r = lib.integrate("s", "KN", prm, qs, l * Nn, qt, l, argv=[256, 1e-4])
+        return int(r[0]), qt.double()
+
+    monkeypatch.setenv("ISVD_UMMA_PAIR_MN", "1")
+    it2, q2 = run()
+    monkeypatch.setenv("ISVD_UMMA_PAIR_MN", "0")
+    it1, q1 = run()
+    assert it2 == it1
+    assert (q2 - q1).abs().max().item() < 1e-5
+
+
 def test_mixed_sketch_internal_omega_matches_native(lib):
     """The internal Omega is drawn exactly in bf16, identical in both precision modes."""
     m, n, k, p, Nn = 700, 500, 20, 12, 4
