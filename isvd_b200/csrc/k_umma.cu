@@ -50,6 +50,8 @@ struct KParams {
   int *status;
   int chunk_kb;   // k-blocks per tensor-memory accumulation chunk
   int stage_out;  // epilogue stages its rows through shared memory (C rows contiguous)
+  int bloop;      // one CTA runs every batch of its tile in turn (grid z = 1, no split-K)
+  int vec_out;    // direct epilogue stores as 16-byte vectors (C rows contiguous and aligned)
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -187,7 +189,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nt = blockIdx.x, mt = blockIdx.y;
-  const int b = blockIdx.z / p.splits, split = blockIdx.z % p.splits;
+  // segments: the batches this CTA accumulates one after the other (bloop), else its one batch
+  // (batch loops and vector stores serve the skinny N <= 128 shapes; the 256-wide sketch tiles keep
+  // their registers for the 128-column accumulators)
+  const bool bloop = BN <= 128 && p.bloop;
+  const int nseg = bloop ? p.batch : 1;
+  const int bz = bloop ? 0 : blockIdx.z / p.splits, split = bloop ? 0 : blockIdx.z % p.splits;
   const int m0 = mt * BM, n0 = nt * BN;
   if (p.upper && n0 + BN <= m0) return;  // tile strictly below the diagonal: mirrored later
   const int kb0 = split * p.kbps;
@@ -217,12 +224,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0 && lane == 0) {
     // ---------------------------------------------------------------- TMA producer
-    const int a_row = (int)(b * p.a_mn_step) + m0;
-    const int b_row = (int)(b * p.b_mn_step) + n0;
     int issued = 0, s = 0;
     uint32_t ph = 1;  // parity of the empty phase to wait for (first pass: none)
+    for (int seg = 0; seg < nseg && !*abort_flag; ++seg) {
+    const int b = bloop ? seg : bz;
+    const int a_row = (int)(b * p.a_mn_step) + m0;
+    const int b_row = (int)(b * p.b_mn_step) + n0;
     for (int kb = 0; kb < nkb; ++kb) {
-      if (kb >= stages && !mbar_try(&empty[s], ph) && !mbar_wait(&empty[s], ph, abort_flag)) {
+      if (issued >= stages && !mbar_try(&empty[s], ph) && !mbar_wait(&empty[s], ph, abort_flag)) {
         *abort_flag = 1;
         break;
       }
@@ -255,6 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         ph ^= 1u;
       }
     }
+    }
     // Drain: every issued load has landed before the CTA can exit (bounded).
     for (int kb = max(0, issued - stages); kb < issued; ++kb) {
       const int s = kb % stages;
@@ -283,6 +293,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int chunk_kb = p.chunk_kb;
     int chunk = 0, cleft = 0, s = 0;
     uint32_t ph = 0, tacc = tmem, accf = 0;
+    for (int seg = 0; seg < nseg && !*abort_flag; ++seg)
     for (int kb = 0; kb < nkb; ++kb) {
       if (cleft == 0) {
         const int b2 = chunk & 1;
@@ -328,12 +339,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int q = warp & 3;                 // TMEM lane quarter accessible to this warp
     const int h = (warp - 2) >> 2;          // column half
     const int row = q * 32 + lane;
-    const int nchunks = (nkb + p.chunk_kb - 1) / p.chunk_kb;
+    const int nchunks = (nkb + p.chunk_kb - 1) / p.chunk_kb;  // per segment
+    const int gm = m0 + row;
+    bool ok = true;
+    int c = 0;  // chunks drained so far (all segments)
+    for (int seg = 0; seg < nseg && ok; ++seg) {
+    const int b = bloop ? seg : bz;
     float acc[C::HALF];
 #pragma unroll
     for (int j = 0; j < C::HALF; ++j) acc[j] = 0.f;
-    bool ok = true;
-    for (int c = 0; c < nchunks; ++c) {
+    for (int cc = 0; cc < nchunks; ++cc, ++c) {
       const int b2 = c & 1;
       int okw = 0;
       if (lane == 0) okw = mbar_wait(&tfull[b2], (c >> 1) & 1, abort_flag) ? 1 : 0;
@@ -356,7 +371,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncwarp();
       if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(&tempty[b2])) : "memory");
     }
-    const int gm = m0 + row;
     if (ok && p.stage_out) {
       // every MMA has completed (last tfull), so every load has landed and the pipeline buffers
       // are free: each warp transposes its 32 x HALF block through them and writes whole rows
@@ -382,6 +396,23 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
         }
       }
+    } else if (BN <= 128 && ok && gm < p.M && p.vec_out && p.splits == 1) {
+      // this thread's row: 16-byte stores of 4 (FP32) or 2 (FP64) consecutive columns
+      const int gn0 = n0 + h * C::HALF;
+      const long long off0 = (long long)b * p.c_step + (long long)gm * p.c_rs + gn0;
+#pragma unroll
+      for (int j = 0; j < C::HALF; j += 4) {
+        if (gn0 + j >= p.N) break;  // N % 4 == 0: a group is either whole or outside
+        if (p.c_double) {
+          double2 *o = (double2 *)((double *)p.C + off0 + j);
+          o[0] = make_double2(p.alpha * (double)acc[j], p.alpha * (double)acc[j + 1]);
+          o[1] = make_double2(p.alpha * (double)acc[j + 2], p.alpha * (double)acc[j + 3]);
+        } else {
+          *(float4 *)((float *)p.C + off0 + j) =
+              make_float4((float)(p.alpha * (double)acc[j]), (float)(p.alpha * (double)acc[j + 1]),
+                          (float)(p.alpha * (double)acc[j + 2]), (float)(p.alpha * (double)acc[j + 3]));
+        }
+      }
     } else if (ok && gm < p.M) {
       const bool upper_tile = p.upper != 0;
 #pragma unroll
@@ -398,6 +429,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
     }
+    }
   }
   __syncthreads();
   if (*abort_flag && threadIdx.x == 0) atomicExch(p.status, (int)kErrTimeout);
@@ -411,9 +443,9 @@ __global__ void __launch_bounds__(kThreads, 1)
 // K-major A and B, no batch / split-K / triangle.  The two CTAs of a cluster compute one 256 x 256
 // tile: CTA r (rank in the pair) stages A rows [m0 + 128 r, +128) and B rows [n0 + 128 r, +128) of
 // every plane in its own shared memory, and CTA 0 issues tcgen05.mma.cta_group::2 (M = 256), which
-// reads the A half and both B halves of each CTA.  Each SM thus stages half a B tile per k-block
-// instead of a whole one: shared-memory traffic per MMA drops from A + B to A + B/2 (the one-CTA
-// kernel spends about a quarter of its time with the tensor pipe waiting on shared memory).
+// reads the A half and both B halves of each CTA.  Each SM thus loads half a B tile per k-block
+// instead of a whole one, which halves the L2-to-SM traffic of B (what limits the many-plane Gram
+// products; the sketch, with one B plane, is not limited by it).
 // Barriers: full[s] lives in CTA 0 and receives the bytes of both CTAs' loads; empty[s] and
 // tfull[b] exist in both CTAs and receive one tcgen05.commit each from CTA 0; tempty[b] lives in
 // CTA 0 and counts the epilogue warps of both CTAs (remote arrivals from CTA 1).  The epilogue
@@ -709,26 +741,49 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 // C(b, r, c) = alpha * sum_s partial(b, s, r, c) (FP64 sum); upper: only c >= r.
 __global__ void umma_reduce_kernel(const KParams p) {
-  const long long MN = (long long)p.M * p.N;
-  const long long total = MN * p.batch;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const long long b = e / MN, r = (e % MN) / p.N, c = e % p.N;
-    if (p.upper && c < r) continue;
-    // eight independent partial sums, so that eight loads are in flight
-    const float *q = p.partial + ((b * p.splits) * p.M + r) * p.N + c;
-    const long long stride = (long long)p.M * p.N;
-    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    int sp = 0;
-    for (; sp + 8 <= p.splits; sp += 8) {
+  // one thread per 4 consecutive columns of a row; the partial of split sp is added into
+  // accumulator sp % 8 and the eight are summed pairwise (a fixed order)
+  const int n4 = (p.N + 3) >> 2;
+  const unsigned groups = (unsigned)p.M * (unsigned)n4 * (unsigned)p.batch;  // < 2^31 (host check)
+  const long long stride = (long long)p.M * p.N;
+  const bool vec = (p.N & 3) == 0;
+  for (unsigned g = blockIdx.x * blockDim.x + threadIdx.x; g < groups; g += gridDim.x * blockDim.x) {
+    const unsigned c4 = g % (unsigned)n4, rb = g / (unsigned)n4;
+    const unsigned r = rb % (unsigned)p.M, b = rb / (unsigned)p.M;
+    const int c0 = (int)c4 * 4;
+    const float *q = p.partial + (((long long)b * p.splits) * p.M + r) * p.N + c0;
+    double acc[8][4];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) acc[u] += (double)q[(sp + u) * stride];
+    for (int u = 0; u < 8; ++u)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[u][j] = 0.0;
+    for (int sp0 = 0; sp0 < p.splits; sp0 += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (sp0 + u < p.splits) {
+          const float *qs = q + (sp0 + u) * stride;
+          float v[4];
+          if (vec) {
+            const float4 t = __ldg((const float4 *)qs);
+            v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) v[j] = (c0 + j < p.N) ? qs[j] : 0.f;
+          }
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[u][j] += (double)v[j];
+        }
+      }
     }
-    for (int u = 0; sp < p.splits; ++sp, ++u) acc[u] += (double)q[sp * stride];
-    const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
-    const long long off = b * p.c_step + r * p.c_rs + c * p.c_cs;
-    if (p.c_double) ((double *)p.C)[off] = p.alpha * s;
-    else ((float *)p.C)[off] = (float)(p.alpha * s);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + j;
+      if (c >= p.N || (p.upper && c < (int)r)) continue;
+      const double sum = ((acc[0][j] + acc[1][j]) + (acc[2][j] + acc[3][j])) + ((acc[4][j] + acc[5][j]) + (acc[6][j] + acc[7][j]));
+      const long long off = (long long)b * p.c_step + (long long)r * p.c_rs + (long long)c * p.c_cs;
+      if (p.c_double) ((double *)p.C)[off] = p.alpha * sum;
+      else ((float *)p.C)[off] = (float)(p.alpha * sum);
+    }
   }
 }
 
@@ -970,8 +1025,19 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   int splits = g.splits;
   if (const char *e = getenv("ISVD_UMMA_SPLITS")) splits = atoi(e);  // diagnostic override
   if (splits <= 0) {
+    // split-K against wave quantisation (one CTA per SM): the time of s splits is
+    // ceil(tiles s / SMs) / s full-K tile times; take the smallest s within 3 % of the best
+    // (s <= 16, at least 8 k-blocks per split)
+    // (only below four waves: beyond, quantisation costs under 6 % and partial sums add traffic)
+    const int smax = tiles < 4LL * rt.num_sms ? (int)std::max(1, std::min(16, p.total_kb / 8)) : 1;
+    double best = 1e30;
+    for (int sp = 1; sp <= smax; ++sp) best = std::min(best, (double)((tiles * sp + rt.num_sms - 1) / rt.num_sms) / sp);
     splits = 1;
-    if (tiles < rt.num_sms) splits = (int)std::min<long long>((rt.num_sms + tiles - 1) / tiles, std::max(1, p.total_kb / 8));
+    for (int sp = 1; sp <= smax; ++sp)
+      if ((double)((tiles * sp + rt.num_sms - 1) / rt.num_sms) / sp <= 1.03 * best) {
+        splits = sp;
+        break;
+      }
   }
   splits = std::max(1, std::min(splits, p.total_kb));
   p.kbps = (p.total_kb + splits - 1) / splits;
@@ -990,13 +1056,18 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.chunk_kb = chunk_kblocks(BK, g.chunk_k);
   // rows of C contiguous (or a split-K partial): stage the epilogue through shared memory when the
   // pipeline buffers can hold the 8 warps' 32 x (BN/2 + 1) blocks
-  p.stage_out = ((p.splits > 1 || g.c_cs == 1) && stages * stage_bytes >= 8 * 32 * (C::HALF + 1) * 4) ? 1 : 0;
+  // many short batches (e.g. N block products of K = l): one CTA per tile runs all of them in turn,
+  // each one accumulation segment, instead of one CTA per (tile, batch) that would mostly set up
+  p.bloop = (BN <= 128 && g.batch > 1 && p.splits == 1 && p.total_kb <= 16) ? 1 : 0;
+  p.stage_out = (!p.bloop && (p.splits > 1 || g.c_cs == 1) && stages * stage_bytes >= 8 * 32 * (C::HALF + 1) * 4) ? 1 : 0;
+  p.vec_out = (BN <= 128 && g.c_cs == 1 && !g.upper && g.N % 4 == 0 && g.c_rs % 4 == 0 && g.c_step % 4 == 0 &&
+               ((uintptr_t)g.C % 16) == 0) ? 1 : 0;
   if (stages < 2) fail(kErrUnsupported, "tcgen05 GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
   static_assert(kThreads == 64 + 32 * kEpiWarps, "warp roles");
   auto kern = umma_gemm_kernel<BN, BK, AMN, BMN>;
   CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  dim3 grid(gx, gy, g.batch * p.splits);
+  dim3 grid(gx, gy, p.bloop ? 1 : g.batch * p.splits);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (profiling()) {
     CK(cudaEventCreate(&e0));
@@ -1015,8 +1086,9 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
     profile_add(g.tag, ms, 2.0 * g.M * (double)g.N * g.K * g.batch * g.nprod);
   }
   if (p.splits > 1) {
-    const long long total = (long long)g.M * g.N * g.batch;
-    const int blocks = (int)std::min<long long>((total + 255) / 256, 16LL * rt.num_sms);
+    const long long groups = (long long)g.M * ((g.N + 3) / 4) * g.batch;
+    if (groups >= (1LL << 31)) fail(kErrUnsupported, "tcgen05 GEMM: split-K output too large");
+    const int blocks = (int)std::min<long long>((groups + 255) / 256, 16LL * rt.num_sms);
     umma_reduce_kernel<<<blocks, 256, 0, st>>>(p);
     KLAUNCHED();
   }
@@ -1172,6 +1244,10 @@ static bool pair_mn_ok(const UmmaGemm &g) {
   const long long tiles = (long long)((g.N + 255) / 256) * ((g.M + 255) / 256);
   return tiles >= Runtime::get().num_sms / 2 && g.K >= 1024 && g.A.np + g.B.np <= 4;
 }
+static bool smalln_bk64() {
+  const char *e = getenv("ISVD_UMMA_SMALLN_BK");
+  return e && atoi(e) == 64;
+}
 static bool bk32_forced() {
   const char *e = getenv("ISVD_UMMA_BK");
   return e && atoi(e) == 32;
@@ -1200,7 +1276,9 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   } else if (bmn) {
     launch_t<128, 64, false, true>(g, st, status);
   } else if (small_n) {
-    launch_t<128, 64, false, false>(g, st, status);
+    // six or more planes: 32-deep k-blocks give four pipeline stages instead of two
+    if (g.A.np + g.B.np >= 5 && !smalln_bk64()) launch_t<128, 32, false, false>(g, st, status);
+    else launch_t<128, 64, false, false>(g, st, status);
   } else if (g.batch == 1 && g.splits <= 0 && !g.upper && pair_ok(g)) {
     if (pair_bk() == 32) launch_pair<32, false>(g, st, status);
     else launch_pair<64, false>(g, st, status);

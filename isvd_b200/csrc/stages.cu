@@ -2,6 +2,7 @@
 // CUDA cores; l x l steps in FP64.  MIXED precision routes the large products to the tcgen05
 // bf16 split-product engine (mixed.cu).
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "kernels.h"
@@ -264,6 +265,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
       g.A = Wcur; g.a_rs = lw; g.a_cs = 1; g.a_bs = l;
       g.B = Fs.p; g.b_rs = l; g.b_cs = 1; g.b_bs = 2 * (long long)ll;
       g.C = Wnext; g.c_rs = lw; g.c_cs = 1; g.c_bs = l;
+      g.splits = 1;  // 2 N l / 64^2 tiles already fill the GPU: no split-K partials to add up
       gemm(g, c.st);
     }
   };
