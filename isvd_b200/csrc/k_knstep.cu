@@ -49,8 +49,10 @@ struct Ks {
 // Inner loop: four quarters of the inner dimension x 256 threads, each with a 2 x 2 output block
 // (three shared-memory loads per four FMAs); the quarters' partial sums meet in shared memory and
 // are added in a fixed order.
+// C2, C3 (optional) receive copies of C.
 __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, const double *A, const double *B,
-                      double beta, const double *Cin, double diag, double *C) {
+                      double beta, const double *Cin, double diag, double *C, double *C2 = nullptr,
+                      double *C3 = nullptr) {
   const int l = k.l, tid = threadIdx.x;
   const int ty = tid >> 5, tx = tid & 31;                    // output (ty, tx) of the tile in the epilogue
   const int qk = tid >> 8, bi = (tid & 255) >> 4, bj = tid & 15;  // quarter, 2 x 2 block of the inner loop
@@ -100,7 +102,12 @@ __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, c
     __syncthreads();
     const int o = ty * 32 + tx;
     const double acc = (k.part[o] + k.part[1024 + o]) + (k.part[2048 + o] + k.part[3072 + o]);
-    if (i < l && j < l) C[(size_t)i * l + j] = alpha * acc + beta * cin + (i == j ? diag : 0.0);
+    if (i < l && j < l) {
+      const double v = alpha * acc + beta * cin + (i == j ? diag : 0.0);
+      C[(size_t)i * l + j] = v;
+      if (C2) C2[(size_t)i * l + j] = v;
+      if (C3) C3[(size_t)i * l + j] = v;
+    }
   }
 }
 
@@ -130,25 +137,37 @@ __device__ double ks_cluster_sum(const Ks &k, cg::cluster_group &cluster, double
   return s;
 }
 
-// Series degree for rho >= ||4 Z||_2: the smallest d whose tail bound is below the target, or -1.
-__device__ int ks_degree(const KnSeries &ser, double rho, double target) {
+// Series degree for rho >= ||4 Z||_2: the smallest d whose tail bound
+//   tail(d) = sum_{d < n < 64} max(|c_n|, |d_n|) (rho / 4)^n + (table remainder)
+// is below the target, or -1 (the remainder beyond the table is bounded by the last term times
+// rho / (1 - rho)).  Evaluated by one warp: lane j holds the terms 2j and 2j + 1, suffix sums by
+// shuffles, and tail is decreasing in d, so the degree is the first d whose bound passes.
+__device__ int ks_degree_warp(const KnSeries &ser, double rho, double target) {
   if (!(rho < 0.9)) return -1;
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31, n0 = 2 * lane;
   const double x = 0.25 * rho;
-  double term[kSeriesLen], xn = 1.0;
-  for (int n = 0; n < kSeriesLen; ++n) {
-    term[n] = fmax(fabs(ser.c[n]), fabs(ser.d[n])) * xn;
-    xn *= x;
+  double xn = 1.0, b = x;  // x^(2 lane) by repeated squaring
+  for (int e = n0; e; e >>= 1, b *= b)
+    if (e & 1) xn *= b;
+  const double t0 = fmax(fabs(ser.c[n0]), fabs(ser.d[n0])) * xn;
+  const double t1 = fmax(fabs(ser.c[n0 + 1]), fabs(ser.d[n0 + 1])) * (xn * x);
+  const double rem = __shfl_sync(full, t1, 31) * rho / (1.0 - rho);
+  if (rem > target) return -1;
+  // suf = sum of the pairs of lanes lane..31
+  double suf = t0 + t1;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double v = __shfl_down_sync(full, suf, o);
+    if (lane + o < 32) suf += v;
   }
-  // tail of degree n: sum_{m>n} term[m] + the remainder beyond the table
-  double tail = term[kSeriesLen - 1] * rho / (1.0 - rho);
-  if (tail > target) return -1;
-  int deg = kSeriesLen - 1;
-  for (int n = kSeriesLen - 1; n >= 1; --n) {
-    tail += term[n];
-    if (tail > target) break;
-    deg = n - 1;
-  }
-  return deg;
+  const double after = __shfl_down_sync(full, suf, 1);  // pairs of lanes lane+1..31
+  const double tail_odd = rem + (lane < 31 ? after : 0.0);  // d = 2 lane + 1
+  const double tail_even = tail_odd + t1;                     // d = 2 lane
+  const unsigned ok_even = __ballot_sync(full, tail_even <= target);
+  const unsigned ok_odd = __ballot_sync(full, tail_odd <= target);
+  const int le = ok_even ? __ffs(ok_even) - 1 : 64, lo = ok_odd ? __ffs(ok_odd) - 1 : 64;
+  const int d = min(2 * le, 2 * lo + 1);
+  return d < 64 ? d : 63;
 }
 
 // Block size s of the Paterson-Stockmeyer scheme: fewest dependent products, then the smallest.
@@ -192,10 +211,13 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
     f += 16.0 * z * z;
   }
   const double rho = sqrt(ks_cluster_sum(k, cluster, f, slots, red));
-  if (threadIdx.x == 0) {
-    plan[0] = ks_degree(ser, rho, a.ns_target);
-    plan[1] = ks_block_size(plan[0]);
-    plan[2] = kn_ns_steps(rho, a.ns_target);
+  if (threadIdx.x < 32) {
+    const int d = ks_degree_warp(ser, rho, a.ns_target);
+    if (threadIdx.x == 0) {
+      plan[0] = d;
+      plan[1] = ks_block_size(d);
+      plan[2] = d < 0 ? kn_ns_steps(rho, a.ns_target) : 0;
+    }
   }
   __syncthreads();
   const int deg = plan[0];
@@ -293,11 +315,8 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
     const double d = cv - (i == j ? 1.0 : 0.0);
     e2 += d * d;
   }
-  ks_mm(k, 0, nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.F);
-  if (a.fstack) {
-    ks_mm(k, nt, 2 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack);
-    ks_mm(k, 2 * nt, 3 * nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.fstack + 2 * ll);
-  }
+  // F once, written to F and to both F slots of the stack
+  ks_mm(k, 0, nt, -1.0, a.Dc, Ci, 1.0, C, 0.0, a.F, a.fstack, a.fstack ? a.fstack + 2 * ll : nullptr);
   const double err = sqrt(ks_cluster_sum(k, cluster, e2, slots + 32, red));
   if (k.rank == 0 && threadIdx.x == 0) {
     *a.err = err;

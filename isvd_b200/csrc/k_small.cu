@@ -16,7 +16,7 @@
 namespace isvdb {
 namespace {
 
-constexpr int kEigThreads = 512;
+constexpr int kEigThreads = 1024;
 constexpr int kMaxSweeps = 60;
 
 // Round-robin tournament: player i at round r (ne even, player 0 fixed).
@@ -34,9 +34,11 @@ __device__ __forceinline__ bool jacobi_rot(double app, double aqq, double apq, d
     s = 0.0;
     return false;
   }
-  const double tau = (aqq - app) / (2.0 * apq);
-  const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-  c = 1.0 / sqrt(1.0 + t * t);
+  // t = tan(theta) = sign(d) 2 apq / (|d| + sqrt(d^2 + 4 apq^2)), d = aqq - app: the smaller root of
+  // t^2 + (d / apq) t - 1 = 0, with one square root, one division and one reciprocal square root
+  const double d = aqq - app, e = 2.0 * apq;
+  const double t = (d >= 0.0 ? e : -e) / (fabs(d) + sqrt(d * d + e * e));
+  c = rsqrt(1.0 + t * t);
   s = t * c;
   return true;
 }
@@ -98,7 +100,7 @@ __global__ void __launch_bounds__(kEigThreads)
 
   const int nblk = np * (np + 1) / 2;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  constexpr int kMaxMine = 8;  // np <= 80: nblk <= 3240 <= 8 * 512 (covers n <= 160)
+  constexpr int kMaxMine = (3240 + kEigThreads - 1) / kEigThreads;  // np <= 80: nblk <= 3240 (n <= 160)
   short myI[kMaxMine], myJ[kMaxMine];
   int nmy = 0;
   for (int e = tid; e < nblk && nmy < kMaxMine; e += nt) {
