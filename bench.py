@@ -49,10 +49,10 @@ def peaks():
         return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-# DRAM bytes (read + write) of one full-panel launch of the sketch kernel (13312 x 20000 panel of
-# the config-2 matrix, N l = 4096): ncu capture of `bench.py --single --size panel`
-SKETCH_PANEL_TRAFFIC = 3.763120e9 + 0.217957e9
-SKETCH_PANEL_ROWS = 13312
+# DRAM bytes (read + write) of the sketch kernel's one launch over the config-2 matrix
+# (200000 x 20000, N l = 4096), from a one-pass ncu capture of a full solve (dram__bytes_read.sum +
+# dram__bytes_write.sum; see profiles/isvd_config2_mixed_launch_list.md)
+SKETCH_LAUNCH_TRAFFIC = 113.735330816e9 + 3.395452928e9
 
 
 class ClockSampler:
@@ -409,14 +409,14 @@ def main():
     # the sketch runs as back-to-back launches inside the solve: the sustained bf16 figure is its
     # denominator; the burst figure is reported beside it
     peak3, peak3_burst = bf16_sus / nprod, bf16 / nprod
-    full_panels = m // SKETCH_PANEL_ROWS if w["n"] == 20000 and l * N == 4096 else 0
+    config2 = (m, n, l * N) == (200000, 20000, 4096)
     roofline = {"bound": "tensor", "kernel": "umma_gemm_kernel (sketch Y = A Omega, %d bf16 plane products)" % nprod,
                 "achieved": achieved, "peak": peak3, "unit": "TFLOP/s",
                 "frac": (achieved / peak3) if achieved else None,
                 "peak_burst": peak3_burst, "frac_burst": (achieved / peak3_burst) if achieved else None,
-                "traffic": SKETCH_PANEL_TRAFFIC if full_panels else None,
-                "traffic_unit": "bytes per full-panel launch (13312 rows; ncu, dram read + write)",
-                "alg_bytes_per_panel": float(SKETCH_PANEL_ROWS * w["n"] * 4 + SKETCH_PANEL_ROWS * l * N * 4),
+                "traffic": SKETCH_LAUNCH_TRAFFIC if config2 and sketch_launches == 1 else None,
+                "traffic_unit": "bytes per launch (one launch over all m rows; ncu, dram read + write)",
+                "alg_bytes_per_launch": float(m * n * 4 + m * l * N * 4 + n * l * N * 2),
                 "convention": "algorithmic 2 m n Nl flops per solve / kernel time; peak = %s bf16 dense "
                               "sustained %.1f TFLOP/s / %d products (burst %.1f / %d also given)"
                               % (peak_kind, bf16_sus, nprod, bf16, nprod),
