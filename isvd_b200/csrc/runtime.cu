@@ -59,6 +59,7 @@ Runtime &Runtime::get() {
   CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
   CK(cudaMalloc(&g_rt.ctl, 4096));
   CK(cudaMemset(g_rt.ctl, 0, 4096));
+  CK(cudaMallocHost(&g_rt.host_pin, 64 * sizeof(double)));
   g_init = true;
   return g_rt;
 }
@@ -68,6 +69,7 @@ void Runtime::reset() {
   if (!g_init) return;
   cudaStreamSynchronize(g_rt.stream);
   cudaFree(g_rt.ctl);
+  cudaFreeHost(g_rt.host_pin);
   cudaStreamDestroy(g_rt.own_stream);
   cudaStreamDestroy(g_rt.copy_stream);
   g_rt = Runtime();

@@ -52,6 +52,8 @@ struct Runtime {
   size_t smem_optin = 0;
   // Device-resident control block (barrier counters, status words), zeroed at init.
   unsigned int *ctl = nullptr;
+  // Pinned host block (64 doubles) for small asynchronous read-backs (iteration errors).
+  double *host_pin = nullptr;
   static Runtime &get();  // initialises on first use (device = current device)
   static bool initialised();
   static void reset();    // releases stream and control block (isvd_Finalize_gpu)

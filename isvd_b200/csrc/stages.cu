@@ -219,7 +219,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     coeff_orthonormalize(c, Nl, l, N, G.p, Xo.p);
   }
   // iterates W = [M | B | Bgc] (Nl x 3l, current and next), [Dc; Dgc], step outputs
-  DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64), err(1);
+  DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64), err(2);
   double *Wc = Wb.p, *Wp = Wb.p + 3 * nl;
   copy2d<double, double>(G.p, Nl, 1, Wc + l, lw, 1, Nl, l, c.st);  // Bc = Qs' Q0 = G[:, 0:l]   (:157)
   set_identity<double>(Wc, Nl, l, lw, c.st);                       // Qc = Q0 = Qs [I; 0]       (:154)
@@ -230,7 +230,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   // One iteration: W(next) from W(cur).  After two eager iterations (which size every buffer and
   // set every kernel attribute) the iteration is captured as one CUDA graph per parity of the
   // ping-pong buffers, so that an iteration costs one graph launch plus the host read of err.
-  auto iteration = [&](double *Wcur, double *Wnext) {
+  auto iteration = [&](double *Wcur, double *Wnext, double *errp) {
     double *Bc = Wcur + l, *Bgc = Wcur + 2 * l;
     if (c.precision == kMixed) {  // Bgc = G Bc / N   (:174-177)
       gprod.apply(c, l, Bc, lw, invN, Bgc, lw);
@@ -254,7 +254,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     // l x l step (:187-218)
     CK(cudaMemsetAsync(rt.ctl, 0, 8, c.st));
     KnStep s;
-    s.l = l; s.Dc = DD.p; s.Dgc = DD.p + ll; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = err.p;
+    s.l = l; s.Dc = DD.p; s.Dgc = DD.p + ll; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = errp;
     s.work = work.p; s.status = c.status; s.bar = rt.ctl;
     s.ns_target = (c.precision == kMixed) ? 1e-12 : 1e-18;  // MIXED carries FP32-level errors anyway
     s.fstack = Fs.p; s.fstack_scale = invN;
@@ -273,17 +273,38 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   IterResult res;
   double herr = 0.0;
   const int cap = maxit > 0 ? maxit : 1000000;
+  // Iteration i + 1 is queued before the host reads the error of iteration i (copied into pinned
+  // memory right behind iteration i), so the GPU never waits for the host's convergence test.
+  // Iteration i + 1 reads W(i) and writes the other buffer and error slot: when iteration i has
+  // converged, its result W(i) is intact and the extra iteration is discarded.
+  double *hpin = rt.host_pin;
+  cudaEvent_t ev[2];
+  for (int e = 0; e < 2; ++e) CK(cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
+  auto launch = [&](int it, double *cur, double *next) {
+    const int par = it & 1;
+    if (graphs.usable && it > 2) graphs.run(par, [&] { iteration(cur, next, err.p + par); });
+    else iteration(cur, next, err.p + par);
+    CK(cudaMemcpyAsync(hpin + par, err.p + par, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    CK(cudaEventRecord(ev[par], c.st));
+  };
   int iter = 1;
-  for (;; ++iter) {
-    const int par = iter & 1;
-    if (graphs.usable && iter > 2) graphs.run(par, [&] { iteration(Wc, Wp); });
-    else iteration(Wc, Wp);
-    CK(cudaMemcpyAsync(&herr, err.p, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+  try {
+    launch(1, Wc, Wp);
+    for (;; ++iter) {
+      if (iter < cap) launch(iter + 1, Wp, Wc);  // speculative next iteration
+      CK(cudaEventSynchronize(ev[iter & 1]));
+      herr = hpin[iter & 1];
+      if (!(herr == herr) || iter % 16 == 0) read_status(c, "Kolmogorov-Nagumo integration");
+      if (herr <= tol) break;                                  // (:235-237)
+      if (iter == cap) { ++iter; break; }                      // (:238-241)
+      std::swap(Wc, Wp);
+    }
     read_status(c, "Kolmogorov-Nagumo integration");
-    if (herr <= tol) break;                                    // (:235-237)
-    if (iter == cap) { ++iter; break; }                        // (:238-241)
-    std::swap(Wc, Wp);
+  } catch (...) {
+    for (int e = 0; e < 2; ++e) cudaEventDestroy(ev[e]);
+    throw;
   }
+  for (int e = 0; e < 2; ++e) cudaEventDestroy(ev[e]);
   res.iterations = iter;
   res.error = herr;
   // Qbar = Qs M+  (:251)
