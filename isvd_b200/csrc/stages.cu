@@ -120,7 +120,12 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
     gemm(g, c.st);
     copy2d<double, T>(P.p, l, 1, Wp.p, l, 1, (long long)N * l, l, c.st);
   }
-  // Q_i = Y_i F_i  (:95-98; the product goes to a temporary and is copied back)
+  // Q_i = Y_i F_i  (:95-98).  MIXED with planes: the product reads only the planes, so it writes
+  // y in place; otherwise it goes to a temporary that is copied back.
+  if (c.precision == kMixed && l % 64 == 0) {
+    mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, y, ldy);
+    return;
+  }
   DBuf<T> tmp((size_t)m * Nl);
   if (c.precision == kMixed) {
     mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, tmp.p, Nl);

@@ -2,6 +2,8 @@
 against FP64: every stage on the reference goldens, and end to end against the FP64 path with
 the same Omega.  Tolerance: singular values within 1e-5 relative, largest principal angle of U
 and V within 1e-4 (the mixed-precision bar); products within FP32 rounding (1e-6 relative)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -212,6 +214,39 @@ def test_mixed_driver_vs_fp64(lib, oracle, x):
     assert np.abs(s1 - s0).max() / s0.max() < 1e-5
     assert oracle.max_principal_angle(u1[:, :k], u0[:, :k]) < 1e-4
     assert oracle.max_principal_angle(v1[:, :k], v0[:, :k]) < 1e-4
+
+
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_mixed_driver_wide_blocks(lib, oracle, where):
+    """l = 64 (device A: one sketch launch; host A: one per streamed 512-row panel): the Gramian
+    orthogonalization's block applies read only Y's planes and write Qs in place.  Against the
+    FP64 path with the same Omega."""
+    torch = pytest.importorskip("torch")
+    m, n, k, p, Nn = 3000, 1500, 40, 24, 8
+    l = k + p
+    a = lowrank(m, n, 400, 10 ** (-3 / 400), 1e-6, 29)
+    om = np.random.default_rng(5).standard_normal((n, l * Nn))
+    prm = lib.create_param(m, n, k, p, Nn)
+    s0 = np.zeros(l); u0 = np.zeros((m, l)); v0 = np.zeros((n, l))
+    retv0, _, st = lib.isvd("d", prm, ("GP", "GR", "KN", "GR"), np.ascontiguousarray(a), n, s0, u0, l, v0, l,
+                            omega=np.ascontiguousarray(om), ldomega=l * Nn, precision=0)
+    assert st == 0, lib.last_error()
+    a32 = np.ascontiguousarray(a.astype(np.float32))
+    if where == "device":
+        a32 = torch.from_numpy(a32).cuda()
+    else:
+        os.environ["ISVD_GPU_PANEL_ROWS"] = "512"
+    try:
+        s1 = np.zeros(l, np.float32); u1 = np.zeros((m, l), np.float32); v1 = np.zeros((n, l), np.float32)
+        retv1, _, st = lib.isvd("s", prm, ("GP", "GR", "KN", "GR"), a32, n, s1, u1, l, v1, l,
+                                omega=np.ascontiguousarray(om.astype(np.float32)), ldomega=l * Nn, precision=1)
+    finally:
+        os.environ.pop("ISVD_GPU_PANEL_ROWS", None)
+    assert st == 0, lib.last_error()
+    assert abs(int(retv1[2][0]) - int(retv0[2][0])) <= 1
+    assert np.abs(s1 - s0).max() / s0.max() < 1e-5
+    assert oracle.max_principal_angle(u1[:, :k].astype(np.float64), u0[:, :k]) < 1e-4
+    assert oracle.max_principal_angle(v1[:, :k].astype(np.float64), v0[:, :k]) < 1e-4
 
 
 @pytest.mark.parametrize("ordera", [b"R", b"C"])
