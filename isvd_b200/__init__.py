@@ -10,6 +10,8 @@ import os
 from .capi import MPI_COMM_WORLD, IsvdLib, Param, ptr  # noqa: F401
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libisvd_gpu_b200.so")
+# ILP64 build (isvd_int_t = int64), the reference's "_64" variant: IsvdLib(LIB64_PATH)
+LIB64_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libisvd_gpu_b200_64.so")
 PRECISION_NATIVE = 0
 PRECISION_MIXED = 1
 

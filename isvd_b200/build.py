@@ -1,11 +1,14 @@
 """Build libisvd_gpu_b200.so in-tree with nvcc for sm_100a.
 
-    python -m isvd_b200.build [--force] [--verbose]
+    python -m isvd_b200.build [--force] [--verbose] [--ilp64]
 
 Each CUDA source under isvd_b200/csrc is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`` and the objects are linked
 into ``isvd_b200/libisvd_gpu_b200.so`` (static CUDA runtime, C ABI of include/isvd.h).
-Sources are rebuilt only when they (or a header) are newer than their object.
+``--ilp64`` builds the 64-bit-index variant (``isvd_int_t`` = int64, ``-DISVD_USE_ILP64``)
+as ``isvd_b200/libisvd_gpu_b200_64.so``, the reference's ``_64`` suffix for that build
+(reference cmake/options.cmake:50-61).  Sources are rebuilt only when they (or a header) are
+newer than their object.
 """
 import glob
 import os
@@ -18,6 +21,8 @@ REPO = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libisvd_gpu_b200.so")
+OBJ64 = os.path.join(HERE, "_build64")
+LIB64 = os.path.join(HERE, "libisvd_gpu_b200_64.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-Xcompiler", "-fvisibility=hidden,-fvisibility-inlines-hidden",
@@ -31,7 +36,20 @@ def _newest_header():
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 
 
-def build(force=False, verbose=False, extra=()):
+def build(force=False, verbose=False, extra=(), ilp64=False):
+    if ilp64:
+        return _build(OBJ64, LIB64, force, verbose, tuple(extra) + ("-DISVD_USE_ILP64",))
+    return _build(OBJ, LIB, force, verbose, extra)
+
+
+def build_all(force=False, verbose=False):
+    """Both index variants: the LP64 library and the ILP64 (_64) one."""
+    lib = build(force, verbose)
+    build(force, verbose, ilp64=True)
+    return lib
+
+
+def _build(OBJ, LIB, force, verbose, extra):
     os.makedirs(OBJ, exist_ok=True)
     # a change of compiler flags rebuilds everything
     stamp = os.path.join(OBJ, "flags.txt")
@@ -74,4 +92,4 @@ def build(force=False, verbose=False, extra=()):
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv))
+    print(build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, ilp64="--ilp64" in sys.argv))

@@ -23,10 +23,20 @@ _PARAM_INT_FIELDS = ["nrow", "ncol", "nrow_proc", "ncol_proc", "nrow_each", "nco
                      "dim_sketch", "dim_sketch_total", "num_sketch"]
 
 
-class Param(ctypes.Structure):
-    """isvd_Param (include/isvd/core/param.h; reference core/param.h:27-92)."""
-    _fields_ = [("mpi_comm", ctypes.c_int), ("mpi_size", c_mpi_int), ("mpi_root", c_mpi_int),
-                ("mpi_rank", c_mpi_int)] + [(f, c_int_t) for f in _PARAM_INT_FIELDS]
+_PARAM_CLASSES = {}
+
+
+def param_class(cint):
+    """isvd_Param (include/isvd/core/param.h; reference core/param.h:27-92) for the index type
+    `cint` (ctypes.c_int32: the LP64 build; ctypes.c_int64: the ILP64 build)."""
+    if cint not in _PARAM_CLASSES:
+        _PARAM_CLASSES[cint] = type("Param" if cint is ctypes.c_int32 else "Param64", (ctypes.Structure,), {
+            "_fields_": [("mpi_comm", ctypes.c_int), ("mpi_size", c_mpi_int), ("mpi_root", c_mpi_int),
+                         ("mpi_rank", c_mpi_int)] + [(f, cint) for f in _PARAM_INT_FIELDS]})
+    return _PARAM_CLASSES[cint]
+
+
+Param = param_class(c_int_t)
 
 
 _VP = ctypes.c_void_p
@@ -53,32 +63,38 @@ def _dt(x):
 class IsvdLib:
     """Thin wrapper over one shared library exporting the iSVD C ABI."""
 
-    STAGE_HEAD = [Param, _VP, c_int_t, _VP, c_int_t]   # param, argv, argc, retv, retc
-
-    def __init__(self, path, mode=ctypes.RTLD_LOCAL):
+    def __init__(self, path, mode=ctypes.RTLD_LOCAL, ilp64=None):
+        """ilp64: the library's isvd_int_t is int64 (default: a file name ending in _64.so, the
+        reference's suffix for that build)."""
         self.path = os.path.abspath(path)
+        if ilp64 is None:
+            ilp64 = self.path.endswith("_64.so")
+        self.ilp64 = bool(ilp64)
+        self.c_int_t = ctypes.c_int64 if self.ilp64 else ctypes.c_int32
+        self.Param = param_class(self.c_int_t)
+        self.STAGE_HEAD = [self.Param, _VP, self.c_int_t, _VP, self.c_int_t]  # param, argv, argc, retv, retc
         self.lib = ctypes.CDLL(self.path, mode=mode)
         L = self.lib
-        L.isvd_createParam.restype = Param
-        L.isvd_createParam.argtypes = [c_int_t] * 5 + [c_mpi_int, ctypes.c_int]
+        L.isvd_createParam.restype = self.Param
+        L.isvd_createParam.argtypes = [self.c_int_t] * 5 + [c_mpi_int, ctypes.c_int]
         H = self.STAGE_HEAD
         for x in "sd":
             self._decl("isvd_%sSketchGaussianProjection" % x,
-                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, c_int_t, c_mpi_int])
+                       H + [_CH, _CH, _VP, self.c_int_t, _VP, self.c_int_t, self.c_int_t, c_mpi_int])
             self._decl("isvd_%sSketchGaussianProjection_gpu" % x,
-                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, c_int_t, c_mpi_int])
+                       H + [_CH, _CH, _VP, self.c_int_t, _VP, self.c_int_t, self.c_int_t, c_mpi_int])
             for name in ("OrthogonalizeTallSkinnyQr", "OrthogonalizeGramian"):
-                self._decl("isvd_%s%s" % (x, name), H + [_VP, c_int_t])
+                self._decl("isvd_%s%s" % (x, name), H + [_VP, self.c_int_t])
             for name in ("IntegrateKolmogorovNagumo", "IntegrateWenYin", "IntegrateHierarchicalReduction"):
-                self._decl("isvd_%s%s" % (x, name), H + [_VP, c_int_t, _VP, c_int_t])
-            post = H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t, c_mpi_int, c_mpi_int]
+                self._decl("isvd_%s%s" % (x, name), H + [_VP, self.c_int_t, _VP, self.c_int_t])
+            post = H + [_CH, _CH, _VP, self.c_int_t, _VP, self.c_int_t, _VP, _VP, self.c_int_t, _VP, self.c_int_t, c_mpi_int, c_mpi_int]
             for name in ("PostprocessTallSkinnyQr", "PostprocessGramian", "PostprocessSymmetric"):
                 self._decl("isvd_%s%s" % (x, name), post)
                 self._decl("isvd_%s%s_gpu" % (x, name), post)
             self._decl("isvd_%sIsvd" % x,
-                       [Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
-                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t,
-                        c_int_t, c_mpi_int, c_mpi_int])
+                       [self.Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, self.c_int_t, _VP, _VP, self.c_int_t, _VP, self.c_int_t,
+                        self.c_int_t, c_mpi_int, c_mpi_int])
 
         # B200 extensions (include/isvd/b200.h)
         self._decl("isvd_gpu_get_last_error", [], ctypes.c_int)
@@ -96,11 +112,11 @@ class IsvdLib:
                    ctypes.c_int)
         for x in "sd":
             self._decl("isvd_%sSketchGaussianProjectionOmega" % x,
-                       H + [_CH, _CH, _VP, c_int_t, _VP, c_int_t, _VP, c_int_t])
+                       H + [_CH, _CH, _VP, self.c_int_t, _VP, self.c_int_t, _VP, self.c_int_t])
             self._decl("isvd_%sIsvd_ex" % x,
-                       [Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
-                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, c_int_t, _VP, _VP, c_int_t, _VP, c_int_t,
-                        c_int_t, c_mpi_int, c_mpi_int, _VP, c_int_t, ctypes.c_int], ctypes.c_int)
+                       [self.Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                        _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, self.c_int_t, _VP, _VP, self.c_int_t, _VP, self.c_int_t,
+                        self.c_int_t, c_mpi_int, c_mpi_int, _VP, self.c_int_t, ctypes.c_int], ctypes.c_int)
 
     def _decl(self, name, argtypes, restype=None):
         fn = getattr(self.lib, name, None)
@@ -180,14 +196,14 @@ class IsvdLib:
         dt = _dt(x)
         keep = []
         argv_arr = (ctypes.c_void_p * 4)()
-        argc_arr = (c_int_t * 4)()
+        argc_arr = (self.c_int_t * 4)()
         for i in range(4):
             av = None if argv is None or argv[i] is None else np.ascontiguousarray(argv[i], dtype=dt)
             keep.append(av)
             argv_arr[i] = ptr(av)
             argc_arr[i] = 0 if av is None else len(av)
         retv_arr = (ctypes.c_void_p * 4)()
-        retc_arr = (c_int_t * 4)()
+        retc_arr = (self.c_int_t * 4)()
         rvs = []
         for i in range(4):
             rv = np.zeros(max(retc[i], 1), dtype=dt)

@@ -116,6 +116,11 @@ const char *arg2str(const char *name, const char *arg, const char *const *opts, 
 void require_single_rank(const isvd_Param &p) {
   if (p.mpi_size != 1)
     fail(kErrUnsupported, "MPI size %d: this build runs one MPI rank per GPU (P = 1)", (int)p.mpi_size);
+  // the ILP64 build takes 64-bit sizes at the boundary; one GPU's kernels index rows, columns and
+  // sketch widths with 32-bit integers (element offsets are 64-bit)
+  const long long lim = 2147483647LL;
+  if ((long long)p.nrow > lim || (long long)p.ncol > lim || (long long)p.dim_sketch_total > lim)
+    fail(kErrUnsupported, "sizes beyond 2^31 - 1 rows, columns or sketch columns are not supported on one GPU");
 }
 
 template <class T>

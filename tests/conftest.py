@@ -64,3 +64,13 @@ def lib():
     """The product library (libisvd_gpu_b200.so)."""
     import isvd_b200
     return isvd_b200.load()
+
+
+@pytest.fixture(scope="session")
+def lib64():
+    """The ILP64 build of the product library (libisvd_gpu_b200_64.so: isvd_int_t = int64)."""
+    import isvd_b200
+    if not os.path.exists(isvd_b200.LIB64_PATH):
+        raise RuntimeError("libisvd_gpu_b200_64.so is not built; run `python -m isvd_b200.build --ilp64`")
+    from isvd_b200.capi import IsvdLib
+    return IsvdLib(isvd_b200.LIB64_PATH)

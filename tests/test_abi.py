@@ -104,6 +104,26 @@ def test_query_defaults_without_gpu(lib, reflib):
         assert np.allclose(lib.query("s", alg, n), reflib.query("s", alg, n))
 
 
+def test_ilp64_library_exports_the_same_abi(lib, lib64):
+    """The ILP64 build (reference cmake/options.cmake:50-61: isvd_int_t = int64, suffix _64) exports
+    exactly the LP64 build's entry points."""
+    assert exported_symbols(lib64.path) == exported_symbols(lib.path)
+
+
+@pytest.mark.parametrize("m,n,k,p,N", [(2000, 1000, 20, 12, 16), (5_000_000_000, 3, 2, 1, 3)])
+def test_ilp64_param_fields_are_64_bit(lib, lib64, m, n, k, p, N):
+    """isvd_Param's index fields are int64 in the ILP64 build: a row count beyond int32 survives."""
+    import ctypes as ct
+    assert lib64.Param.nrow.size == 8 and lib.Param.nrow.size == 4
+    a = lib64.create_param(m, n, k, p, N)
+    assert a.nrow == m and a.dim_sketch == k + p and a.dim_sketch_total == (k + p) * N
+    if m < 2 ** 31:
+        b = lib.create_param(m, n, k, p, N)
+        for f, _ in b._fields_:
+            assert getattr(a, f) == getattr(b, f), f
+    assert ct.sizeof(lib64.Param) > ct.sizeof(lib.Param)
+
+
 def build_c_demo(tmp_path, lib):
     """Compile tests/c/isvd_demo.c against include/ and link it with the library (plain gcc)."""
     exe = str(tmp_path / "isvd_demo")
@@ -118,4 +138,15 @@ def build_c_demo(tmp_path, lib):
 def test_c_caller_compiles_and_links(tmp_path, lib):
     """A C program written against include/isvd.h builds and links against the library alone."""
     exe = build_c_demo(tmp_path, lib)
+    assert os.path.exists(exe)
+
+
+def test_c_caller_links_ilp64(tmp_path, lib64):
+    """The same C program compiled with -DISVD_USE_ILP64 links against the _64 library."""
+    exe = str(tmp_path / "isvd_demo64")
+    libdir = os.path.dirname(lib64.path)
+    cmd = ["gcc", "-std=gnu99", "-O1", "-Wall", "-Werror", "-DISVD_USE_ILP64", "-I", os.path.join(REPO, "include"),
+           "-I", os.path.join(REPO, "include", "mpi_shim"), os.path.join(REPO, "tests", "c", "isvd_demo.c"), "-o",
+           exe, "-L" + libdir, "-lisvd_gpu_b200_64", "-Wl,-rpath," + libdir, "-lm"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
     assert os.path.exists(exe)
