@@ -6,6 +6,8 @@
 #ifndef ISVD_B200_H_
 #define ISVD_B200_H_
 
+#include <stddef.h>
+
 #include <isvd/def.h>
 #include <isvd/core/param.h>
 
@@ -165,6 +167,37 @@ int isvd_dSvdAdjoint(
     const isvd_d_val_t *dvt, const isvd_int_t lddvt, isvd_d_val_t *da, const isvd_int_t ldda,
     const int cg_iters, const double tol, int *iterations
 );
+
+/* ---------------------------------------------------------------- several ranks without MPI
+ * Row-block execution over P processes (one GPU each) whose only exchange is a sum-AllReduce
+ * that the caller supplies (NCCL, MPI, gloo ...).  It stands in for the reference's own MPI
+ * collectives (MPI_Allreduce in core/stage/@x@_integrate_kolmogorov_nagumo.c:160,178,
+ * @x@_integrate_wen_yin.c:206-345, @x@_postprocess_gramian.c:146, ...), which this single-rank
+ * build does not call.  After isvd_gpu_set_allreduce(fn, user, nranks, rank, on_device):
+ *   - isvd_getMpiSize / isvd_getMpiRank return nranks / rank, so isvd_createParam gives the
+ *     reference's row blocks (this rank holds rows [rowidxbegin, rowidxend) = nrow_proc rows);
+ *   - with dista 'R' the driver (and the sketch, orthogonalization and integration stages) take
+ *     this rank's rows of A, yst and qt, and exchange through fn: the N block Grams (Gramian
+ *     orthogonalization; each CholeskyQR pass and the top rows for the sign rule of the
+ *     tall-skinny QR), G = Qs'Qs (KN, WY: one exchange per solve
+ *     instead of two per iteration; every rank then runs the same iterations on the same G) and
+ *     Z = A'Qbar (Gramian postprocessing);
+ *   - outputs as the reference's: ut_root = -1 leaves this rank's rows of U in ut, ut_root >= 0
+ *     gathers all m rows on that rank; vt_root = -1 leaves this rank's column block of V
+ *     (rows [colidxbegin, colidxend)) in vt, vt_root >= 0 all n rows on that rank (the other
+ *     ranks keep their own rows / column block, as after the reference's MPI_Gather);
+ *   - fn(buf, count, dtype, stream, user) sums `count` values of type dtype (ISVD_GPU_DTYPE_F32 /
+ *     ISVD_GPU_DTYPE_F64) at buf over the ranks, in place.  on_device = 1: buf is device memory
+ *     and fn enqueues the reduction on `stream` (a cudaStream_t); on_device = 0: buf is pinned host
+ *     memory (the library copies through it and synchronises around the call);
+ *   - with nranks > 1, dista 'C', HR integration, TS / SY postprocessing and the postprocessing
+ *     stage called on its own return ISVD_GPU_ERROR_UNSUPPORTED.
+ * nranks = 1 or fn = NULL returns to single-process execution.  Every rank must make the same
+ * calls in the same order. */
+#define ISVD_GPU_DTYPE_F32 0
+#define ISVD_GPU_DTYPE_F64 1
+typedef void (*isvd_gpu_allreduce_fn)( void *buf, size_t count, int dtype, void *stream, void *user );
+void isvd_gpu_set_allreduce( isvd_gpu_allreduce_fn fn, void *user, int nranks, int rank, int on_device );
 
 /* ---------------------------------------------------------------- no device allocation
  * Kolmogorov-Nagumo integration in FP64 that allocates no device memory: no cudaMalloc or

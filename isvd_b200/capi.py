@@ -60,6 +60,49 @@ def _dt(x):
     return np.float32 if x == "s" else np.float64
 
 
+# isvd_gpu_allreduce_fn (include/isvd/b200.h): (buf, count, dtype, stream, user)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_void_p,
+                                ctypes.c_void_p)
+
+
+def host_array(buf, count, dtype):
+    """NumPy view of the `count` values at host address `buf` (dtype 0: FP32, 1: FP64)."""
+    ct = ctypes.c_float if dtype == 0 else ctypes.c_double
+    return np.ctypeslib.as_array((ct * count).from_address(buf))
+
+
+def torch_host_allreduce(group=None):
+    """A host-memory sum-AllReduce over torch.distributed (e.g. the gloo backend) for
+    IsvdLib.set_allreduce(..., on_device=False)."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(buf, count, dtype, stream, user):
+        dist.all_reduce(torch.from_numpy(host_array(buf, count, dtype)), group=group)
+    return fn
+
+
+class _DeviceBuffer:
+    """`count` values at a device address, exposed through __cuda_array_interface__."""
+
+    def __init__(self, buf, count, dtype):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f4" if dtype == 0 else "<f8",
+                                         "data": (buf, False), "version": 2, "strides": None}
+
+
+def torch_device_allreduce(group=None):
+    """A device-memory sum-AllReduce over torch.distributed (NCCL, or gloo with CUDA tensors) for
+    IsvdLib.set_allreduce(..., on_device=True): the reduction is ordered on the library's stream."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(buf, count, dtype, stream, user):
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream or 0)):
+            t = torch.as_tensor(_DeviceBuffer(buf, count, dtype), device="cuda")
+            dist.all_reduce(t, group=group)
+    return fn
+
+
 class IsvdLib:
     """Thin wrapper over one shared library exporting the iSVD C ABI."""
 
@@ -107,6 +150,8 @@ class IsvdLib:
         self._decl("isvd_gpu_set_stream", [_VP])
         self._decl("isvd_gpu_get_stream", [], _VP)
         self._decl("isvd_gpu_profile_reset", [])
+        self._decl("isvd_gpu_set_allreduce", [ALLREDUCE_FN, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int])
+        self._allreduce_cb = None
         self._decl("isvd_gpu_profile_get", [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_ulonglong), ctypes.POINTER(ctypes.c_double)],
                    ctypes.c_int)
@@ -127,6 +172,13 @@ class IsvdLib:
 
     def has(self, name):
         return hasattr(self.lib, name)
+
+    def set_allreduce(self, fn, nranks, rank, on_device=False):
+        """Join `nranks` processes as row blocks (isvd_gpu_set_allreduce): fn(buf, count, dtype,
+        stream, user) sums in place over the ranks.  fn = None returns to one process."""
+        self._allreduce_cb = ALLREDUCE_FN(fn) if fn is not None else ALLREDUCE_FN()
+        self.lib.isvd_gpu_set_allreduce(self._allreduce_cb, None, nranks if fn is not None else 1, rank if fn else 0,
+                                        1 if on_device else 0)
 
     # ------------------------------------------------------------------ parameters
     def create_param(self, m, n, k, p, N, root=0, comm=MPI_COMM_WORLD):

@@ -114,8 +114,11 @@ const char *arg2str(const char *name, const char *arg, const char *const *opts, 
 }
 
 void require_single_rank(const isvd_Param &p) {
-  if (p.mpi_size != 1)
-    fail(kErrUnsupported, "MPI size %d: this build runs one MPI rank per GPU (P = 1)", (int)p.mpi_size);
+  // several ranks: only through the caller's AllReduce (isvd_gpu_set_allreduce), row blocks
+  const Collective &cl = collective();
+  if (p.mpi_size != 1 && !(cl.nranks == p.mpi_size && cl.rank == p.mpi_rank))
+    fail(kErrUnsupported, "MPI size %d: this build joins several ranks only through isvd_gpu_set_allreduce",
+         (int)p.mpi_size);
   // the ILP64 build takes 64-bit sizes at the boundary; one GPU's kernels index rows, columns and
   // sketch widths with 32-bit integers (element offsets are 64-bit)
   const long long lim = 2147483647LL;
@@ -182,7 +185,9 @@ void sketch_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, is
   const char dista_ = arg2char("DISTA", dista, "CR");
   const char ordera_ = arg2char("ORDERA", ordera, "CR");
   require_single_rank(p);
-  const int m = p.nrow, n = p.ncol, Nl = p.dim_sketch_total;
+  if (p.mpi_size > 1 && dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
+  // several ranks: this rank's rows [rowidxbegin, rowidxend) of A and Y
+  const int m = p.mpi_size > 1 ? (int)p.nrow_proc : (int)p.nrow, n = p.ncol, Nl = p.dim_sketch_total;
   if (dista_ == 'C') {
     REQUIRE(ordera_ == 'C' ? lda >= m : lda >= p.ncol_proc);
     REQUIRE(ldyst == Nl);
@@ -212,8 +217,9 @@ void orth_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd
   require_single_rank(p);
   const int m = p.nrow_proc, l = p.dim_sketch, N = p.num_sketch, Nl = p.dim_sketch_total;
   REQUIRE(ldyst >= Nl);
-  if (tsqr) REQUIRE(m >= l);
+  if (tsqr) REQUIRE(p.nrow >= l);
   Ctx c(-1);
+  if (p.mpi_size > 1) c.sc.m_total = p.nrow;
   View<T> Y;
   Y.bind(yst, Nl, m, ldyst, true, c.sc.st);
   if (tsqr) orth_tsqr_dev<T>(c.sc, m, l, N, Y.d, ldyst);
@@ -300,6 +306,7 @@ void post_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd
   const char dista_ = arg2char("DISTA", dista, "CR");
   const char ordera_ = arg2char("ORDERA", ordera, "CR");
   require_single_rank(p);
+  if (p.mpi_size > 1) fail(kErrUnsupported, "several ranks: postprocessing runs inside isvd_?Isvd (the driver)");
   const int m = p.nrow, n = p.ncol, k = p.rank, l = p.dim_sketch;
   if (alg == 2) {
     // symmetric: U and V are the same matrix; the first requested one is computed (:101-104)
@@ -438,6 +445,15 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   require_single_rank(p);
   const int m = p.nrow, n = p.ncol, k = p.rank, l = p.dim_sketch, N = p.num_sketch, Nl = p.dim_sketch_total;
   const bool root = p.mpi_rank == p.mpi_root;
+  // several ranks (isvd_gpu_set_allreduce): this rank holds rows [rowidxbegin, rowidxend) of A
+  const bool multi = p.mpi_size > 1;
+  if (multi) {
+    if (dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
+    if (bi == "HR" || bp != "GR")
+      fail(kErrUnsupported, "several ranks: Gramian or TS orthogonalization, KN or WY integration and Gramian "
+                            "postprocessing only");
+  }
+  const int ml = multi ? (int)p.nrow_proc : m;  // rows of A held here
   if (stream && root) {
     const char *tn = TypeName<T>::name;
     fprintf(stream, "Using %s Precision %s.\n", tn, alg_name('S', "GP", true));
@@ -460,6 +476,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   cudaStream_t st = c.sc.st;
   MixedCache mcache;  // A's bf16 planes, shared by the sketch and the postprocess
   c.sc.cache = &mcache;
+  if (multi) c.sc.m_total = m;
   StageTimer tm;
   auto progress = [&](const char *what) {
     if (stream && root) { fprintf(stream, "%s", what); fflush(stream); }
@@ -476,13 +493,13 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   const bool mixed = c.sc.precision == kMixed;
   View<T> A, Om;
   if (!mixed) {
-    if (ordera_ == 'R') A.bind(a, n, m, lda, true, st);
-    else A.bind(a, m, n, lda, true, st);
+    if (ordera_ == 'R') A.bind(a, n, ml, lda, true, st);
+    else A.bind(a, ml, n, lda, true, st);
   }
   const T *a_use = mixed ? a : A.d;
   if (omega) Om.bind(omega, Nl, n, ldomega, true, st);
-  DBuf<T> Y((size_t)m * Nl), Q((size_t)m * l);
-  sketch_dev<T>(c.sc, m, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
+  DBuf<T> Y((size_t)ml * Nl), Q((size_t)ml * l);
+  sketch_dev<T>(c.sc, ml, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
                 Nl);
   tm.mark(1, st);
   sync();
@@ -490,7 +507,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   // ---- orthogonalize
   progress("Orthogonalizing ............... ");
   if (bo == "TS") {
-    orth_tsqr_dev<T>(c.sc, m, l, N, Y.p, Nl);
+    orth_tsqr_dev<T>(c.sc, ml, l, N, Y.p, Nl);
   } else {
     // KN and WY form G = Qs' Qs anyway: they take over the second pass in the coordinates of G
     c.sc.deferred_orth = (bi == "KN" || bi == "WY");
@@ -498,7 +515,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
     // so the blocks' bases are free: Cholesky factors instead of eigendecompositions.  (The TS
     // postprocessing of the reference depends on the basis of Qbar, so it keeps the eigenbasis.)
     c.sc.chol_basis = (bp != "TS");
-    orth_gramian_dev<T>(c.sc, m, l, N, Y.p, Nl);
+    orth_gramian_dev<T>(c.sc, ml, l, N, Y.p, Nl);
     c.sc.chol_basis = false;
   }
   tm.mark(2, st);
@@ -512,7 +529,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
     const int maxit = (ac[2] > ++ai) ? (int)av[2][ai] : 256;
     const double tol = (ac[2] > ++ai) ? (double)av[2][ai] : 1e-4;
     REQUIRE(maxit >= 0 && tol >= 0);
-    ir = integrate_kn_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l, maxit, tol);
+    ir = integrate_kn_dev<T>(c.sc, ml, l, N, Y.p, Nl, Q.p, l, maxit, tol);
   } else if (bi == "WY") {
     WyArgs w;
     int ai = -1;
@@ -526,9 +543,9 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
     if (ac[2] > ++ai) w.beta = x[ai];
     if (ac[2] > ++ai) w.sigma = x[ai];
     if (ac[2] > ++ai) w.eta = x[ai];
-    ir = integrate_wy_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l, w);
+    ir = integrate_wy_dev<T>(c.sc, ml, l, N, Y.p, Nl, Q.p, l, w);
   } else {
-    integrate_hr_dev<T>(c.sc, m, l, N, Y.p, Nl, Q.p, l);
+    integrate_hr_dev<T>(c.sc, ml, l, N, Y.p, Nl, Q.p, l);
   }
   tm.mark(3, st);
   sync();
@@ -558,6 +575,42 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
                            st));
       V2.back(st, k);
       sync();
+    }
+  } else if (multi) {
+    // row blocks: U rows of this rank; V (all n rows) is the same on every rank
+    const bool wu = ut_root >= -1, wv = vt_root >= -1;
+    DBuf<T> Ul((size_t)ml * l), Vf((size_t)n * l);
+    post_gramian_dev<T>(c.sc, ml, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, Ul.p, l, Vf.p, l, wu, wv);
+    tm.mark(4, st);
+    S.back(st);
+    const bool me_u = ut_root < 0 || ut_root != p.mpi_rank;  // this rank's rows only
+    if (wu && me_u) {
+      U.bind(ut, k, ml, ldut, false, st);
+      CK(cudaMemcpy2DAsync(U.d, ldut * sizeof(T), Ul.p, l * sizeof(T), k * sizeof(T), ml, cudaMemcpyDeviceToDevice,
+                           st));
+      U.back(st, k);
+    }
+    if (ut_root >= 0) {  // gather (reference MPI_Gather, @x@_postprocess_gramian.c:162-165): a sum of
+      DBuf<T> Ug((size_t)m * l);  // zero-padded copies of the ranks' rows
+      CK(cudaMemsetAsync(Ug.p, 0, (size_t)m * l * sizeof(T), st));
+      CK(cudaMemcpyAsync(Ug.p + (size_t)p.rowidxbegin * l, Ul.p, (size_t)ml * l * sizeof(T), cudaMemcpyDeviceToDevice,
+                         st));
+      allreduce_sum(Ug.p, (size_t)m * l, st);
+      if (ut_root == p.mpi_rank) {
+        U.bind(ut, k, m, ldut, false, st);
+        CK(cudaMemcpy2DAsync(U.d, ldut * sizeof(T), Ug.p, l * sizeof(T), k * sizeof(T), m, cudaMemcpyDeviceToDevice,
+                             st));
+        U.back(st, k);
+      }
+    }
+    if (wv) {  // this rank's column block; all rows at the root (reference MPI_Gather, :176-183)
+      const bool all = vt_root >= 0 && vt_root == p.mpi_rank;
+      const long long v0 = all ? 0 : (long long)p.colidxbegin;
+      const long long vn = all ? (long long)n : (long long)p.ncol_proc;
+      V.bind(vt, k, vn, ldvt, false, st);
+      CK(cudaMemcpy2DAsync(V.d, ldvt * sizeof(T), Vf.p + v0 * l, l * sizeof(T), k * sizeof(T), vn,
+                           cudaMemcpyDeviceToDevice, st));
+      V.back(st, k);
     }
   } else {
     const bool wu = ut_root >= -1, wv = vt_root >= -1;
@@ -698,14 +751,31 @@ int isvd_gpu_profile_get(const char *tag, double *ms, unsigned long long *launch
 
 // ---------------------------------------------------------------- utilities
 mpi_int_t isvd_getMpiSize(const isvd_MpiComm comm) {
+  if (collective().nranks > 1) return collective().nranks;  // ranks joined by isvd_gpu_set_allreduce
   int s = 0;
   MPI_Comm_size(comm, &s);
   return s;
 }
 mpi_int_t isvd_getMpiRank(const isvd_MpiComm comm) {
+  if (collective().nranks > 1) return collective().rank;
   int r = 0;
   MPI_Comm_rank(comm, &r);
   return r;
+}
+void isvd_gpu_set_allreduce(isvd_gpu_allreduce_fn fn, void *user, int nranks, int rank, int on_device) {
+  api_call([&] {
+    REQUIRE(nranks >= 1 && rank >= 0 && rank < nranks);
+    Collective &c = collective();
+    if (!fn || nranks == 1) {
+      c = Collective();
+      return;
+    }
+    c.fn = fn;
+    c.user = user;
+    c.nranks = nranks;
+    c.rank = rank;
+    c.on_device = on_device ? 1 : 0;
+  });
 }
 
 static void *aligned64(size_t bytes) {

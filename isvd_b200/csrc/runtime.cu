@@ -152,6 +152,42 @@ GraphPair::~GraphPair() {
   for (int i = 0; i < 2; ++i)
     if (exec[i]) cudaGraphExecDestroy(exec[i]);
 }
+Collective &collective() {
+  static Collective c;
+  return c;
+}
+
+namespace {
+template <class T>
+void allreduce_impl(T *p, size_t count, int dtype, cudaStream_t st) {
+  Collective &c = collective();
+  if (c.nranks <= 1 || !c.fn || count == 0) return;
+  if (c.on_device) {
+    c.fn(p, count, dtype, st, c.user);
+    CK(cudaGetLastError());
+    return;
+  }
+  static void *pin = nullptr;
+  static size_t pin_bytes = 0;
+  const size_t bytes = count * sizeof(T);
+  if (bytes > pin_bytes) {
+    if (pin) cudaFreeHost(pin);
+    pin = nullptr;
+    pin_bytes = 0;
+    if (cudaMallocHost(&pin, bytes) != cudaSuccess) fail(kErrMemory, "pinned staging for the AllReduce");
+    pin_bytes = bytes;
+  }
+  CK(cudaMemcpyAsync(pin, p, bytes, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  c.fn(pin, count, dtype, st, c.user);
+  CK(cudaMemcpyAsync(p, pin, bytes, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));  // the staging buffer is reused by the next call
+}
+}  // namespace
+
+void allreduce_sum(double *p, size_t count, cudaStream_t st) { allreduce_impl(p, count, 1, st); }
+void allreduce_sum(float *p, size_t count, cudaStream_t st) { allreduce_impl(p, count, 0, st); }
+
 void profile_add(const char *tag, double ms, double flops) {
   std::lock_guard<std::mutex> lk(g_prof_mu);
   ProfEntry &e = g_prof[tag];

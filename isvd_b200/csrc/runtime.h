@@ -107,6 +107,18 @@ bool is_device_pointer(const void *p);
 
 void sync();  // synchronise the library stream, converting errors into Error
 
+// Multi-rank execution through a caller-provided sum-AllReduce (isvd_gpu_set_allreduce).
+struct Collective {
+  void (*fn)(void *, size_t, int, void *, void *) = nullptr;
+  void *user = nullptr;
+  int nranks = 1, rank = 0, on_device = 0;
+};
+Collective &collective();
+// In-place sum over the ranks of `count` values at the device pointer p, ordered on st (no-op on
+// one rank).  A host-memory reduction goes through pinned memory after a stream synchronisation.
+void allreduce_sum(double *p, size_t count, cudaStream_t st);
+void allreduce_sum(float *p, size_t count, cudaStream_t st);
+
 // Optional per-kernel timing (CUDA events on the launching stream), off by default.
 bool profiling();
 void set_profiling(bool on);

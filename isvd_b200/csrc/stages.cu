@@ -86,6 +86,7 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
     g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
     gemm(g, c.st);
   }
+  allreduce_sum(W.p, N * ll, c.st);  // row blocks on several ranks: the blocks' Grams are sums
   DBuf<T> Wp(N * ll);
   bool done = false;
   if (c.chol_basis) {
@@ -217,6 +218,10 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, c.st);
   }
+  // Row blocks on several ranks: G is the one exchange of the integration (the reference
+  // exchanges Bc and Bgc in every iteration, @x@_integrate_kolmogorov_nagumo.c:160,178); every
+  // rank then runs the same iterations on the same G.
+  allreduce_sum(G.p, (size_t)Nl * Nl, c.st);
   DBuf<double> Xo;  // deferred second orthogonalization pass, applied in the coordinates of G
   const bool defer = (c.precision == kMixed && c.deferred_orth);
   if (defer) {
@@ -333,6 +338,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
 // Hierarchical reduction (reference @x@_integrate_hierarchical_reduction.c:90-130).
 template <class T>
 void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt) {
+  if (collective().nranks > 1) fail(kErrUnsupported, "hierarchical reduction: one rank only");
   const size_t ll = (size_t)l * l;
   const int hmax = N / 2 > 0 ? N / 2 : 1;
   DBuf<double> Bs(hmax * ll), W(hmax * ll), Vv(hmax * ll), s((size_t)hmax * l);
@@ -391,6 +397,7 @@ void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l);
   project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
+  allreduce_sum(Z.p, (size_t)n * l, c.st);  // row blocks on several ranks: Z = sum of A_j' Qbar_j
   DBuf<double> W(ll), V(ll), w(l);
   {  // W = Z' Z  (reference @x@_postprocess_gramian.c:145)
     Gemm<T, double> g;
@@ -428,6 +435,7 @@ void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera
 template <class T>
 void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                         const T *qt, long long ldqt, T *s, T *ut, long long ldut, bool wu) {
+  if (collective().nranks > 1) fail(kErrUnsupported, "symmetric postprocessing: one rank only");
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l);
   project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);

@@ -21,6 +21,9 @@ struct StageCtx {
   // Gramian orthogonalization may return any orthonormal basis of each span(Y_i) (Cholesky factor
   // instead of the eigenbasis): set by the driver when the rest of the pipeline is basis-invariant
   bool chol_basis = false;
+  // rows of the whole matrix when this process holds a row block of it (multi-rank; 0: the
+  // stage's own rows are all of them)
+  long long m_total = 0;
 };
 
 struct IterResult {

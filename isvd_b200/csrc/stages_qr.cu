@@ -77,10 +77,29 @@ void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long 
       g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
       gemm(g, c.st);
     }
-    const double shift_rel = (pass == 0) ? (std::sqrt((double)rows) + l + 1) * u : 0.0;
+    allreduce_sum(W.p, N * ll, c.st);  // row blocks on several ranks: the Grams are sums
+    const double mrows = c.m_total > 0 ? (double)c.m_total : (double)rows;
+    const double shift_rel = (pass == 0) ? (std::sqrt(mrows) + l + 1) * u : 0.0;
     const double piv_rel = (pass == 0) ? 0.0 : l * u;
     chol_inv_batched(l, N, W.p, 1.0, 0.0, shift_rel, piv_rel, X.p, 1.0, kCholFactor, c.status, c.st);
-    if (pass == 2) hh_sign_batched<T>(l, N, src, lds, l, X.p, c.st);
+    if (pass == 2) {
+      if (collective().nranks > 1) {
+        // the sign rule reads the first l rows of each block, held by rank 0: every rank takes
+        // them from a sum in which the other ranks contribute zeros
+        DBuf<T> top((size_t)l * Nl);
+        if (collective().rank == 0) {
+          if (rows < l) fail(kErrUnsupported, "tall-skinny QR: rank 0 holds fewer than l rows");
+          CK(cudaMemcpy2DAsync(top.p, (size_t)Nl * sizeof(T), src, lds * sizeof(T), (size_t)Nl * sizeof(T), l,
+                               cudaMemcpyDeviceToDevice, c.st));
+        } else {
+          CK(cudaMemsetAsync(top.p, 0, (size_t)l * Nl * sizeof(T), c.st));
+        }
+        allreduce_sum(top.p, (size_t)l * Nl, c.st);
+        hh_sign_batched<T>(l, N, top.p, Nl, l, X.p, c.st);
+      } else {
+        hh_sign_batched<T>(l, N, src, lds, l, X.p, c.st);
+      }
+    }
     copy2d<double, T>(X.p, l, 1, Xt.p, l, 1, (long long)N * l, l, c.st);
     if (mixed) {
       mixed_block_apply<T>(c, yp.P, (int)rows, l, N, src, lds, Xt.p, dst, ldd);
@@ -142,6 +161,9 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
     gemm(g, st);
   }
+  // row blocks on several ranks: G is the integration's one exchange (the reference exchanges Bc,
+  // Bgc and two scalars per iteration, @x@_integrate_wen_yin.c:206-345)
+  allreduce_sum(G.p, (size_t)Nl * Nl, st);
   DBuf<double> Xo;  // deferred second orthogonalization pass, applied in the coordinates of G
   const bool defer = (mixed && c.deferred_orth);
   if (defer) {
@@ -291,6 +313,7 @@ template <class T>
 void post_tsqr_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                    const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
                    bool wv) {
+  if (collective().nranks > 1) fail(kErrUnsupported, "tall-skinny QR postprocessing: one rank only");
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l), Qz((size_t)n * l);
   project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);

@@ -240,6 +240,61 @@ def isvd(a, omega, k, p, N, alg_o="GR", alg_i="KN", alg_p="GR", argv_i=None):
     return dict(s=s, u=u, v=v, qbar=qbar, iters=it, err=err)
 
 
+def row_block(m, P, rank):
+    """Rows [begin, end) of rank `rank` of P, core/param.c:47-55 (ceil(m / P) rows each)."""
+    each = (m - 1) // P + 1
+    return min(rank * each, m), min(rank * each + each, m)
+
+
+def isvd_row_block(a_rows, omega, k, p, N, allreduce, maxit=256, tol=1e-4):
+    """The Gramian / KN / Gramian driver on one rank's rows of a row-distributed A (dista 'R'),
+    with every reduction over the ranks done by ``allreduce(x)`` (an in-place sum of a float64
+    array, the reference's MPI_Allreduce with MPI_SUM):
+      * orthogonalization W_i = sum_ranks Y_i' Y_i, core/stage/@x@_orthogonalize_gramian.c:82-85;
+      * KN B_c = Qs' Q_c and Qs' G_c, core/stage/@x@_integrate_kolmogorov_nagumo.c:157-160, 176-178;
+      * postprocessing Z = A' Qbar (projectBlockRow, core/stage/@x@_postprocess.h:96-162, whose
+        MPI_Reduce_scatter_block leaves each rank its column block of the sum; here every rank keeps
+        the whole sum) and W = Z' Z (core/stage/@x@_postprocess_gramian.c:145-146).
+    Returns (s, U rows of this rank, V (all n rows), iterations, error)."""
+    a_rows = np.asarray(a_rows, np.float64)
+    l = k + p
+    y = a_rows @ np.asarray(omega, np.float64)
+    q = np.empty_like(y)
+    for i in range(N):
+        yi = y[:, i * l:(i + 1) * l]
+        w = allreduce(yi.T @ yi)
+        u, s, _ = np.linalg.svd(w)
+        q[:, i * l:(i + 1) * l] = yi @ (u / np.sqrt(s))
+    qc = q[:, :l].copy()
+    bc = allreduce(q.T @ qc)
+    it = 1
+    while True:
+        gc = q @ bc / N
+        bgc = allreduce(q.T @ gc)
+        dc = bc.T @ bc / N
+        z = _sym_upper(bc.T @ bgc / N - dc @ dc)
+        lam, vec = np.linalg.eigh(z, UPLO="U")
+        sv = np.sqrt(0.5 + np.sqrt(0.25 - lam))
+        ss = np.sqrt(sv)
+        c = (vec * ss) @ (vec * ss).T
+        cinv = (vec / ss) @ (vec / ss).T
+        fc = c - dc @ cinv
+        qp = qc @ fc + gc @ cinv
+        bp = bc @ fc + bgc @ cinv
+        err = float(np.linalg.norm(sv - 1.0))
+        if err <= tol:
+            break
+        if it == maxit:
+            it += 1
+            break
+        qc, bc = qp, bp
+        it += 1
+    z = allreduce(a_rows.T @ qp)
+    w, s, _ = np.linalg.svd(z.T @ z)
+    sig = np.sqrt(s)
+    return sig, qp @ w[:, :k], (z @ w[:, :k]) / sig[:k], it, err
+
+
 # ---------------------------------------------------------------------------------------------
 # Comparison helpers (sign- and rotation-invariant)
 
