@@ -8,9 +8,11 @@
 extern "C" {
 #endif
 
-/* Replaces the global of reference gpu/env.c:19.  0 = no limit.  When A does not fit
- * under the limit next to the sketch, A is streamed through the device in column
- * panels as the reference does (gpu/stage/@x@_sketch_gpu.h:65-77). */
+/* Replaces the global of reference gpu/env.c:19.  0 = no limit.  Device memory is planned
+ * against min(free device memory, this limit): a host A that does not fit beside the solve's
+ * other buffers is streamed through the device in row panels, by the sketch and again by the
+ * postprocessing projection, each copy overlapped with the previous panel's products (the
+ * reference streams column panels sized the same way, gpu/stage/@x@_sketch_gpu.h:65-135). */
 extern size_t isvd_gpu_memory_limit;
 
 /* Replaces isvd_Init_gpu (reference gpu/env.c:27): selects device (rank % device count). */

@@ -15,6 +15,7 @@
 #include "batched.h"
 #include "kernels.h"
 #include "mixed.h"
+#include "panels.h"
 #include "runtime.h"
 #include "stages.h"
 
@@ -162,6 +163,20 @@ struct View {
   }
 };
 
+// Out of core: rows per streamed panel of a host A (ml x n held by this rank), or 0 when A fits on
+// the device beside the solve's other buffers (Y, Qbar, the Nl x Nl and n x l FP64 work) and is
+// copied whole.  MIXED keeps A as bf16 planes instead of the FP32/FP64 copy.
+template <class T>
+long long plan_a_panels(const T *a, long long ml, long long n, long long Nl, long long l, bool mixed) {
+  if (a == nullptr || ml <= 0 || n <= 0 || is_device_pointer(a)) return 0;
+  const size_t s = sizeof(T), pld = (size_t)plane_ld(n);
+  const size_t resident = mixed ? (size_t)plane_rows(ml) * pld * 2 * sketch_planes() : (size_t)ml * n * s;
+  const size_t row_bytes = 2 * (size_t)n * s + (mixed ? pld * 2 * 3 : 0);  // two staging rows + planes
+  const size_t work = (size_t)ml * Nl * s * 3 + (size_t)ml * l * s * 4 + (size_t)Nl * Nl * 8 * 4 +
+                      (size_t)n * l * 8 * 4 + (size_t)n * Nl * s + ((size_t)64 << 20);
+  return host_panel_rows(ml, n, resident, row_bytes, work, s);
+}
+
 struct Ctx {
   StageCtx sc;
   explicit Ctx(int precision) {
@@ -198,12 +213,15 @@ void sketch_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, is
   if (omega) REQUIRE(ldomega >= Nl);
   Ctx c(precision);
   View<T> A, Om, Y;
-  if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
-  else A.bind(a, m, n, lda, true, c.sc.st);
+  c.sc.a_panel_rows = plan_a_panels<T>(a, m, n, Nl, p.dim_sketch, c.sc.precision == kMixed);
+  if (c.sc.a_panel_rows == 0) {  // otherwise a host A is streamed in row panels by the sketch
+    if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
+    else A.bind(a, m, n, lda, true, c.sc.st);
+  }
   if (omega) Om.bind(omega, Nl, n, ldomega, true, c.sc.st);
   Y.bind(yst, Nl, m, ldyst, false, c.sc.st);
-  sketch_dev<T>(c.sc, m, n, Nl, ordera_, A.d, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.d,
-                ldyst);
+  sketch_dev<T>(c.sc, m, n, Nl, ordera_, c.sc.a_panel_rows ? a : A.d, lda, omega ? Om.d : nullptr, ldomega,
+                (uint64_t)(uint32_t)seed, Y.d, ldyst);
   Y.back(c.sc.st);
   sync();
 }
@@ -331,8 +349,12 @@ void post_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd
   if (alg == 1) REQUIRE(n >= l);
   Ctx c(precision);
   View<T> A, Q, S, U, V;
-  if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
-  else A.bind(a, m, n, lda, true, c.sc.st);
+  c.sc.a_panel_rows = plan_a_panels<T>(a, m, n, 0, l, c.sc.precision == kMixed);
+  if (c.sc.a_panel_rows == 0) {  // otherwise a host A is streamed in row panels by the projection
+    if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
+    else A.bind(a, m, n, lda, true, c.sc.st);
+  }
+  const T *a_use = c.sc.a_panel_rows ? a : A.d;
   Q.bind(qt, l, m, ldqt, true, c.sc.st);
   S.bind(s, l, 1, l, false, c.sc.st);
   if (alg == 2) {
@@ -340,7 +362,7 @@ void post_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd
     T *u = (ut_root >= -1) ? ut : vt;
     const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
     U.bind(u, k, m, ld, false, c.sc.st);
-    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ld, wu);
+    post_symmetric_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.d, ldqt, S.d, U.d, ld, wu);
     S.back(c.sc.st);
     if (wu) U.back(c.sc.st, k);
     if (ut_root >= -1 && vt_root >= -1) {
@@ -360,9 +382,9 @@ void post_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, isvd
   if (wu) U.bind(ut, k, m, ldut, false, c.sc.st);
   if (wv) V.bind(vt, vcols, n, ldvt, false, c.sc.st);
   if (alg == 0)
-    post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+    post_gramian_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
   else
-    post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, A.d, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
+    post_tsqr_dev<T>(c.sc, m, n, k, l, ordera_, a_use, lda, Q.d, ldqt, S.d, U.d, ldut, V.d, ldvt, wu, wv);
   S.back(c.sc.st);
   if (wu) U.back(c.sc.st, k);
   if (wv) V.back(c.sc.st, vcols);
@@ -491,12 +513,15 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   // MIXED precision streams a host A through the device in panels inside the sketch and keeps
   // only its bf16 planes (reused by the postprocess); NATIVE precision copies A once.
   const bool mixed = c.sc.precision == kMixed;
+  // out of core: a host A that does not fit beside the solve's buffers is streamed in row panels
+  // by the sketch and again by the projection
+  c.sc.a_panel_rows = plan_a_panels<T>(a, ml, n, Nl, l, mixed);
   View<T> A, Om;
-  if (!mixed) {
+  if (!mixed && c.sc.a_panel_rows == 0) {
     if (ordera_ == 'R') A.bind(a, n, ml, lda, true, st);
     else A.bind(a, ml, n, lda, true, st);
   }
-  const T *a_use = mixed ? a : A.d;
+  const T *a_use = (mixed || c.sc.a_panel_rows > 0) ? a : A.d;
   if (omega) Om.bind(omega, Nl, n, ldomega, true, st);
   DBuf<T> Y((size_t)ml * Nl), Q((size_t)ml * l);
   sketch_dev<T>(c.sc, ml, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,

@@ -17,6 +17,7 @@
 
 #include "kernels.h"
 #include "mixed.h"
+#include "panels.h"
 #include "runtime.h"
 
 namespace isvdb {
@@ -68,7 +69,7 @@ static long long panel_rows(long long m, long long n, size_t elem) {
 
 // bf16 planes of A used by the sketch (2, or 3 with ISVD_GPU_SKETCH_PLANES=3); the postprocess
 // reads the first two.
-static int sketch_planes() {
+int sketch_planes() {
   static const int np = [] {
     const char *e = getenv("ISVD_GPU_SKETCH_PLANES");
     return (e && atoi(e) == 3) ? 3 : 2;
@@ -81,20 +82,30 @@ static int sketch_planes() {
 // memory, panel p + 1 is copied to the device on the copy stream while panel p is split and
 // multiplied, so that the PCIe transfer overlaps the tensor-core work (the reference streams A in
 // column panels through the GPU for the same reason, gpu/stage/@x@_sketch_gpu.h:238-254).  The
-// FP32 A is never resident on the device in this mode.
+// FP32 A is never resident on the device in this mode.  Out of core (c.a_panel_rows > 0, host A):
+// only one panel's planes exist at a time and none are kept; the projection streams A again.
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                   long long ldom, uint64_t seed, T *y, long long ldy) {
-  Runtime &rt = Runtime::get();
   const bool a_dev = is_device_pointer(a);
-  const long long ld = plane_ld(n), rp = plane_rows(m), ps = rp * ld;
+  const bool ooc = !a_dev && c.a_panel_rows > 0;
+  const long long P = ooc ? c.a_panel_rows : panel_rows(m, n, sizeof(T));
+  const long long held = ooc ? P : m;  // rows of planes held at once
+  const long long ld = plane_ld(n), rp = plane_rows(held), ps = rp * ld;
   MixedCache local;
-  MixedCache *mc = c.cache ? c.cache : &local;
+  MixedCache *mc = (c.cache && !ooc) ? c.cache : &local;
+  if (ooc && c.cache) {
+    c.cache->buf.release();
+    c.cache->src = nullptr;
+  }
   const int na = sketch_planes();
   mc->buf.alloc((size_t)na * ps);
-  for (int q = 0; q < na; ++q)  // zero rows [m, rp): TMA boxes of the last tile read them
-    if (rp > m)
-      CK(cudaMemsetAsync(mc->buf.p + (size_t)q * ps + (size_t)m * ld, 0, (size_t)(rp - m) * ld * 2, c.st));
+  auto zero_rows_from = [&](long long r) {  // TMA boxes of the last tile read rows [r, rp)
+    for (int q = 0; q < na; ++q)
+      if (rp > r)
+        CK(cudaMemsetAsync(mc->buf.p + (size_t)q * ps + (size_t)r * ld, 0, (size_t)(rp - r) * ld * 2, c.st));
+  };
+  zero_rows_from(held);
   Planes all;
   all.ptr = mc->buf.p; all.np = na; all.rows = m; all.cols = n; all.ld = ld; all.plane_stride = ps;
   PlaneBuf om;
@@ -105,19 +116,6 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     om.P.ptr = om.buf.p; om.P.np = 1; om.P.rows = Nl; om.P.cols = n; om.P.ld = old; om.P.plane_stride = orp * old;
   } else {
     make_planes<T>(om, omega, ldom, n, Nl, 3, true, c.st);  // Omega' planes (Nl x n)
-  }
-  const long long P = panel_rows(m, n, sizeof(T));
-  DBuf<T> stage[2];
-  cudaEvent_t copied[2] = {nullptr, nullptr}, consumed[2] = {nullptr, nullptr}, ready = nullptr;
-  if (!a_dev) {
-    for (int b = 0; b < 2; ++b) {
-      stage[b].alloc((size_t)P * n);
-      CK(cudaEventCreateWithFlags(&copied[b], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&consumed[b], cudaEventDisableTiming));
-    }
-    CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
-    CK(cudaEventRecord(ready, c.st));  // staging buffers allocated on the compute stream
-    CK(cudaStreamWaitEvent(rt.copy_stream, ready, 0));
   }
   UmmaGemm g;
   g.N = Nl; g.K = n;
@@ -139,44 +137,26 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     g.A = all;
     g.C = y;
     umma_gemm(g, c.st);
-  }
-  int p = 0;
-  for (long long r0 = 0; r0 < m && !a_dev; r0 += P, ++p) {
+  } else {
     // A in host memory: panel p + 1 is copied while panel p is split and multiplied
-    const long long rows = std::min<long long>(P, m - r0);
-    __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
-    const int b = p & 1;
-    if (p >= 2) CK(cudaStreamWaitEvent(rt.copy_stream, consumed[b], 0));
-    if (ordera == 'R') {
-      CK(cudaMemcpy2DAsync(stage[b].p, n * sizeof(T), a + r0 * lda, lda * sizeof(T), n * sizeof(T), rows,
-                           cudaMemcpyHostToDevice, rt.copy_stream));
-    } else {
-      CK(cudaMemcpy2DAsync(stage[b].p, rows * sizeof(T), a + r0, lda * sizeof(T), rows * sizeof(T), n,
-                           cudaMemcpyHostToDevice, rt.copy_stream));
-    }
-    CK(cudaEventRecord(copied[b], rt.copy_stream));
-    CK(cudaStreamWaitEvent(c.st, copied[b], 0));
-    if (ordera == 'R') split_rows<T>(stage[b].p, n, 1, rows, n, na, false, dst, ld, ps, c.st);
-    else split_rows<T>(stage[b].p, rows, 1, n, rows, na, true, dst, ld, ps, c.st);
-    CK(cudaEventRecord(consumed[b], c.st));
-    Planes ap = all;
-    ap.ptr = dst;
-    ap.rows = rows;
-    g.M = (int)rows;
-    g.A = ap;
-    g.C = y + r0 * ldy;
-    umma_gemm(g, c.st);
+    for_each_host_panel<T>(c, a, lda, ordera, m, n, P, [&](long long r0, long long rows, const T *ap, long long ldp) {
+      __nv_bfloat16 *dst = ooc ? mc->buf.p : mc->buf.p + (size_t)r0 * ld;
+      if (ooc && rows < P) zero_rows_from(rows);  // the last panel: rows of the previous one
+      if (ordera == 'R') split_rows<T>(ap, ldp, 1, rows, n, na, false, dst, ld, ps, c.st);
+      else split_rows<T>(ap, ldp, 1, n, rows, na, true, dst, ld, ps, c.st);
+      Planes pp = all;
+      pp.ptr = dst;
+      pp.rows = rows;
+      g.M = (int)rows;
+      g.A = pp;
+      g.C = y + r0 * ldy;
+      umma_gemm(g, c.st);
+    });
   }
-  if (!a_dev) {
-    CK(cudaStreamSynchronize(c.st));
-    for (int b = 0; b < 2; ++b) {
-      cudaEventDestroy(copied[b]);
-      cudaEventDestroy(consumed[b]);
-    }
-    cudaEventDestroy(ready);
+  if (!ooc) {
+    mc->src = a; mc->m = m; mc->n = n; mc->ordera = ordera;
+    mc->A = all;
   }
-  mc->src = a; mc->m = m; mc->n = n; mc->ordera = ordera;
-  mc->A = all;
 }
 
 template <class T>
@@ -271,6 +251,40 @@ void mixed_apply_coeff(const StageCtx &c, const Planes &qp, int m, int Nl, int l
   umma_gemm(g, c.st);
 }
 
+// Out-of-core projection: Z = sum over row panels of A_p' Qbar_p, each panel of the host A split
+// into two bf16 planes on arrival and multiplied on the tensor cores, the panel sums added in FP64.
+template <class T>
+void mixed_project_streamed(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda,
+                            const T *qt, long long ldqt, T *z) {
+  const long long P = c.a_panel_rows, ld = plane_ld(n), rp = plane_rows(P), ps = rp * ld;
+  DBuf<__nv_bfloat16> pl((size_t)2 * ps);
+  auto zero_rows_from = [&](long long r) {
+    for (int q = 0; q < 2; ++q)
+      if (rp > r) CK(cudaMemsetAsync(pl.p + (size_t)q * ps + (size_t)r * ld, 0, (size_t)(rp - r) * ld * 2, c.st));
+  };
+  zero_rows_from(P);
+  DBuf<double> zacc((size_t)n * l), zp((size_t)n * l);
+  for_each_host_panel<T>(c, a, lda, ordera, m, n, P, [&](long long r0, long long rows, const T *ap, long long ldp) {
+    if (rows < P) zero_rows_from(rows);
+    if (ordera == 'R') split_rows<T>(ap, ldp, 1, rows, n, 2, false, pl.p, ld, ps, c.st);
+    else split_rows<T>(ap, ldp, 1, n, rows, 2, true, pl.p, ld, ps, c.st);
+    PlaneBuf qp;
+    make_planes<T>(qp, qt + r0 * ldqt, ldqt, rows, l, 2, true, c.st);  // Qbar_p' planes (l x rows)
+    Planes b;  // the panel's planes, rows x n (n contiguous): as the N x K = n x rows operand, MN-major
+    b.ptr = pl.p; b.np = 2; b.rows = rows; b.cols = n; b.ld = ld; b.plane_stride = ps; b.mn_major = true;
+    UmmaGemm g;
+    g.M = l; g.N = n; g.K = (int)rows;
+    g.A = qp.P; g.B = b;
+    set_products(g, 2, 2);
+    g.C = r0 == 0 ? zacc.p : zp.p; g.c_double = true; g.c_rs = 1; g.c_cs = l;
+    g.status = c.status;
+    g.tag = "project";
+    umma_gemm(g, c.st);
+    if (r0 > 0) lincomb(zacc.p, zacc.p, 1.0, zp.p, 1.0, 0.0, n, l, c.st);
+  });
+  copy2d<double, T>(zacc.p, l, 1, z, l, 1, n, l, c.st);
+}
+
 template <class T>
 void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
                    long long ldqt, T *z) {
@@ -281,6 +295,9 @@ void mixed_project(const StageCtx &c, int m, int n, int l, char ordera, const T 
   MixedCache *mc = c.cache;
   if (mc && mc->src == a && mc->m == m && mc->n == n && mc->ordera == ordera && mc->buf.p) {
     ap = mc->A;
+  } else if (!is_device_pointer(a) && c.a_panel_rows > 0) {
+    mixed_project_streamed<T>(c, m, n, l, ordera, a, lda, qt, ldqt, z);
+    return;
   } else {
     if (!is_device_pointer(a)) fail(kErrArgument, "mixed postprocess: A is not on the device and not cached");
     if (ordera == 'R') make_planes<T>(local, a, lda, m, n, 2, false, c.st);

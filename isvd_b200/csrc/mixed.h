@@ -44,6 +44,9 @@ struct MixedCache {
 // Y = A * Omega (m x Nl, row-major ldy).  omega == nullptr: Omega is drawn exactly in bf16
 // (Philox + Box-Muller, rounded), so only A is split (2 products, one per A plane).  Otherwise
 // Omega is split too.
+// bf16 planes of A the MIXED sketch keeps per element (2; 3 with ISVD_GPU_SKETCH_PLANES=3).
+int sketch_planes();
+
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                   long long ldom, uint64_t seed, T *y, long long ldy);

@@ -1,6 +1,7 @@
 // Device context, errors and stream-ordered allocation for libisvd_gpu_b200.
 #include "runtime.h"
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -9,6 +10,8 @@
 #include <mutex>
 #include <string>
 #include <vector>
+
+extern "C" size_t isvd_gpu_memory_limit;  // include/isvd/gpu/env.h
 
 namespace isvdb {
 
@@ -95,6 +98,37 @@ void *dev_alloc(size_t bytes) {
     fail(kErrMemory, "device allocation of %zu bytes failed (%s)", bytes, cudaGetErrorString(e));
   }
   return p;
+}
+
+size_t device_budget() {
+  Runtime &rt = Runtime::get();
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  // memory the library's pool holds but does not use counts as free (it is reused first)
+  cudaMemPool_t pool;
+  CK(cudaDeviceGetDefaultMemPool(&pool, rt.device));
+  unsigned long long reserved = 0, used = 0;
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+  CK(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+  if (reserved > used) free_b += (size_t)(reserved - used);
+  const size_t lim = isvd_gpu_memory_limit;
+  return lim > 0 ? std::min(free_b, lim) : free_b;
+}
+
+long long host_panel_rows(long long m, long long n, size_t resident_bytes, size_t row_bytes, size_t work_bytes,
+                          size_t elem) {
+  const size_t budget = device_budget();
+  if (resident_bytes + work_bytes <= budget) return 0;
+  const size_t avail = budget > work_bytes ? budget - work_bytes : 0;
+  long long P = (long long)(avail / std::max<size_t>(row_bytes, 1));
+  const long long cap = std::max<long long>(128, (long long)((1ll << 30) / ((long long)n * (long long)elem)));
+  P = std::min(P, cap);
+  if (P >= m) return m;
+  P = P / 128 * 128;
+  if (P < 128)
+    fail(kErrMemory, "not enough GPU memory for a host A streamed in panels of 128 rows (%zu bytes usable, "
+                     "%zu needed)", budget, work_bytes + 128 * row_bytes);
+  return P;
 }
 
 void dev_free(void *p) {

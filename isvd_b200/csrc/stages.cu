@@ -7,6 +7,7 @@
 
 #include "kernels.h"
 #include "mixed.h"
+#include "panels.h"
 #include "runtime.h"
 #include "stages.h"
 
@@ -55,11 +56,17 @@ void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a
     omega = om.p;
     ldom = Nl;
   }
-  Gemm<T, T> g = gm<T>(m, Nl, n);
-  g.A = a; set_a(g, ordera, lda, false);
-  g.B = omega; g.b_rs = ldom; g.b_cs = 1;
-  g.C = y; g.c_rs = ldy; g.c_cs = 1;
-  gemm(g, c.st);
+  auto rows_times_omega = [&](long long r0, long long rows, const T *ap, long long ld) {
+    Gemm<T, T> g = gm<T>((int)rows, Nl, n);
+    g.A = ap; set_a(g, ordera, ld, false);
+    g.B = omega; g.b_rs = ldom; g.b_cs = 1;
+    g.C = y + r0 * ldy; g.c_rs = ldy; g.c_cs = 1;
+    gemm(g, c.st);
+  };
+  if (c.a_panel_rows > 0 && !is_device_pointer(a))  // out-of-core A: Y's rows panel by panel
+    for_each_host_panel<T>(c, a, lda, ordera, m, n, c.a_panel_rows, rows_times_omega);
+  else
+    rows_times_omega(0, m, a, lda);
 }
 
 // -------------------------------------------------------------------------- orthogonalize
@@ -383,11 +390,18 @@ void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, lo
     mixed_project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, z);
     return;
   }
-  Gemm<T, T> g = gm<T>(n, l, m);
-  g.A = a; set_a(g, ordera, lda, true);
-  g.B = qt; g.b_rs = ldqt; g.b_cs = 1;
-  g.C = z; g.c_rs = l; g.c_cs = 1;
-  gemm(g, c.st);
+  auto add_rows = [&](long long r0, long long rows, const T *ap, long long ld) {  // Z += A_p' Qbar_p
+    Gemm<T, T> g = gm<T>(n, l, (int)rows);
+    g.A = ap; set_a(g, ordera, ld, true);
+    g.B = qt + r0 * ldqt; g.b_rs = ldqt; g.b_cs = 1;
+    g.C = z; g.c_rs = l; g.c_cs = 1;
+    g.beta = r0 > 0 ? 1.0 : 0.0;
+    gemm(g, c.st);
+  };
+  if (c.a_panel_rows > 0 && !is_device_pointer(a))  // out-of-core A
+    for_each_host_panel<T>(c, a, lda, ordera, m, n, c.a_panel_rows, add_rows);
+  else
+    add_rows(0, m, a, lda);
 }
 
 template <class T>

@@ -24,6 +24,9 @@ struct StageCtx {
   // rows of the whole matrix when this process holds a row block of it (multi-rank; 0: the
   // stage's own rows are all of them)
   long long m_total = 0;
+  // out-of-core A: a host A is streamed through the device in row panels of this many rows by the
+  // sketch and the projection (0: A is on the device, or copied there whole)
+  long long a_panel_rows = 0;
 };
 
 struct IterResult {
