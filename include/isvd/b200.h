@@ -168,6 +168,26 @@ int isvd_dSvdAdjoint(
     const int cg_iters, const double tol, int *iterations
 );
 
+/* ---------------------------------------------------------------- Matrix Market files
+ * The file format of the reference's data files (*.mtx) and demo/cdemo.c:51-73 (read there through the
+ * NIST mmio library and one isvd_dFget per value).  isvd_?MtxRead stores the size of the matrix in
+ * `path` in *m, *n and, when a != NULL, its values in a (ordera 'C': a[i + j*lda], lda >= m;
+ * 'R': a[i*lda + j], lda >= n).  Formats "array" (dense, column-major values) and "coordinate"
+ * (1-based triplets; omitted entries are zero), fields real / integer / pattern, symmetries
+ * general / symmetric / skew-symmetric (mirrored).  The values of a dense file are parsed on all
+ * host threads.  isvd_?MtxWrite writes a as "matrix array real general", each value in the
+ * shortest decimal form that reads back to it exactly.  Both return an ISVD_GPU_* status
+ * (ISVD_GPU_ERROR_ARGUMENT with the reason for a file that cannot be read, written or parsed).
+ * No device work. */
+int isvd_sMtxRead( const char *path, isvd_int_t *m, isvd_int_t *n, isvd_s_val_t *a, const isvd_int_t lda,
+                   const char ordera );
+int isvd_dMtxRead( const char *path, isvd_int_t *m, isvd_int_t *n, isvd_d_val_t *a, const isvd_int_t lda,
+                   const char ordera );
+int isvd_sMtxWrite( const char *path, const isvd_int_t m, const isvd_int_t n, const isvd_s_val_t *a,
+                    const isvd_int_t lda, const char ordera );
+int isvd_dMtxWrite( const char *path, const isvd_int_t m, const isvd_int_t n, const isvd_d_val_t *a,
+                    const isvd_int_t lda, const char ordera );
+
 /* ---------------------------------------------------------------- several ranks without MPI
  * Row-block execution over P processes (one GPU each) whose only exchange is a sum-AllReduce
  * that the caller supplies (NCCL, MPI, gloo ...).  It stands in for the reference's own MPI

@@ -162,6 +162,10 @@ class IsvdLib:
                        [self.Param, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                         _VP, _VP, _VP, _VP, _VP, _VP, _CH, _CH, _VP, self.c_int_t, _VP, _VP, self.c_int_t, _VP, self.c_int_t,
                         self.c_int_t, c_mpi_int, c_mpi_int, _VP, self.c_int_t, ctypes.c_int], ctypes.c_int)
+            it = self.c_int_t
+            self._decl("isvd_%sMtxRead" % x, [ctypes.c_char_p, ctypes.POINTER(it), ctypes.POINTER(it), _VP, it, _CH],
+                       ctypes.c_int)
+            self._decl("isvd_%sMtxWrite" % x, [ctypes.c_char_p, it, it, _VP, it, _CH], ctypes.c_int)
 
     def _decl(self, name, argtypes, restype=None):
         fn = getattr(self.lib, name, None)
@@ -221,6 +225,31 @@ class IsvdLib:
         fn = getattr(self.lib, "isvd_%s%s%s" % (x, name, "_gpu" if gpu else ""))
         fn(param, None, 0, None, 0, dista, ordera, ptr(a), lda, ptr(qt), ldqt, ptr(s), ptr(ut), ldut, ptr(vt),
            ldvt, ut_root, vt_root)
+
+    # ------------------------------------------------------------------ Matrix Market files
+    def mtx_read(self, path, x="d", ordera=b"C", pad=0):
+        """isvd_?MtxRead: (status, m x n array or None).  ordera / pad choose the layout and the
+        leading dimension the library writes (m + pad for 'C', n + pad for 'R')."""
+        f = getattr(self.lib, "isvd_%sMtxRead" % x)
+        m, n = self.c_int_t(0), self.c_int_t(0)
+        p = os.fsencode(str(path))
+        st = f(p, ctypes.byref(m), ctypes.byref(n), None, 1, ordera)
+        if st:
+            return st, None
+        dt = _dt(x)
+        if ordera == b"C":
+            buf = np.zeros((n.value, m.value + pad), dt)  # column j at buf[j, :m]
+            st = f(p, ctypes.byref(m), ctypes.byref(n), buf.ctypes.data, m.value + pad, ordera)
+            return st, None if st else buf[:, :m.value].T.copy()
+        buf = np.zeros((m.value, n.value + pad), dt)
+        st = f(p, ctypes.byref(m), ctypes.byref(n), buf.ctypes.data, n.value + pad, ordera)
+        return st, None if st else buf[:, :n.value].copy()
+
+    def mtx_write(self, path, a, x="d"):
+        """isvd_?MtxWrite of a 2-D array ("matrix array real general"); returns the status."""
+        a = np.ascontiguousarray(a, _dt(x))
+        return getattr(self.lib, "isvd_%sMtxWrite" % x)(os.fsencode(str(path)), a.shape[0], a.shape[1],
+                                                        a.ctypes.data, a.shape[1], b"R")
 
     # ------------------------------------------------------------------ extensions
     def last_error(self):

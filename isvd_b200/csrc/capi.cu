@@ -15,6 +15,7 @@
 #include "batched.h"
 #include "kernels.h"
 #include "mixed.h"
+#include "mtx.h"
 #include "panels.h"
 #include "runtime.h"
 #include "stages.h"
@@ -821,6 +822,39 @@ void isvd_sMemcpy(isvd_s_val_t *d, const isvd_s_val_t *s, const size_t num) { me
 void isvd_dMemcpy(isvd_d_val_t *d, const isvd_d_val_t *s, const size_t num) { memcpy(d, s, num * sizeof(*d)); }
 
 // ---------------------------------------------------------------- environment
+// ---------------------------------------------------------------- text I/O, OpenMP queries
+void isvd_iFget(FILE *stream, isvd_int_t *varp) {
+  long long v = 0;
+  if (stream && varp && fscanf(stream, "%lld", &v) == 1) { *varp = (isvd_int_t)v; return; }
+  record_error(kErrArgument, "isvd_iFget: no integer could be read");
+}
+void isvd_sFget(FILE *stream, isvd_s_val_t *varp) {
+  if (!(stream && varp && fscanf(stream, "%f", varp) == 1)) record_error(kErrArgument, "isvd_sFget: no value could be read");
+}
+void isvd_dFget(FILE *stream, isvd_d_val_t *varp) {
+  if (!(stream && varp && fscanf(stream, "%lf", varp) == 1)) record_error(kErrArgument, "isvd_dFget: no value could be read");
+}
+omp_int_t isvd_getOmpMaxSize(void) { return 1; }
+omp_int_t isvd_getOmpSize(void) { return 1; }
+omp_int_t isvd_getOmpRank(void) { return 0; }
+
+#define ISVD_MTX(x, T)                                                                                          \
+  int isvd_##x##MtxRead(const char *path, isvd_int_t *m, isvd_int_t *n, T *a, const isvd_int_t lda,             \
+                        const char ordera) {                                                                    \
+    return api_call([&] {                                                                                       \
+      const MtxInfo h = mtx_read<T>(path, a, lda, ordera);                                                      \
+      if (m) *m = (isvd_int_t)h.m;                                                                              \
+      if (n) *n = (isvd_int_t)h.n;                                                                              \
+    });                                                                                                         \
+  }                                                                                                             \
+  int isvd_##x##MtxWrite(const char *path, const isvd_int_t m, const isvd_int_t n, const T *a,                  \
+                         const isvd_int_t lda, const char ordera) {                                             \
+    return api_call([&] { mtx_write<T>(path, m, n, a, lda, ordera); });                                         \
+  }
+ISVD_MTX(s, float)
+ISVD_MTX(d, double)
+#undef ISVD_MTX
+
 void isvd_Init_cpu(int *argcp, char ***argvp, const isvd_MpiComm mpi_comm) {
   (void)mpi_comm;
   MPI_Init(argcp, argvp);
