@@ -1,0 +1,206 @@
+// FP64 matrix product on the FP64 tensor-core path (mma.sync m8n8k4 .f64: the only tensor-core
+// instruction with FP64 operands on sm_100a; tcgen05 has no FP64 kind).  Same contract as the
+// CUDA-core gemm<double, double> (arbitrary strides with one unit stride per operand, batch,
+// split-K, alpha / beta); every product term is an IEEE FP64 fused multiply-add, so results
+// differ from the CUDA-core kernel only in the order of the K summation.
+//
+// Tiling: BM x BN output tile per CTA of WM x WN warps, each warp a (BM / WM) x (BN / WN) block
+// of 8 x 8 mma tiles held in registers.  BK = 16 deep K slices are copied global -> shared by
+// cp.async (8-byte elements, zero-filled outside the matrix) in a 3-stage ring.  Each operand is
+// staged in the orientation of its unit stride (K-contiguous rows of BK + 4, or MN-contiguous
+// rows of BM + 4 / BN + 4 doubles), which makes both the copies and the fragment reads free of
+// shared-memory bank conflicts.
+#include <algorithm>
+#include <cstdlib>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace isvdb {
+namespace {
+
+constexpr int kBK = 16, kStages = 3, kPad = 4;
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// D = A B + D for one 8 x 8 x 4 tile: a = A(lane / 4, lane % 4), b = B(lane % 4, lane / 4),
+// d = D(lane / 4, 2 (lane % 4) + {0, 1}).
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+template <int BM, int BN, bool A_KC, bool B_NC>
+struct DmmaLayout {
+  static constexpr int a_elems = A_KC ? BM * (kBK + kPad) : kBK * (BM + kPad);
+  static constexpr int b_elems = B_NC ? kBK * (BN + kPad) : BN * (kBK + kPad);
+  static constexpr int stage = a_elems + b_elems;
+  __device__ static int a_at(int m, int k) { return A_KC ? m * (kBK + kPad) + k : k * (BM + kPad) + m; }
+  __device__ static int b_at(int k, int n) { return B_NC ? k * (BN + kPad) + n : n * (kBK + kPad) + k; }
+};
+
+template <int BM, int BN, int WM, int WN, bool A_KC, bool B_NC>
+__global__ void __launch_bounds__(WM * WN * 32)
+    dmma_gemm_kernel(const Gemm<double, double> g, const int splits, const int kchunk, double *__restrict__ partial) {
+  using L = DmmaLayout<BM, BN, A_KC, B_NC>;
+  constexpr int NT = WM * WN * 32;
+  constexpr int TM = BM / WM / 8, TN = BN / WN / 8;  // 8 x 8 tiles per warp
+  constexpr int LA = BM * kBK / NT, LB = BN * kBK / NT;
+  static_assert(LA * NT == BM * kBK && LB * NT == BN * kBK, "tile / thread mismatch");
+  extern __shared__ double smem[];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp / WN) * (BM / WM), wn0 = (warp % WN) * (BN / WN);
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
+  const int kb = sp * kchunk, ke = min(g.K, kb + kchunk);
+  const double *__restrict__ A = g.A + (long long)b * g.a_bs;
+  const double *__restrict__ B = g.B + (long long)b * g.b_bs;
+  const int nk = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
+
+  auto issue = [&](int kt) {  // k slice kt into stage kt % kStages
+    double *As = smem + (kt % kStages) * L::stage, *Bs = As + L::a_elems;
+    const int k0 = kb + kt * kBK;
+#pragma unroll
+    for (int r = 0; r < LA; ++r) {
+      const int e = tid + r * NT;
+      const int mm = A_KC ? e / kBK : e % BM, kk = A_KC ? e % kBK : e / BM;
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < g.M && gk < ke;
+      cp_async8(As + L::a_at(mm, kk), ok ? A + (long long)gm * g.a_rs + (long long)gk * g.a_cs : A, ok);
+    }
+#pragma unroll
+    for (int r = 0; r < LB; ++r) {
+      const int e = tid + r * NT;
+      const int nn = B_NC ? e % BN : e / kBK, kk = B_NC ? e / BN : e % kBK;
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < g.N && gk < ke;
+      cp_async8(Bs + L::b_at(kk, nn), ok ? B + (long long)gk * g.b_rs + (long long)gn * g.b_cs : B, ok);
+    }
+  };
+
+  double acc[TM][TN][2];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < kStages - 1; ++s) {
+    if (s < nk) issue(s);
+    cp_async_commit();
+  }
+  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column within an 8 x 4 (4 x 8) tile
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<kStages - 2>();
+    __syncthreads();  // slice kt visible to all; slice kt - 1 no longer read (its stage is refilled)
+    if (kt + kStages - 1 < nk) issue(kt + kStages - 1);
+    cp_async_commit();
+    const double *As = smem + (kt % kStages) * L::stage, *Bs = As + L::a_elems;
+#pragma unroll
+    for (int k4 = 0; k4 < kBK; k4 += 4) {
+      double av[TM], bv[TN];
+#pragma unroll
+      for (int i = 0; i < TM; ++i) av[i] = As[L::a_at(wm0 + 8 * i + fr, k4 + fc)];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) bv[j] = Bs[L::b_at(k4 + fc, wn0 + 8 * j + fr)];
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) dmma884(acc[i][j], av[i], bv[j]);
+    }
+  }
+  cp_async_wait<0>();
+
+  const bool direct = splits == 1;
+  double *__restrict__ C = direct ? g.C + (long long)b * g.c_bs : partial + ((long long)blockIdx.z * g.M) * g.N;
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+    const int gm = m0 + wm0 + 8 * i + fr;
+    if (gm >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int gn = n0 + wn0 + 8 * j + 2 * fc + h;
+        if (gn >= g.N) continue;
+        if (direct) {
+          double *c = C + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+          double v = g.alpha * acc[i][j][h];
+          if (g.beta != 0.0) v += g.beta * *c;
+          *c = v;
+        } else {
+          C[(long long)gm * g.N + gn] = acc[i][j][h];
+        }
+      }
+  }
+}
+
+template <int BM, int BN, int WM, int WN>
+void dmma_launch(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t st) {
+  Runtime &rt = Runtime::get();
+  const int gx = (g.M + BM - 1) / BM, gy = (g.N + BN - 1) / BN;
+  const long long tiles = (long long)gx * gy * g.batch;
+  int splits = g.splits;
+  if (splits <= 0) {
+    const long long target = 2LL * rt.num_sms;
+    splits = 1;
+    if (tiles < target) {
+      const long long s = (target + tiles - 1) / tiles;
+      const long long smax = std::max<long long>(1, g.K / (8 * kBK));
+      splits = (int)std::min<long long>(s, smax);
+    }
+  }
+  int kchunk = (g.K + splits - 1) / splits;
+  kchunk = ((kchunk + kBK - 1) / kBK) * kBK;
+  if (kchunk <= 0) kchunk = kBK;
+  splits = std::max(1, (g.K + kchunk - 1) / kchunk);
+  DBuf<double> part;
+  if (splits > 1) part.alloc((size_t)g.batch * splits * g.M * g.N);
+  const dim3 grid(gx, gy, g.batch * splits);
+  constexpr int NT = WM * WN * 32;
+#define ISVD_DMMA_CASE(AK, BNC)                                                                        \
+  if (a_kc == AK && b_nc == BNC) {                                                                     \
+    auto *k = dmma_gemm_kernel<BM, BN, WM, WN, AK, BNC>;                                               \
+    const int bytes = kStages * DmmaLayout<BM, BN, AK, BNC>::stage * (int)sizeof(double);              \
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));                   \
+    k<<<grid, NT, bytes, st>>>(g, splits, kchunk, part.p);                                             \
+    KLAUNCHED();                                                                                       \
+  }
+  ISVD_DMMA_CASE(true, true)
+  ISVD_DMMA_CASE(true, false)
+  ISVD_DMMA_CASE(false, true)
+  ISVD_DMMA_CASE(false, false)
+#undef ISVD_DMMA_CASE
+  if (splits > 1) splitk_reduce(g, splits, part.p, st);
+}
+
+}  // namespace
+
+bool dmma_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("ISVD_GPU_DMMA");
+    return !(e && atoi(e) == 0);
+  }();
+  return on;
+}
+
+void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t st) {
+  // 128 x 128 tiles when they fill the GPU or a long K lets split-K fill it; otherwise 64 x 64
+  const long long tiles128 = (long long)((g.M + 127) / 128) * ((g.N + 127) / 128) * g.batch;
+  const int sms = Runtime::get().num_sms;
+  const bool long_k = g.splits <= 0 && (long long)g.K >= 2048 && tiles128 * (g.K / 1024) >= 2LL * sms;
+  if (g.M <= 64 || g.N <= 64 || (tiles128 < 2LL * sms && !long_k))
+    dmma_launch<64, 64, 2, 2>(g, a_kc, b_nc, st);
+  else
+    dmma_launch<128, 128, 2, 4>(g, a_kc, b_nc, st);
+}
+
+}  // namespace isvdb

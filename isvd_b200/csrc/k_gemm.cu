@@ -6,6 +6,7 @@
 // block at rows ty + 16 i, cols tx + 16 j (conflict-free shared reads, coalesced stores).
 // Tall-skinny products (K >> M N) are split along K; partials are summed in FP64.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.h"
 #include "runtime.h"
@@ -237,6 +238,13 @@ void launch_fixed(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, int sms, T *part
 
 }  // namespace
 
+void splitk_reduce(const Gemm<double, double> &g, int splits, const double *partial, cudaStream_t st) {
+  const long long total = (long long)g.M * g.N * g.batch;
+  const int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * Runtime::get().num_sms);
+  splitk_reduce_kernel<double, double><<<blocks, 256, 0, st>>>(g, splits, partial);
+  KLAUNCHED();
+}
+
 template <class T, class Tout>
 void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return;
@@ -248,6 +256,12 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
   const bool b_nc = (g.b_cs == 1);
   if (!a_kc && g.a_rs != 1) fail(kErrArgument, "gemm: operand A has no unit stride");
   if (!b_nc && g.b_rs != 1) fail(kErrArgument, "gemm: operand B has no unit stride");
+  if constexpr (std::is_same<T, double>::value && std::is_same<Tout, double>::value) {
+    if (dmma_enabled()) {  // FP64 operands: the FP64 tensor-core path (k_dmma.cu)
+      dmma_gemm(g, a_kc, b_nc, st);
+      return;
+    }
+  }
   // 128 x 128 tiles when they fill the GPU, or when a long inner dimension lets split-K fill it
   // (8 x 8 register blocks: half the shared-memory reads per FMA of 64 x 64 tiles); otherwise
   // 64 x 64 tiles (4x more CTAs)

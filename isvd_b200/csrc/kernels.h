@@ -30,6 +30,14 @@ struct Gemm {
 template <class T, class Tout>
 void gemm(const Gemm<T, Tout> &g, cudaStream_t st);
 
+// FP64 operands and result on the FP64 tensor-core path (mma.sync m8n8k4, k_dmma.cu); gemm()
+// routes Gemm<double, double> here unless ISVD_GPU_DMMA=0.  a_kc: A has unit K stride; b_nc: B
+// has unit N stride.
+bool dmma_enabled();
+void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t st);
+// C = alpha * (sum of the `splits` partial products) + beta * C (partials: batch x splits x M x N).
+void splitk_reduce(const Gemm<double, double> &g, int splits, const double *partial, cudaStream_t st);
+
 // ------------------------------------------------------------------ elementwise
 // Omega(j, c) for j < rows, c < cols: standard normal values from Philox4x32-10 (key = seed)
 // with Box-Muller, rounded to bf16; value index = offset + j * cols + c.  Written at out[j*ld + c].
