@@ -59,6 +59,7 @@ __global__ void __launch_bounds__(WM * WN * 32)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp / WN) * (BM / WM), wn0 = (warp % WN) * (BN / WN);
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (g.upper && n0 + BN <= m0) return;  // tile strictly below the diagonal: mirrored by the caller
   const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
   const int kb = sp * kchunk, ke = min(g.K, kb + kchunk);
   const double *__restrict__ A = g.A + (long long)b * g.a_bs;

@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(kThreads)
 
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (g.upper && n0 + BN <= m0) return;  // tile strictly below the diagonal: mirrored by the caller
   const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
   const int kb = sp * kchunk;
   const int ke = min(g.K, kb + kchunk);

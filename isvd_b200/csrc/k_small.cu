@@ -7,7 +7,11 @@
 // matrices.  Jacobi methods are used because they are accurate to working precision in the
 // eigenvectors and map onto one CTA; rotation order is the round-robin tournament, so each
 // round applies l/2 disjoint rotations in parallel.
+#include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 #include "kernels.h"
 #include "kn_common.cuh"
@@ -177,6 +181,18 @@ __global__ void __launch_bounds__(kEigThreads)
     const int f = *flag;
     __syncthreads();
     if (!f) break;
+    // the next sweep would rotate nothing when every pair is below the threshold: stop here
+    if (tid == 0) *flag = 0;
+    __syncthreads();
+    for (int i = warp; i < n; i += nwarp) {
+      const double aii = fabs(A[pk(i, i, n)]);
+      for (int j = i + 1 + lane; j < n; j += 32)
+        if (fabs(A[pk(i, j, n)]) > tol * fmax(sqrt(aii * fabs(A[pk(j, j, n)])), floor_)) *flag = 1;
+    }
+    __syncthreads();
+    const int g = *flag;
+    __syncthreads();
+    if (!g) break;
   }
   if (sweep == kMaxSweeps && tid == 0) atomicExch(status, kErrNumerical);
 
@@ -516,6 +532,276 @@ __global__ void __launch_bounds__(kKnThreads) kn_step_kernel(KnStep a) {
   }
 }
 
+// ------------------------------------------------------------------------------------------
+// The same two-sided Jacobi on one thread-block cluster (one matrix): the round-robin pairs are
+// spread over the cluster's CTAs, each CTA holding the full rows of A and of V' (row i =
+// eigenvector i) of the players of its pairs.  A round's rotation A := R' A R then touches only
+// rows a CTA holds (the column rotations act within each row, the row rotations within each
+// pair), so a round is local work plus one exchange: each row is stored into the shared memory
+// of the CTA that holds its player in the next round, and each CTA publishes to all CTAs the
+// diagonal entries of its rows and the off-diagonal entry A(p, q) of each next-round pair whose
+// smaller player it holds.  Every CTA then computes all rotations of the round from the same
+// table (identical results, so every CTA reaches the same convergence decision), and one
+// hardware cluster barrier per round separates the exchange from its use.  No software waits.
+constexpr int kEcThreads = 256;
+
+struct EcShape {
+  int n, ne, np, pp, rows;  // pairs per CTA (pp), rows per CTA (2 pp)
+};
+
+__device__ __forceinline__ EcShape ec_shape(int n, int cs) {
+  EcShape e;
+  e.n = n;
+  e.ne = n + (n & 1);
+  e.np = e.ne / 2;
+  e.pp = (e.np + cs - 1) / cs;
+  e.rows = 2 * e.pp;
+  return e;
+}
+
+// Position -> (slot, member): positions [0, np) are the first members of slots 0..np-1, the
+// others the second members of slots ne-1-i.
+__device__ __forceinline__ void ec_slot(int i, int np, int ne, int &slot, int &member) {
+  if (i < np) { slot = i; member = 0; } else { slot = ne - 1 - i; member = 1; }
+}
+
+__global__ void __launch_bounds__(kEcThreads, 1)
+    sym_eig_cluster_kernel(int n, const double *__restrict__ A0, double *__restrict__ V, double *__restrict__ w,
+                           int order, bool absval, int *status) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int cs = (int)cluster.num_blocks(), me = (int)cluster.block_rank();
+  const EcShape sh = ec_shape(n, cs);
+  const int ne = sh.ne, np = sh.np, R = sh.rows, tid = threadIdx.x, nt = blockDim.x;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  extern __shared__ double sm[];
+  double *rowsA = sm;                                   // [2][R][n]
+  double *rowsV = rowsA + 2 * (size_t)R * n;            // [2][R][n]
+  double *diag = rowsV + 2 * (size_t)R * n;             // [2][ne]
+  double *off = diag + 2 * ne;                          // [2][np]
+  double *rc = off + 2 * np, *rs = rc + np;             // this round's rotations
+  double *red = rs + np;                                // [kEcThreads]
+  int *rp = (int *)(red + kEcThreads), *rq = rp + np;   // this round's pairs (p < q)
+  int *mv = rq + np;                                    // per held row: [dst, dst row, player, partner, next slot]
+  int *conv = mv + 5 * R;                               // [2][16] per-CTA "a pair above the threshold" flags
+  int *any = conv + 32, *exc = any + 1;
+  double *keyb = red;                                   // diagonal after a round (reuses the reduction buffer, n <= 160 < 256)
+  __shared__ double *peerA[16], *peerV[16], *peerD[16], *peerO[16];
+  __shared__ int *peerC[16];
+  if (tid < cs) {  // the same buffers in every CTA of the cluster (distributed shared memory)
+    peerA[tid] = cluster.map_shared_rank(rowsA, tid);
+    peerV[tid] = cluster.map_shared_rank(rowsV, tid);
+    peerD[tid] = cluster.map_shared_rank(diag, tid);
+    peerO[tid] = cluster.map_shared_rank(off, tid);
+    peerC[tid] = cluster.map_shared_rank(conv, tid);
+  }
+
+  // symmetrised A, ||A||_F (every CTA the same sum in the same order), round-0 rows and tables
+  double fr = 0.0;
+  for (int e = tid; e < n * n; e += nt) {
+    const int i = e / n, j = e - i * n;
+    const double v = 0.5 * (A0[(size_t)i * n + j] + A0[(size_t)j * n + i]);
+    fr += v * v;
+  }
+  red[tid] = fr;
+  __syncthreads();
+  for (int h = nt / 2; h > 0; h >>= 1) {
+    if (tid < h) red[tid] += red[tid + h];
+    __syncthreads();
+  }
+  const double tol = kEps * fmax(1.0, sqrt((double)n));
+  const double floor_ = kEps * sqrt(red[0]);
+  for (int lr = warp; lr < R; lr += nwarp) {
+    const int slot = me * sh.pp + lr / 2;
+    const int x = slot < np ? rr_player((lr & 1) ? ne - 1 - slot : slot, 0, ne) : ne;
+    for (int j = lane; j < n; j += 32) {
+      rowsA[(size_t)lr * n + j] = x < n ? 0.5 * (A0[(size_t)x * n + j] + A0[(size_t)j * n + x]) : 0.0;
+      rowsV[(size_t)lr * n + j] = (x == j) ? 1.0 : 0.0;
+    }
+  }
+  for (int x = tid; x < ne; x += nt) diag[x] = x < n ? A0[(size_t)x * n + x] : 0.0;
+  for (int k = tid; k < np; k += nt) {
+    int p = rr_player(k, 0, ne), q = rr_player(ne - 1 - k, 0, ne);
+    if (p > q) { const int t = p; p = q; q = t; }
+    off[k] = q < n ? 0.5 * (A0[(size_t)p * n + q] + A0[(size_t)q * n + p]) : 0.0;
+  }
+  __syncthreads();
+
+  int cb = 0, sweep = 0, round = 0;
+  bool rotated_in_sweep = false;
+  for (;;) {
+    double *A = rowsA + (size_t)cb * R * n, *Vt = rowsV + (size_t)cb * R * n;
+    const double *dg = diag + cb * ne, *of = off + cb * np;
+    const int nb = cb ^ 1, nround = (round + 1) % (ne - 1);
+    // 1. all rotations of the round (every CTA alike) and where each held row goes next
+    if (tid == 0) *any = 0;
+    __syncthreads();
+    for (int k = tid; k < np; k += nt) {
+      int p = rr_player(k, round, ne), q = rr_player(ne - 1 - k, round, ne);
+      if (p > q) { const int t = p; p = q; q = t; }
+      double c = 1.0, sn = 0.0;
+      if (q < n && jacobi_rot(dg[p], dg[q], of[k], tol, floor_, c, sn)) *any = 1;
+      rp[k] = p; rq[k] = q; rc[k] = c; rs[k] = sn;
+    }
+    for (int lr = tid; lr < R; lr += nt) {
+      const int slot = me * sh.pp + lr / 2;
+      if (slot >= np) continue;
+      const int i = (lr & 1) ? ne - 1 - slot : slot;  // position this round
+      const int i2 = (i == 0) ? 0 : (i == 1 ? ne - 1 : i - 1);
+      int s2, m2;
+      ec_slot(i2, np, ne, s2, m2);
+      mv[5 * lr + 0] = s2 / sh.pp;
+      mv[5 * lr + 1] = 2 * (s2 % sh.pp) + m2;
+      mv[5 * lr + 2] = rr_player(i, round, ne);
+      mv[5 * lr + 3] = rr_player(ne - 1 - i2, nround, ne);
+      mv[5 * lr + 4] = s2;
+    }
+    __syncthreads();
+    if (*any) rotated_in_sweep = true;
+    // 2. A := A R on the held rows: warp per row, lanes over the column pairs
+    for (int lr = warp; lr < R; lr += nwarp) {
+      double *row = A + (size_t)lr * n;
+      for (int k = lane; k < np; k += 32) {
+        const double sn = rs[k];
+        if (sn == 0.0) continue;
+        const double c = rc[k];
+        const int p = rp[k], q = rq[k];
+        const double xp = row[p], xq = row[q];
+        row[p] = c * xp - sn * xq;
+        row[q] = sn * xp + c * xq;
+      }
+    }
+    __syncthreads();
+    // 3. A := R' A and V' := R' V' on the held row pairs (warp per pair); closed form on the
+    //    pair's 2 x 2 block
+    for (int ls = warp; ls < sh.pp; ls += nwarp) {
+      const int slot = me * sh.pp + ls;
+      if (slot >= np) continue;
+      const double sn = rs[slot];
+      if (sn == 0.0) continue;
+      const double c = rc[slot], t = sn / c;
+      const int p = rp[slot], q = rq[slot];
+      const bool first_is_p = mv[5 * (2 * ls) + 2] == p;  // member 0 holds the player at position `slot`
+      const int lp = 2 * ls + (first_is_p ? 0 : 1), lq = 2 * ls + (first_is_p ? 1 : 0);
+      double *ap = A + (size_t)lp * n, *aq = A + (size_t)lq * n;
+      double *vp = Vt + (size_t)lp * n, *vq = Vt + (size_t)lq * n;
+      for (int j = lane; j < n; j += 32) {
+        if (j == p) { ap[p] = dg[p] - t * of[slot]; aq[p] = 0.0; }
+        else if (j == q) { aq[q] = dg[q] + t * of[slot]; ap[q] = 0.0; }
+        else {
+          const double x1 = ap[j], x2 = aq[j];
+          ap[j] = c * x1 - sn * x2;
+          aq[j] = sn * x1 + c * x2;
+        }
+        const double v1 = vp[j], v2 = vq[j];
+        vp[j] = c * v1 - sn * v2;
+        vq[j] = sn * v1 + c * v2;
+      }
+    }
+    __syncthreads();
+    // 4. end of a sweep: stop when no rotation happened in it, or when every pair was found below
+    //    the threshold at the end of the previous sweep (the next sweep would rotate nothing);
+    //    the same decision in every CTA
+    const bool last_round = (round == ne - 2);
+    bool converged = false;
+    if (round == 0 && sweep > 0) {
+      converged = true;
+      for (int c = 0; c < cs; ++c) converged &= conv[cb * 16 + c] == 0;
+    }
+    const bool done = (last_round && !rotated_in_sweep) || converged;
+    const bool exhausted = last_round && sweep + 1 >= kMaxSweeps;
+    // diagonal after this round: the table and the closed forms of step 3 (the values the rows hold)
+    double *key = keyb;
+    if (done || exhausted || last_round) {
+      for (int y = tid; y < n; y += nt) {
+        const int pos = (y == 0) ? 0 : 1 + ((y - 1 - round) % (ne - 1) + (ne - 1)) % (ne - 1);
+        int sl, mb;
+        ec_slot(pos, np, ne, sl, mb);
+        double ky = dg[y];
+        if (rs[sl] != 0.0) {
+          const double t = rs[sl] / rc[sl];
+          ky = (y == rp[sl]) ? dg[y] - t * of[sl] : dg[y] + t * of[sl];
+        }
+        key[y] = ky;
+      }
+      if (tid == 0) *exc = 0;
+      __syncthreads();
+    }
+    if (done || exhausted) {
+      if (exhausted && !done && me == 0 && tid == 0) atomicExch(status, kErrNumerical);
+      // each CTA writes the eigenpairs of the players it holds, ranked by `order`
+      for (int lr = warp; lr < R; lr += nwarp) {
+        const int slot = me * sh.pp + lr / 2;
+        if (slot >= np) continue;
+        const int x = mv[5 * lr + 2];
+        if (x >= n) continue;
+        const double kx = key[x];
+        int rank = 0;
+        for (int y = lane; y < n; y += 32) {
+          const double ky = key[y];
+          rank += (order > 0) ? (fabs(ky) > fabs(kx) || (fabs(ky) == fabs(kx) && y < x))
+                              : (ky < kx || (ky == kx && y < x));
+        }
+        for (int o = 16; o > 0; o >>= 1) rank += __shfl_xor_sync(0xffffffffu, rank, o);
+        if (lane == 0) w[rank] = absval ? fabs(kx) : kx;
+        const double *vrow = Vt + (size_t)lr * n;
+        for (int j = lane; j < n; j += 32) V[(size_t)j * n + rank] = vrow[j];
+      }
+      return;
+    }
+    if (last_round) {  // any off-diagonal entry of a held row above the rotation threshold?
+      for (int lr = warp; lr < R; lr += nwarp) {
+        const int slot = me * sh.pp + lr / 2;
+        if (slot >= np) continue;
+        const int x = mv[5 * lr + 2];
+        if (x >= n) continue;
+        const double *row = A + (size_t)lr * n;
+        const double kx = fabs(key[x]);
+        for (int j = lane; j < n; j += 32)
+          if (j != x && fabs(row[j]) > tol * fmax(sqrt(kx * fabs(key[j])), floor_)) *exc = 1;
+      }
+      __syncthreads();
+    }
+    // 5. exchange: each held row to its next-round holder (warp per row, coalesced stores into
+    //    that CTA's shared memory), the diagonal and next-pair off-diagonal entries to every CTA
+    for (int lr = warp; lr < R; lr += nwarp) {
+      const int slot = me * sh.pp + lr / 2;
+      if (slot >= np) continue;
+      const int dst = mv[5 * lr + 0];
+      const size_t drow = ((size_t)nb * R + mv[5 * lr + 1]) * n;
+      const double *a = A + (size_t)lr * n, *v = Vt + (size_t)lr * n;
+      double *ra = peerA[dst] + drow, *rv = peerV[dst] + drow;
+      for (int j = lane; j < n; j += 32) {
+        ra[j] = a[j];
+        rv[j] = v[j];
+      }
+    }
+    for (int e = tid; e < R * cs; e += nt) {
+      const int lr = e % R, dst = e / R;
+      const int slot = me * sh.pp + lr / 2;
+      if (slot >= np) continue;
+      const int x = mv[5 * lr + 2], partner = mv[5 * lr + 3], s2 = mv[5 * lr + 4];
+      const double *row = A + (size_t)lr * n;
+      peerD[dst][nb * ne + x] = x < n ? row[x] : 0.0;
+      if (x < partner && partner < n) peerO[dst][nb * np + s2] = row[partner];
+      else if (partner >= n && x < n) peerO[dst][nb * np + s2] = 0.0;
+    }
+    if (last_round && tid < cs) peerC[tid][nb * 16 + me] = *exc;
+    cluster.sync();
+    cb = nb;
+    round = nround;
+    if (round == 0) {
+      ++sweep;
+      rotated_in_sweep = false;
+    }
+  }
+}
+
+size_t eig_cluster_smem(int n, int cs) {
+  const int ne = n + (n & 1), np = ne / 2, pp = (np + cs - 1) / cs, R = 2 * pp;
+  return (size_t)(4 * R * n + 2 * ne + 2 * np + 2 * np + kEcThreads) * 8 + (size_t)(2 * np + 5 * R + 32 + 2) * 4;
+}
+
 size_t eig_smem(int n, bool vs) {
   const int ne = n + (n & 1), np = ne / 2;
   const size_t npk = ((size_t)n * (n + 1) / 2 + 1) & ~(size_t)1;
@@ -525,10 +811,109 @@ size_t svd_smem(int n) { return (size_t)n * n * 8 + (size_t)n * 8 + 16; }
 
 }  // namespace
 
+namespace {
+
+// Cluster size for the one-matrix eigensolver (0: use the one-CTA kernel): the largest of 16, 8,
+// 4, 2 that the device can co-schedule, for 112 <= n <= 160.  A round costs about 2.5 us on the
+// cluster whatever n (barrier and exchange), against shared-memory bandwidth on one CTA, which
+// grows as n^2: measured per solve on B200, 3.45 against 4.18 ms at n = 128 and 5.7 against
+// 10.8 ms at n = 160, but 2.49 against 2.19 ms at n = 96.
+int eig_cluster_size(int n, cudaStream_t st) {
+  static int decided[2] = {-1, -1};  // per size class: n <= 128, n <= 160
+  if (n < 112 || n > 160) return 0;
+  // ISVD_GPU_EIG_CLUSTER: 0 off, 2..16 the largest size tried
+  static const int top = [] {
+    const char *e = getenv("ISVD_GPU_EIG_CLUSTER");
+    return e ? std::max(0, std::min(16, atoi(e))) : 16;
+  }();
+  if (top < 2) return 0;
+  int &d = decided[n > 128 ? 1 : 0];
+  if (d >= 0) return d;
+  CK(cudaFuncSetAttribute(sym_eig_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  d = 0;
+  for (int cs = top; cs >= 2; cs /= 2) {
+    const size_t smem = eig_cluster_smem(n > 128 ? 160 : 128, cs);
+    if (cudaFuncSetAttribute(sym_eig_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(kEcThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cs;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, sym_eig_cluster_kernel, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nc >= 1) {
+      d = cs;
+      break;
+    }
+  }
+  return d;
+}
+
+}  // namespace
+
+// Kernel time under `tag` when kernel timing is on (isvd_gpu_profile_enable).
+struct ProfileScope {
+  const char *tag;
+  cudaStream_t st;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ProfileScope(const char *t, cudaStream_t s) : tag(t), st(s) {
+    if (!profiling()) return;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, st));
+  }
+  ~ProfileScope() {
+    if (!e0) return;
+    float ms = 0.f;
+    if (cudaEventRecord(e1, st) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+      profile_add(tag, ms, 0.0);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+};
+
 void sym_eig_batched(int n, int batch, const double *A, double *V, double *w, int order, bool absval, int *status,
                      cudaStream_t st) {
   if (n <= 0 || batch <= 0) return;
+  ProfileScope prof("sym_eig", st);
   Runtime &rt = Runtime::get();
+  if (batch == 1) {
+    const int cs = eig_cluster_size(n, st);
+    if (cs > 0) {
+      const size_t smem = eig_cluster_smem(n, cs);
+      CK(cudaFuncSetAttribute(sym_eig_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(cs);
+      cfg.blockDim = dim3(kEcThreads);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = st;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = cs;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      CK(cudaLaunchKernelEx(&cfg, sym_eig_cluster_kernel, n, A, V, w, order, absval, status));
+      KLAUNCHED();
+      return;
+    }
+  }
   const size_t smem_vs = eig_smem(n, true);
   if (smem_vs <= rt.smem_optin) {
     CK(cudaFuncSetAttribute(sym_eig_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_vs));

@@ -25,6 +25,9 @@ struct Gemm {
   long long c_rs = 0, c_cs = 0, c_bs = 0;
   int batch = 1;
   int splits = 0;  // 0: choose automatically
+  // C symmetric (M == N, A = B'): tiles entirely below the diagonal are not computed; the caller
+  // completes C with mirror_upper
+  bool upper = false;
 };
 
 template <class T, class Tout>

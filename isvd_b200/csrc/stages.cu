@@ -223,7 +223,9 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.A = qs; g.a_rs = 1; g.a_cs = ldq;
     g.B = qs; g.b_rs = ldq; g.b_cs = 1;
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
+    g.upper = true;  // G is symmetric: the upper triangle's tiles, then mirrored
     gemm(g, c.st);
+    mirror_upper(G.p, Nl, Nl, c.st);
   }
   // Row blocks on several ranks: G is the one exchange of the integration (the reference
   // exchanges Bc and Bgc in every iteration, @x@_integrate_kolmogorov_nagumo.c:160,178); every

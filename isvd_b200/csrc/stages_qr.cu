@@ -159,7 +159,9 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     g.A = qs; g.a_rs = 1; g.a_cs = ldq;
     g.B = qs; g.b_rs = ldq; g.b_cs = 1;
     g.C = G.p; g.c_rs = Nl; g.c_cs = 1;
+    g.upper = true;  // G is symmetric: the upper triangle's tiles, then mirrored
     gemm(g, st);
+    mirror_upper(G.p, Nl, Nl, st);
   }
   // row blocks on several ranks: G is the integration's one exchange (the reference exchanges Bc,
   // Bgc and two scalars per iteration, @x@_integrate_wen_yin.c:206-345)

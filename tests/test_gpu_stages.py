@@ -185,3 +185,33 @@ def test_invalid_leading_dimension_reports_error(lib, golden):
     code, msg = lib.last_error()
     assert code == 1 and "ldyst" in msg
     lib.clear_error()
+
+
+@pytest.mark.parametrize("l", [64, 65, 97, 128, 129, 160])
+def test_postprocess_wide_sketch_eigensolver(lib, oracle, l):
+    """Gramian and symmetric postprocessing at l = 64..160 (the l x l eigensolver on a thread-block
+    cluster when the device allows one; odd l pairs one row with a dummy in every round): FP64
+    results against the oracle, eigenvalues to 1e-12 and vectors to 1e-9."""
+    rng = np.random.default_rng(l)
+    m, n = 400, 900
+    a = rng.standard_normal((m, n)) * 0.99 ** np.arange(n)
+    q = np.linalg.qr(rng.standard_normal((m, l)))[0]
+    prm = lib.create_param(m, n, l, 0, 1)
+    s = np.zeros(l)
+    ut = np.zeros((m, l))
+    vt = np.zeros((n, l))
+    lib.postprocess("d", "GR", prm, a, n, q, l, s, ut, l, vt, l)
+    assert lib.last_error()[0] == 0, lib.last_error()
+    s_o, u_o, v_o = oracle.postprocess_gramian(a, q, l)
+    assert np.abs(s - s_o).max() < 1e-12 * s_o.max()
+    assert oracle.column_angles(ut, u_o).max() < 1e-9
+    assert oracle.column_angles(vt, v_o).max() < 1e-9
+    sym = a[:, :m] @ a[:, :m].T / m - 0.3 * np.eye(m)  # indefinite: ascending order with signs
+    prm = lib.create_param(m, m, l, 0, 1)
+    s = np.zeros(l)
+    u = np.zeros((m, l))
+    lib.postprocess("d", "SY", prm, sym, m, q, l, s, u, l, None, l, ut_root=-1, vt_root=-2)
+    assert lib.last_error()[0] == 0, lib.last_error()
+    lam, u_s = oracle.postprocess_symmetric(sym, q, l)
+    assert np.abs(s - lam).max() < 1e-12 * np.abs(lam).max()
+    assert oracle.column_angles(u, u_s).max() < 1e-9
