@@ -151,13 +151,27 @@ void dmma_launch(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream
   const long long tiles = (long long)gx * gy * g.batch;
   int splits = g.splits;
   if (splits <= 0) {
-    const long long target = 2LL * rt.num_sms;
+    // split-K by a time model: the busiest SM runs ceil(tiles s / SMs) CTAs of BM BN (K / s) FMAs
+    // (about 0.23 TFLOP/s per SM on mma.sync f64) plus a fixed 2 us each, and s > 1 adds the
+    // partial sums' round trip (s + 1) M N 8 bytes at about 4 TB/s; the smallest s within 3 % of
+    // the best, with at least 64 of K per split and at most 512 MB of partials
+    const double rate = 0.23e12, fixed = 2e-6, bw = 4e12;
+    const long long mnb = (long long)g.M * g.N * g.batch;
+    auto model = [&](long long s) {
+      const long long per_sm = (tiles * s + rt.num_sms - 1) / rt.num_sms;
+      const double kc = (double)((g.K + s - 1) / s);
+      return per_sm * (2.0 * BM * BN * kc / rate + fixed) + (s > 1 ? (double)(s + 1) * mnb * 8.0 / bw : 0.0);
+    };
+    const long long smax = std::max<long long>(
+        1, std::min<long long>({64, (long long)g.K / 64, (512LL << 20) / std::max<long long>(1, mnb * 8)}));
+    double best = model(1);
+    for (long long s = 2; s <= smax; ++s) best = std::min(best, model(s));
     splits = 1;
-    if (tiles < target) {
-      const long long s = (target + tiles - 1) / tiles;
-      const long long smax = std::max<long long>(1, g.K / (8 * kBK));
-      splits = (int)std::min<long long>(s, smax);
-    }
+    for (long long s = 1; s <= smax; ++s)
+      if (model(s) <= 1.03 * best) {
+        splits = (int)s;
+        break;
+      }
   }
   int kchunk = (g.K + splits - 1) / splits;
   kchunk = ((kchunk + kBK - 1) / kBK) * kBK;
