@@ -429,6 +429,7 @@ void kn_step(const KnStep &a, cudaStream_t st) {
   if (a.l > kKsMaxL) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > %d", a.l, kKsMaxL);
   const int cs = choose_cluster_size(a, st);
   if (cs == 0) {  // no cluster launch on this device: the grid-barrier kernel (work 8 l^2 + 64 fits)
+    CK(cudaMemsetAsync(a.bar, 0, 8, st));  // its barrier counters
     kn_step_fixed(a, Runtime::get().num_sms, st);
     return;
   }

@@ -238,7 +238,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
     coeff_orthonormalize(c, Nl, l, N, G.p, Xo.p);
   }
   // iterates W = [M | B | Bgc] (Nl x 3l, current and next), [Dc; Dgc], step outputs
-  DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64), err(2);
+  DBuf<double> Wb(6 * nl), DD(2 * ll), C(ll), Ci(ll), F(ll), Fs(4 * ll), work(kKnWorkMatrices * ll + 64);
   double *Wc = Wb.p, *Wp = Wb.p + 3 * nl;
   copy2d<double, double>(G.p, Nl, 1, Wc + l, lw, 1, Nl, l, c.st);  // Bc = Qs' Q0 = G[:, 0:l]   (:157)
   set_identity<double>(Wc, Nl, l, lw, c.st);                       // Qc = Q0 = Qs [I; 0]       (:154)
@@ -271,7 +271,6 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
       gemm(g, c.st);
     }
     // l x l step (:187-218)
-    CK(cudaMemsetAsync(rt.ctl, 0, 8, c.st));
     KnStep s;
     s.l = l; s.Dc = DD.p; s.Dgc = DD.p + ll; s.C = C.p; s.Cinv = Ci.p; s.F = F.p; s.err = errp;
     s.work = work.p; s.status = c.status; s.bar = rt.ctl;
@@ -292,18 +291,18 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   IterResult res;
   double herr = 0.0;
   const int cap = maxit > 0 ? maxit : 1000000;
-  // Iteration i + 1 is queued before the host reads the error of iteration i (copied into pinned
-  // memory right behind iteration i), so the GPU never waits for the host's convergence test.
-  // Iteration i + 1 reads W(i) and writes the other buffer and error slot: when iteration i has
-  // converged, its result W(i) is intact and the extra iteration is discarded.
+  // Iteration i + 1 is queued before the host reads the error of iteration i, so the GPU never
+  // waits for the host's convergence test.  The step kernel writes the error straight into pinned
+  // host memory (one slot per parity; no copy behind the iteration).  Iteration i + 1 reads W(i)
+  // and writes the other buffer and error slot: when iteration i has converged, its result W(i)
+  // is intact and the extra iteration is discarded.
   double *hpin = rt.host_pin;
   cudaEvent_t ev[2];
   for (int e = 0; e < 2; ++e) CK(cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming));
   auto launch = [&](int it, double *cur, double *next) {
     const int par = it & 1;
-    if (graphs.usable && it > 2) graphs.run(par, [&] { iteration(cur, next, err.p + par); });
-    else iteration(cur, next, err.p + par);
-    CK(cudaMemcpyAsync(hpin + par, err.p + par, sizeof(double), cudaMemcpyDeviceToHost, c.st));
+    if (graphs.usable && it > 2) graphs.run(par, [&] { iteration(cur, next, hpin + par); });
+    else iteration(cur, next, hpin + par);
     CK(cudaEventRecord(ev[par], c.st));
   };
   int iter = 1;
