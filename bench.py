@@ -210,6 +210,79 @@ def config_dict(w):
 BATCH = dict(count=256, m=(512, 8192), n=(256, 4096), k=(8, 16, 32, 64), N=8, noise=1e-4, seed=4)
 
 
+CONFIG3 = dict(m=50000, n=50000, rank=5000, k=64, p=64, N=64, noise=1e-3, seed=3)
+
+
+def config3_main(args):
+    """The 50000 x 50000 FP32 parity case: sigma_i = (1 + i)^(-1/2) for i < 5000 on Haar factors,
+    + 1e-3 noise; k = 64, p = 64, N = 64; GP / TS / WY (tol 1e-4, maxit 512) / GR on column blocks
+    (dista 'C').  One line: the MIXED solve (A resident, device-timed over K solves after W warm-up
+    solves) beside one NATIVE FP64 solve on the FP64 copy of A with the same seed, and the largest
+    relative difference of the k leading singular values."""
+    import torch
+    import isvd_b200
+    w = CONFIG3
+    dev = torch.device("cuda", 0)
+    lib = isvd_b200.load()
+    stream = torch.cuda.current_stream(dev)
+    lib.lib.isvd_gpu_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    g = torch.Generator(device=dev).manual_seed(w["seed"])
+    m, n, r, k, p, N = w["m"], w["n"], w["rank"], w["k"], w["p"], w["N"]
+    l = k + p
+    u = torch.linalg.qr(torch.randn(m, r, generator=g, device=dev, dtype=torch.float32))[0]
+    v = torch.linalg.qr(torch.randn(n, r, generator=g, device=dev, dtype=torch.float32))[0]
+    sig = (1.0 + torch.arange(r, device=dev, dtype=torch.float32)) ** -0.5
+    a = torch.randn(m, n, generator=g, device=dev, dtype=torch.float32).mul_(w["noise"])
+    a.addmm_(u * sig, v.t())
+    del u, v
+    prm = lib.create_param(m, n, k, p, N)
+    algs = ("GP", "TS", "WY", "GR")
+
+    def run(x, mat, precision):
+        dt = mat.dtype
+        s = torch.zeros(l, dtype=dt, device=dev)
+        ut = torch.zeros((m, l), dtype=dt, device=dev)
+        vt = torch.zeros((n, l), dtype=dt, device=dev)
+        retv, times, status = lib.isvd(x, prm, algs, mat, n, s, ut, l, vt, l, seed=w["seed"], dista=b"C", ordera=b"R",
+                                       retc=(0, 0, 2, 0), argv=[None, None, [512, 1e-4], None], precision=precision)
+        if status != 0:
+            raise RuntimeError("config 3 solve failed: %s" % (lib.last_error(),))
+        return s, retv, times
+
+    for _ in range(args.warmup):
+        run("s", a, 1)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stage = np.zeros(4)
+    with ClockSampler(0) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            s_mixed, retv, times = run("s", a, 1)
+            stage += np.array(times)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    mixed_ms = ev0.elapsed_time(ev1) / args.steps
+    wy_mixed = int(retv[2][0])
+    a64 = a.double()
+    del a
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    s64, retv64, times64 = run("d", a64, 0)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    fp64_ms = ev0.elapsed_time(ev1)
+    s_ref = s64[:k].cpu().numpy()
+    err = float(np.abs(s_mixed[:k].double().cpu().numpy() - s_ref).max() / s_ref.max())
+    lib.lib.isvd_gpu_set_stream(None)
+    print(json.dumps({"workload": "iSVD config 3: 50000x50000 FP32, sigma_i=(1+i)^-0.5 (i<5000) + 1e-3 noise; "
+                                  "k=64 p=64 N=64; GP/TS/WY(1e-4,512)/GR, column blocks, 1 MPI rank",
+                      "mixed_ms_per_solve": mixed_ms, "mixed_stage_ms": list(1e3 * stage / args.steps),
+                      "mixed_wy_iterations": wy_mixed, "fp64_ms": fp64_ms,
+                      "fp64_stage_ms": [1e3 * t for t in times64], "fp64_wy_iterations": int(retv64[2][0]),
+                      "sigma_rel_err_max": err, "steps": args.steps, "warmup": args.warmup,
+                      "clocks": clk.summary()}), flush=True)
+
+
 def batch_main(args):
     """Batched uneven solves: 256 FP32 matrices, m log-uniform in [512, 8192], n log-uniform in
     [256, 4096] with n <= m, each rank 4k with a geometric spectrum (1 .. 1e-3) plus noise, k in
@@ -316,9 +389,13 @@ def main():
                     help="one MIXED solve and its stage times, nothing else (for ncu launch lists / captures)")
     ap.add_argument("--batched", action="store_true",
                     help="the batched-solves workload (256 uneven matrices) instead of the single large solve")
+    ap.add_argument("--config3", action="store_true",
+                    help="the 50000 x 50000 TS / WY / column-block parity case, MIXED beside FP64")
     args = ap.parse_args()
     if args.batched:
         return batch_main(args)
+    if args.config3:
+        return config3_main(args)
     w = WORKLOADS[args.size]
     if args.impl == "reference":
         return reference_arm(args, w)

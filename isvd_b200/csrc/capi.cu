@@ -534,6 +534,9 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   progress("Orthogonalizing ............... ");
   if (bo == "TS") {
     orth_tsqr_dev<T>(c.sc, ml, l, N, Y.p, Nl);
+    // MIXED: KN and WY re-orthonormalize the blocks in the coordinates of G (G_ii = I exactly),
+    // removing what the tensor-core CholeskyQR leaves of non-orthogonality
+    c.sc.deferred_orth = (bi == "KN" || bi == "WY");
   } else {
     // KN and WY form G = Qs' Qs anyway: they take over the second pass in the coordinates of G
     c.sc.deferred_orth = (bi == "KN" || bi == "WY");

@@ -213,20 +213,21 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
 }
 
 template <class T>
-void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G) {
+void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G,
+                     int np) {
   UmmaGemm g;
   g.M = Nl; g.N = Nl; g.K = m;
   PlaneBuf qt;
   if (Nl % 8 == 0) {
     Planes a = qp;
-    a.np = 2;
+    a.np = np;
     a.mn_major = true;
     g.A = a; g.B = a;
   } else {
-    make_planes<T>(qt, qs, ldq, m, Nl, 2, true, c.st);  // Qs' planes (Nl x m)
+    make_planes<T>(qt, qs, ldq, m, Nl, np, true, c.st);  // Qs' planes (Nl x m)
     g.A = qt.P; g.B = qt.P;
   }
-  set_products(g, 2, 2);
+  set_products(g, np, np);
   g.C = G; g.c_double = true; g.c_rs = Nl; g.c_cs = 1;
   g.upper = true;
   g.status = c.status;
@@ -345,7 +346,7 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, long long 
   template void mixed_block_apply<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
                                      const T *, T *, long long);                                           \
   template void mixed_gram_full<T>(const StageCtx &, const Planes &, int, int, const T *, long long,          \
-                                   double *);                                                              \
+                                   double *, int);                                                              \
   template void mixed_apply_coeff<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
                                      const double *, T *, long long);                                      \
   template void mixed_project<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *,     \

@@ -67,7 +67,8 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
 
 // G = Qs' Qs (Nl x Nl, FP64 out; symmetric, computed on the upper triangle and mirrored).
 template <class T>
-void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G);
+void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G,
+                     int np = 2);
 
 // Qbar = Qs M (M: Nl x l FP64, row-major) -> qt (m x l, ld ldqt).
 template <class T>
