@@ -52,7 +52,7 @@ def peaks():
 # DRAM bytes (read + write) of the sketch kernel's one launch over the config-2 matrix
 # (200000 x 20000, N l = 4096), from a one-pass ncu capture of a full solve (dram__bytes_read.sum +
 # dram__bytes_write.sum; see profiles/isvd_config2_mixed_launch_list.md)
-SKETCH_LAUNCH_TRAFFIC = 113.735330816e9 + 3.395452928e9
+SKETCH_LAUNCH_TRAFFIC = 86.989471744e9 + 3.400887296e9
 
 
 class ClockSampler:
