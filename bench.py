@@ -28,7 +28,7 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 WORKLOADS = {
-    # BASELINE config 2 (the metric's configuration)
+    # the headline workload: 200000 x 20000 FP32, rank-2000 factors, k = 100, p = 28, N = 32
     "full": dict(m=200000, n=20000, rank=2000, k=100, p=28, N=32, noise=1e-4, seed=2),
     # a reduced shape of the same construction, for quick checks
     "small": dict(m=20000, n=4000, rank=400, k=100, p=28, N=8, noise=1e-4, seed=2),
@@ -49,9 +49,9 @@ def peaks():
         return 6650.0, 1590.0, 1400.0, "fallback"
 
 
-# DRAM bytes (read + write) of the sketch kernel's one launch over the config-2 matrix
-# (200000 x 20000, N l = 4096), from a one-pass ncu capture of a full solve (dram__bytes_read.sum +
-# dram__bytes_write.sum; see profiles/isvd_config2_mixed_launch_list.md)
+# DRAM bytes (read + write) of the sketch kernel's one launch over the 200000 x 20000 matrix
+# (N l = 4096), from a one-pass ncu capture of a full solve (dram__bytes_read.sum +
+# dram__bytes_write.sum, graphs off, `bench.py --single`)
 SKETCH_LAUNCH_TRAFFIC = 86.989471744e9 + 3.400887296e9
 
 
@@ -198,7 +198,7 @@ def reference_arm(args, w):
 
 
 def config_dict(w):
-    return {"workload": "iSVD config 2: %dx%d FP32, rank-%d Haar factors, sigma 1..1e-3 geometric, +%.0e noise; "
+    return {"workload": "iSVD %dx%d FP32, rank-%d Haar factors, sigma 1..1e-3 geometric, +%.0e noise; "
                         "k=%d p=%d N=%d; GP/GR/KN(1e-4,256)/GR, row block, 1 MPI rank"
                         % (w["m"], w["n"], w["rank"], w["noise"], w["k"], w["p"], w["N"]),
             "m": w["m"], "n": w["n"], "k": w["k"], "p": w["p"], "N": w["N"], "seed": w["seed"],
@@ -210,10 +210,10 @@ def config_dict(w):
 BATCH = dict(count=256, m=(512, 8192), n=(256, 4096), k=(8, 16, 32, 64), N=8, noise=1e-4, seed=4)
 
 
-CONFIG3 = dict(m=50000, n=50000, rank=5000, k=64, p=64, N=64, noise=1e-3, seed=3)
+SQUARE50K = dict(m=50000, n=50000, rank=5000, k=64, p=64, N=64, noise=1e-3, seed=3)
 
 
-def config3_main(args):
+def square50k_main(args):
     """The 50000 x 50000 FP32 parity case: sigma_i = (1 + i)^(-1/2) for i < 5000 on Haar factors,
     + 1e-3 noise; k = 64, p = 64, N = 64; GP / TS / WY (tol 1e-4, maxit 512) / GR on column blocks
     (dista 'C').  One line: the MIXED solve (A resident, device-timed over K solves after W warm-up
@@ -221,7 +221,7 @@ def config3_main(args):
     relative difference of the k leading singular values."""
     import torch
     import isvd_b200
-    w = CONFIG3
+    w = SQUARE50K
     dev = torch.device("cuda", 0)
     lib = isvd_b200.load()
     stream = torch.cuda.current_stream(dev)
@@ -246,7 +246,7 @@ def config3_main(args):
         retv, times, status = lib.isvd(x, prm, algs, mat, n, s, ut, l, vt, l, seed=w["seed"], dista=b"C", ordera=b"R",
                                        retc=(0, 0, 2, 0), argv=[None, None, [512, 1e-4], None], precision=precision)
         if status != 0:
-            raise RuntimeError("config 3 solve failed: %s" % (lib.last_error(),))
+            raise RuntimeError("50000 x 50000 solve failed: %s" % (lib.last_error(),))
         return s, retv, times
 
     for _ in range(args.warmup):
@@ -274,7 +274,7 @@ def config3_main(args):
     s_ref = s64[:k].cpu().numpy()
     err = float(np.abs(s_mixed[:k].double().cpu().numpy() - s_ref).max() / s_ref.max())
     lib.lib.isvd_gpu_set_stream(None)
-    print(json.dumps({"workload": "iSVD config 3: 50000x50000 FP32, sigma_i=(1+i)^-0.5 (i<5000) + 1e-3 noise; "
+    print(json.dumps({"workload": "iSVD 50000x50000 FP32, sigma_i=(1+i)^-0.5 (i<5000) + 1e-3 noise; "
                                   "k=64 p=64 N=64; GP/TS/WY(1e-4,512)/GR, column blocks, 1 MPI rank",
                       "mixed_ms_per_solve": mixed_ms, "mixed_stage_ms": list(1e3 * stage / args.steps),
                       "mixed_wy_iterations": wy_mixed, "fp64_ms": fp64_ms,
@@ -389,13 +389,13 @@ def main():
                     help="one MIXED solve and its stage times, nothing else (for ncu launch lists / captures)")
     ap.add_argument("--batched", action="store_true",
                     help="the batched-solves workload (256 uneven matrices) instead of the single large solve")
-    ap.add_argument("--config3", action="store_true",
+    ap.add_argument("--square50k", action="store_true",
                     help="the 50000 x 50000 TS / WY / column-block parity case, MIXED beside FP64")
     args = ap.parse_args()
     if args.batched:
         return batch_main(args)
-    if args.config3:
-        return config3_main(args)
+    if args.square50k:
+        return square50k_main(args)
     w = WORKLOADS[args.size]
     if args.impl == "reference":
         return reference_arm(args, w)
@@ -486,12 +486,12 @@ def main():
     # the sketch runs as back-to-back launches inside the solve: the sustained bf16 figure is its
     # denominator; the burst figure is reported beside it
     peak3, peak3_burst = bf16_sus / nprod, bf16 / nprod
-    config2 = (m, n, l * N) == (200000, 20000, 4096)
+    headline_shape = (m, n, l * N) == (200000, 20000, 4096)
     roofline = {"bound": "tensor", "kernel": "umma_gemm_kernel (sketch Y = A Omega, %d bf16 plane products)" % nprod,
                 "achieved": achieved, "peak": peak3, "unit": "TFLOP/s",
                 "frac": (achieved / peak3) if achieved else None,
                 "peak_burst": peak3_burst, "frac_burst": (achieved / peak3_burst) if achieved else None,
-                "traffic": SKETCH_LAUNCH_TRAFFIC if config2 and sketch_launches == 1 else None,
+                "traffic": SKETCH_LAUNCH_TRAFFIC if headline_shape and sketch_launches == 1 else None,
                 "traffic_unit": "bytes per launch (one launch over all m rows; ncu, dram read + write)",
                 "alg_bytes_per_launch": float(m * n * 4 + m * l * N * 4 + n * l * N * 2),
                 "convention": "algorithmic 2 m n Nl flops per solve / kernel time; peak = %s bf16 dense "

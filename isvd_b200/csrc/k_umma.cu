@@ -1237,7 +1237,7 @@ static bool pair_ok(const UmmaGemm &g) {
 }
 // MN-major pairs (Gram matrices Q'Q of row-major panels; ISVD_UMMA_PAIR_MN=0 turns them off): each
 // SM stages half of the B tile, which halves the L2 traffic of these shared-operand products (the
-// config-2 Gram Qs'Qs, 4096 x 4096 x 200000 as 2 x 2 planes: 13.3 -> 8.0 ms).
+// Gram Qs'Qs of a 200000 x 4096 Qs, as 2 x 2 planes: 13.3 -> 8.0 ms).
 static bool pair_mn_ok(const UmmaGemm &g) {
   const char *e = getenv("ISVD_UMMA_PAIR_MN");
   if (e && atoi(e) == 0) return false;
