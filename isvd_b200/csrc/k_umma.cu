@@ -1025,16 +1025,25 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   int splits = g.splits;
   if (const char *e = getenv("ISVD_UMMA_SPLITS")) splits = atoi(e);  // diagnostic override
   if (splits <= 0) {
-    // split-K against wave quantisation (one CTA per SM): the time of s splits is
-    // ceil(tiles s / SMs) / s full-K tile times; take the smallest s within 3 % of the best
-    // (s <= 16, at least 8 k-blocks per split)
-    // (only below four waves: beyond, quantisation costs under 6 % and partial sums add traffic)
+    // split-K by a time model (one CTA per SM): the busiest SM runs ceil(tiles s / SMs) CTAs of
+    // ceil(k-blocks / s) k-blocks (BM BN BK 2 nprod flops each at about 9.5 TFLOP/s of bf16 per
+    // SM) plus a fixed 3 us (TMEM, pipeline fill, epilogue), and s > 1 adds the FP32 partials'
+    // round trip, (s + 1) M N 4 bytes at about 3 TB/s; the smallest s within 3 % of the best
+    // (s <= 16, at least 8 k-blocks per split; only below four waves, beyond which quantisation
+    // costs under 6 % and partial sums add traffic)
     const int smax = tiles < 4LL * rt.num_sms ? (int)std::max(1, std::min(16, p.total_kb / 8)) : 1;
+    const double t_kb = (double)BM * BN * BK * 2.0 * g.nprod / 9.5e12, t_fixed = 3e-6, bw = 3e12;
+    const double mnb = (double)g.M * g.N * g.batch;
+    auto model = [&](int sp) {
+      const long long per_sm = (tiles * sp + rt.num_sms - 1) / rt.num_sms;
+      const long long kb = (p.total_kb + sp - 1) / sp;
+      return per_sm * (kb * t_kb + t_fixed) + (sp > 1 ? (sp + 1) * mnb * 4.0 / bw : 0.0);
+    };
     double best = 1e30;
-    for (int sp = 1; sp <= smax; ++sp) best = std::min(best, (double)((tiles * sp + rt.num_sms - 1) / rt.num_sms) / sp);
+    for (int sp = 1; sp <= smax; ++sp) best = std::min(best, model(sp));
     splits = 1;
     for (int sp = 1; sp <= smax; ++sp)
-      if ((double)((tiles * sp + rt.num_sms - 1) / rt.num_sms) / sp <= 1.03 * best) {
+      if (model(sp) <= 1.03 * best) {
         splits = sp;
         break;
       }
@@ -1276,8 +1285,13 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   } else if (bmn) {
     launch_t<128, 64, false, true>(g, st, status);
   } else if (small_n) {
-    // six or more planes: 32-deep k-blocks give four pipeline stages instead of two
-    if (g.A.np + g.B.np >= 5 && !smalln_bk64()) launch_t<128, 32, false, false>(g, st, status);
+    // six or more planes: 32-deep k-blocks give four pipeline stages instead of two, which pays
+    // when there are many tiles; for a few split-K tiles (the Kolmogorov-Nagumo G B product,
+    // 4096 x 128 x 4096) 64-deep k-blocks halve the per-k-block overhead (19.4 against 20.7 ms
+    // for 107 iterations)
+    const long long tiles128 = (long long)((g.N + 127) / 128) * ((g.M + BM - 1) / BM) * g.batch;
+    const bool few_tiles = tiles128 < Runtime::get().num_sms;
+    if (g.A.np + g.B.np >= 5 && !smalln_bk64() && !few_tiles) launch_t<128, 32, false, false>(g, st, status);
     else launch_t<128, 64, false, false>(g, st, status);
   } else if (g.batch == 1 && g.splits <= 0 && !g.upper && pair_ok(g)) {
     if (pair_bk() == 32) launch_pair<32, false>(g, st, status);
