@@ -543,12 +543,19 @@ def main():
         del a
         torch.cuda.synchronize()
         solve(lib, "s", prm, ah, n, sh, uh, vh, l, seed, 1)  # warm
+        torch.cuda.synchronize()
         barrier()
-        t0 = time.perf_counter()
+        torch.cuda.synchronize()
+        # device-timed on the library's stream: the panel copies run on the library's copy stream
+        # but each is joined into this stream before the call returns, as are the output copies
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         reps = 2
+        e0.record(stream)
         for _ in range(reps):
             solve(lib, "s", prm, ah, n, sh, uh, vh, l, seed, 1)
-        te = (time.perf_counter() - t0) / reps
+        e1.record(stream)
+        torch.cuda.synchronize()
+        te = e0.elapsed_time(e1) / 1e3 / reps
         if dist is not None:
             t = torch.tensor([te], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
