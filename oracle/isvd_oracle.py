@@ -62,19 +62,26 @@ def _sym_upper(x):
     return np.triu(x) + np.triu(x, 1).T
 
 
-def integrate_kolmogorov_nagumo(qs, l, N, maxit=256, tol=1e-4, trace=None):
+def _local(x):
+    return x
+
+
+def integrate_kolmogorov_nagumo(qs, l, N, maxit=256, tol=1e-4, trace=None, allreduce=None):
     """Kolmogorov-Nagumo integration, core/stage/@x@_integrate_kolmogorov_nagumo.c:153-266.
 
     Returns (Qbar, iterations, error) with the reference's retv conventions:
-    iterations = maxit + 1 when maxit is hit (:238-241)."""
+    iterations = maxit + 1 when maxit is hit (:238-241).  With ``allreduce`` (an in-place sum over
+    the ranks of a float64 array) ``qs`` holds this rank's rows and Bc, Bgc are summed where the
+    reference calls MPI_Allreduce (:160, :178)."""
+    ar = allreduce or _local
     qs = np.asarray(qs, np.float64)
     qc = qs[:, :l].copy()                                     # :154
-    bc = qs.T @ qc                                            # :157
+    bc = ar(qs.T @ qc)                                        # :157-160
     it = 1
     err = -np.inf
     while True:
         gc = qs @ bc / N                                      # :174
-        bgc = qs.T @ gc                                       # :177
+        bgc = ar(qs.T @ gc)                                   # :177-178
         dc = bc.T @ bc / N                                    # :181
         z = bc.T @ bgc / N                                    # :184 (upper used)
         z = _sym_upper(z - dc @ dc)                           # :190 syrk 'U'
@@ -100,19 +107,22 @@ def integrate_kolmogorov_nagumo(qs, l, N, maxit=256, tol=1e-4, trace=None):
 
 
 def integrate_wen_yin(qs, l, N, maxit=256, tol=1e-3, tau0=1.0, taumax=1e14, taumin=1e-14, taumaxit=20,
-                      beta=0.5, sigma=1e-4, eta=0.85):
+                      beta=0.5, sigma=1e-4, eta=0.85, allreduce=None):
     """Wen-Yin integration, core/stage/@x@_integrate_wen_yin.c:197-360.
 
     Returns (Qbar, iterations, mu).  The 2l x 2l inverse of the line-search
     matrix C (:262) is taken with numpy.linalg.inv (LU with partial pivoting,
-    the same factorization as the reference's getrf+getri)."""
+    the same factorization as the reference's getrf+getri).  With ``allreduce`` ``qs`` holds this
+    rank's rows and Bc, Bgc and the two step-size sums are summed over the ranks where the
+    reference calls MPI_Allreduce (:206, :216, :303, :345)."""
+    ar = allreduce or _local
     qs = np.asarray(qs, np.float64)
     I = np.eye(l)
     qc = qs[:, :l].copy()                                     # :200
-    bc = qs.T @ qc                                            # :203
+    bc = ar(qs.T @ qc)                                        # :203-206
     dc = bc.T @ bc / N                                        # :209
     gc = qs @ bc / N                                          # :212
-    bgc = qs.T @ gc                                           # :215
+    bgc = ar(qs.T @ gc)                                       # :215-216
     dgc = bc.T @ bgc / N                                      # :219
     xc = gc - qc @ dc                                         # :222-223
     mu = np.trace(dgc) - np.sum(dc * dc)                      # :226
@@ -141,7 +151,7 @@ def integrate_wen_yin(qs, l, N, maxit=256, tol=1e-3, tau0=1.0, taumax=1e14, taum
         qp = qc @ fc + gc @ fgc                               # :292-293
         dc = bp.T @ bp / N                                    # :296
         gc = qs @ bp / N                                      # :299
-        bgc = qs.T @ gc                                       # :302
+        bgc = ar(qs.T @ gc)                                   # :302-303
         dgc = bp.T @ bgc / N                                  # :306
         mu = np.trace(dgc) - np.sum(dc * dc)                  # :309
         if mu < tol * tol:                                    # :314
@@ -152,10 +162,11 @@ def integrate_wen_yin(qs, l, N, maxit=256, tol=1e-3, tau0=1.0, taumax=1e14, taum
         xp = gc - qp @ dc                                     # :327-328
         d1, d2 = qc - qp, xc - xp                             # :331-332
         if it % 2:
-            t0, t1 = np.sum(d1 * d1), np.sum(d1 * d2)         # :336-338
+            t = np.array([np.sum(d1 * d1), np.sum(d1 * d2)])  # :336-338
         else:
-            t0, t1 = np.sum(d2 * d1), np.sum(d2 * d2)         # :339-341
-        taug = min(max(abs(t0 / t1), taumin), taumax)         # :344-347
+            t = np.array([np.sum(d2 * d1), np.sum(d2 * d2)])  # :339-341
+        t0, t1 = ar(t)                                        # :345
+        taug = min(max(abs(t0 / t1), taumin), taumax)         # :347-349
         qc, xc, bc = qp, xp, bp                               # :352-354
         it += 1
     return qp, it, float(mu)
@@ -246,16 +257,17 @@ def row_block(m, P, rank):
     return min(rank * each, m), min(rank * each + each, m)
 
 
-def isvd_row_block(a_rows, omega, k, p, N, allreduce, maxit=256, tol=1e-4):
-    """The Gramian / KN / Gramian driver on one rank's rows of a row-distributed A (dista 'R'),
-    with every reduction over the ranks done by ``allreduce(x)`` (an in-place sum of a float64
-    array, the reference's MPI_Allreduce with MPI_SUM):
+def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None):
+    """The Gramian / KN-or-WY / Gramian driver on one rank's rows of a row-distributed A
+    (dista 'R'), with every reduction over the ranks done by ``allreduce(x)`` (an in-place sum of a
+    float64 array, the reference's MPI_Allreduce with MPI_SUM):
       * orthogonalization W_i = sum_ranks Y_i' Y_i, core/stage/@x@_orthogonalize_gramian.c:82-85;
-      * KN B_c = Qs' Q_c and Qs' G_c, core/stage/@x@_integrate_kolmogorov_nagumo.c:157-160, 176-178;
+      * integration as the reference's integrate stages with ``allreduce`` (Bc, Bgc and, for WY,
+        the step-size sums);
       * postprocessing Z = A' Qbar (projectBlockRow, core/stage/@x@_postprocess.h:96-162, whose
         MPI_Reduce_scatter_block leaves each rank its column block of the sum; here every rank keeps
         the whole sum) and W = Z' Z (core/stage/@x@_postprocess_gramian.c:145-146).
-    Returns (s, U rows of this rank, V (all n rows), iterations, error)."""
+    Returns (s, U rows of this rank, V (all n rows), iterations, error or mu)."""
     a_rows = np.asarray(a_rows, np.float64)
     l = k + p
     y = a_rows @ np.asarray(omega, np.float64)
@@ -265,30 +277,11 @@ def isvd_row_block(a_rows, omega, k, p, N, allreduce, maxit=256, tol=1e-4):
         w = allreduce(yi.T @ yi)
         u, s, _ = np.linalg.svd(w)
         q[:, i * l:(i + 1) * l] = yi @ (u / np.sqrt(s))
-    qc = q[:, :l].copy()
-    bc = allreduce(q.T @ qc)
-    it = 1
-    while True:
-        gc = q @ bc / N
-        bgc = allreduce(q.T @ gc)
-        dc = bc.T @ bc / N
-        z = _sym_upper(bc.T @ bgc / N - dc @ dc)
-        lam, vec = np.linalg.eigh(z, UPLO="U")
-        sv = np.sqrt(0.5 + np.sqrt(0.25 - lam))
-        ss = np.sqrt(sv)
-        c = (vec * ss) @ (vec * ss).T
-        cinv = (vec / ss) @ (vec / ss).T
-        fc = c - dc @ cinv
-        qp = qc @ fc + gc @ cinv
-        bp = bc @ fc + bgc @ cinv
-        err = float(np.linalg.norm(sv - 1.0))
-        if err <= tol:
-            break
-        if it == maxit:
-            it += 1
-            break
-        qc, bc = qp, bp
-        it += 1
+    argv_i = dict(argv_i or {})
+    if alg_i == "KN":
+        qp, it, err = integrate_kolmogorov_nagumo(q, l, N, allreduce=allreduce, **argv_i)
+    else:
+        qp, it, err = integrate_wen_yin(q, l, N, allreduce=allreduce, **argv_i)
     z = allreduce(a_rows.T @ qp)
     w, s, _ = np.linalg.svd(z.T @ z)
     sig = np.sqrt(s)
