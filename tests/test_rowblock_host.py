@@ -1,8 +1,8 @@
 """Row blocks over several ranks, host side (no GPU): isvd_createParam splits rows and columns
 like the reference's core/param.c:47-55 once isvd_gpu_set_allreduce joins P ranks, and the
-exchange algebra -- every reduction the library hands to the caller's AllReduce, run through
-capi.torch_host_allreduce over gloo with world_size 2 -- reproduces the one-rank solve, for KN and
-WY integration."""
+reference's row-block exchange algebra -- the oracle's row-block driver with each of the
+reference's MPI_Allreduce calls run through the library's capi.torch_host_allreduce callback over
+gloo with world_size 2 -- reproduces the one-rank solve, for KN and WY integration."""
 import ctypes
 import datetime
 import multiprocessing as mp
