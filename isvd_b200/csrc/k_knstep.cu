@@ -34,8 +34,10 @@ namespace {
 
 constexpr int kKsThreads = 1024;  // one output of a 32 x 32 tile per thread
 constexpr int kKsMaxL = 160;
-constexpr int kAld = kKsMaxL + 1;  // shared-memory row stride of the A tile (32 x l)
-constexpr int kBld = 34;           // shared-memory row stride of the B tile (l x 32; even: 16-byte pairs)
+// shared-memory row strides of the A tile (32 x l) and the B tile (l x 32), both 4 (mod 16) doubles:
+// the mma.sync fragment reads (8 rows x 4 inner indices, or 4 x 8) hit 16 distinct bank pairs
+constexpr int kAld = kKsMaxL + 4;
+constexpr int kBld = 36;
 constexpr int kKsPer = (32 * kKsMaxL + kKsThreads - 1) / kKsThreads;
 
 struct Ks {
@@ -46,17 +48,18 @@ struct Ks {
 // C = alpha A B + beta Cin + diag I on the 32 x 32 output tiles [tile_begin, tile_end) of a phase
 // (tiles numbered across the products of the phase); CTA r takes the tiles t = r mod cs.
 // Row-major l x l operands; every load goes through L2 (__ldcg), as they are written by other CTAs.
-// Inner loop: four quarters of the inner dimension x 256 threads, each with a 2 x 2 output block
-// (three shared-memory loads per four FMAs); the quarters' partial sums meet in shared memory and
-// are added in a fixed order.
+// Tile product on the FP64 tensor-core path (mma.sync m8n8k4 f64): 16 tiles of 8 x 8, two warps
+// per tile (halves of the inner dimension, zero-padded to a multiple of 4); the halves' partial
+// sums meet in shared memory and are added in a fixed order.
 // C2, C3 (optional) receive copies of C.
 __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, const double *A, const double *B,
                       double beta, const double *Cin, double diag, double *C, double *C2 = nullptr,
                       double *C3 = nullptr) {
   const int l = k.l, tid = threadIdx.x;
-  const int ty = tid >> 5, tx = tid & 31;                    // output (ty, tx) of the tile in the epilogue
-  const int qk = tid >> 8, bi = (tid & 255) >> 4, bj = tid & 15;  // quarter, 2 x 2 block of the inner loop
-  const int kq = (l + 3) >> 2, kb = qk * kq, ke = min(l, kb + kq);
+  const int ty = tid >> 5, tx = tid & 31;  // output (ty, tx) of the tile in the epilogue
+  const int lane = tid & 31, half = ty >> 4, mt = ty & 15, ti = mt >> 2, tj = mt & 3;  // warp: 8 x 8 tile, half
+  const int l4 = (l + 3) & ~3, kh = ((l4 >> 1) + 3) & ~3;
+  const int kb = half * kh, ke = min(l4, kb + kh);
   const int first = tile_begin + (((k.rank - tile_begin) % k.cs) + k.cs) % k.cs;
   for (int t = first; t < tile_end; t += k.cs) {
     const int tt = t - tile_begin;
@@ -82,26 +85,28 @@ __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, c
         k.Bs[(e >> 5) * kBld + (e & 31)] = rb[u];
       }
     }
-    __syncthreads();
-    double c00 = 0.0, c01 = 0.0, c10 = 0.0, c11 = 0.0;
-    const double *a0 = k.As + (2 * bi) * kAld, *a1 = a0 + kAld;
-    const double *bp = k.Bs + 2 * bj;
-    for (int kk = kb; kk < ke; ++kk) {
-      const double x0 = a0[kk], x1 = a1[kk];
-      const double2 y = *reinterpret_cast<const double2 *>(bp + kk * kBld);
-      c00 = fma(x0, y.x, c00);
-      c01 = fma(x0, y.y, c01);
-      c10 = fma(x1, y.x, c10);
-      c11 = fma(x1, y.y, c11);
+    for (int e = tid; e < 32 * 4; e += kKsThreads) {  // zero the inner-dimension padding [l, l4)
+      const int r = e >> 2, kk = l + (e & 3);
+      if (kk < l4) {
+        k.As[r * kAld + kk] = 0.0;
+        k.Bs[kk * kBld + r] = 0.0;
+      }
     }
-    double *part = k.part + qk * 1024;  // 32 x 32 partial sums of this quarter
-    part[(2 * bi) * 32 + 2 * bj] = c00;
-    part[(2 * bi) * 32 + 2 * bj + 1] = c01;
-    part[(2 * bi + 1) * 32 + 2 * bj] = c10;
-    part[(2 * bi + 1) * 32 + 2 * bj + 1] = c11;
+    __syncthreads();
+    double d[2] = {0.0, 0.0};
+    const double *ap = k.As + (ti * 8 + (lane >> 2)) * kAld + (lane & 3);
+    const double *bq = k.Bs + (lane & 3) * kBld + tj * 8 + (lane >> 2);
+    for (int kk = kb; kk < ke; kk += 4)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                   : "+d"(d[0]), "+d"(d[1])
+                   : "d"(ap[kk]), "d"(bq[kk * kBld]));
+    double *part = k.part + half * 1024;  // 32 x 32 partial sums of this half
+    const int orow = ti * 8 + (lane >> 2), ocol = tj * 8 + 2 * (lane & 3);
+    part[orow * 32 + ocol] = d[0];
+    part[orow * 32 + ocol + 1] = d[1];
     __syncthreads();
     const int o = ty * 32 + tx;
-    const double acc = (k.part[o] + k.part[1024 + o]) + (k.part[2048 + o] + k.part[3072 + o]);
+    const double acc = k.part[o] + k.part[1024 + o];
     if (i < l && j < l) {
       const double v = alpha * acc + beta * cin + (i == j ? diag : 0.0);
       C[(size_t)i * l + j] = v;
@@ -192,7 +197,7 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
   const int l = a.l;
   const size_t ll = (size_t)l * l;
   Ks k{l, (l + 31) / 32, (int)cluster.num_blocks(), (int)cluster.block_rank(), sm, sm + 32 * kAld,
-         sm + 32 * kAld + kKsMaxL * kBld};
+         sm + 32 * kAld + (kKsMaxL + 4) * kBld};
   const int nt = k.nr * k.nr;
   const int gtid = k.rank * kKsThreads + threadIdx.x, gstride = k.cs * kKsThreads;
   // work: Z | P_1..P_8 | accC x2 | accCi x2 | BC_0..BC_7 | BI_0..BI_7 (Newton-Schulz: P_1..P_5), then
@@ -356,7 +361,7 @@ KnSeries make_series() {
   return s;
 }
 
-constexpr size_t kKsSmem = (size_t)(32 * kAld + kKsMaxL * kBld + 4 * 1024) * sizeof(double);
+constexpr size_t kKsSmem = (size_t)(32 * kAld + (kKsMaxL + 4) * kBld + 4 * 1024) * sizeof(double);
 int g_cluster_size = -1;  // -1: not decided yet; 0: no cluster launch possible
 
 int choose_cluster_size(const KnStep &a, cudaStream_t st) {
