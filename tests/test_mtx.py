@@ -153,3 +153,23 @@ def test_omp_queries(lib):
     for name, want in (("isvd_getOmpMaxSize", 1), ("isvd_getOmpSize", 1), ("isvd_getOmpRank", 0)):
         getattr(L, name).restype = ctypes.c_int
         assert getattr(L, name)() == want
+
+
+@pytest.mark.parametrize("ilp64", [False, True])
+def test_headers_compile_as_cpp_and_mmio_writers_round_trip(tmp_path, lib, lib64, ilp64):
+    """include/ compiles as C++17 (both index widths) and links with the matching library; the
+    mmio writers' banner and size read back through the mmio readers and isvd_dFget."""
+    L = lib64 if ilp64 else lib
+    exe = str(tmp_path / "header_check")
+    libdir = os.path.dirname(L.path)
+    name = "isvd_gpu_b200_64" if ilp64 else "isvd_gpu_b200"
+    cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"), "-I",
+           os.path.join(REPO, "include", "mpi_shim"), "-I", os.path.join(REPO, "include", "mmio_shim"),
+           os.path.join(REPO, "tests", "c", "header_check.cpp"), "-o", exe, "-L" + libdir, "-l" + name,
+           "-Wl,-rpath," + libdir]
+    if ilp64:
+        cmd.insert(1, "-DISVD_USE_ILP64")
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    out = subprocess.run([exe, str(tmp_path / "w.mtx")], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
+    assert out.stdout.strip() == "sum 18.0 dim_sketch 6 omp 1 error 0"
