@@ -233,12 +233,17 @@ void isvd_gpu_set_allreduce( isvd_gpu_allreduce_fn fn, void *user, int nranks, i
  *     doubles) per device.  Sizes that do not fit -- (N l)^2 + 5 N l^2 + 13 l^2 + 96 doubles, each
  *     term rounded up to 32 -- or l > 160 are rejected with ISVD_GPU_ERROR_ARGUMENT and a message
  *     (N l = 512 with l = 64 fits; N l = 1024 does not).
+ *   - one rank only: with ranks joined by isvd_gpu_set_allreduce, or param.mpi_size != 1, it returns
+ *     ISVD_GPU_ERROR_UNSUPPORTED (it never sums the Gram over ranks);
+ *   - the call is synchronous: it reads the iteration error back on the host after every iteration
+ *     and returns only once all of its work on `stream` has completed.
  * The first call on each device sets up: it looks up the array's address (which loads the device
- * code that holds it) and reads the SM count; make that first call before any stream capture on
- * the device.  Nothing in the array has to be zero on entry: each call clears its own status and
- * barrier words.  The array is shared by all calls on a device, so overlapping calls would race
- * on it; each call holds the library's process-wide lock until its work has completed, which makes
- * calls from several threads or streams run one after another.
+ * code that holds it), reads the SM count and resolves every kernel the entry point can launch, so
+ * that with lazy module loading no later call, whatever its shape, loads code; make that first call
+ * before any stream capture on the device.  Nothing in the array has to be zero on entry: each call
+ * clears its own status and barrier words.  The array is shared by all calls on a device, so
+ * overlapping calls would race on it; each call holds the library's process-wide lock until its
+ * work has completed, which makes calls from several threads or streams run one after another.
  * Returns an ISVD_GPU_* status. */
 int isvd_dIntegrateKolmogorovNagumo_noalloc(
     const isvd_Param param, const isvd_d_val_t *argv, const isvd_int_t argc, isvd_d_val_t *retv,

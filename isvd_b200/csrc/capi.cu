@@ -1024,6 +1024,11 @@ int isvd_dIntegrateKolmogorovNagumo_noalloc(const isvd_Param param, const isvd_d
       query_kn(retv, retc);
       return;
     }
+    // one rank only: this variant never sums G = Qs'Qs over the ranks joined by
+    // isvd_gpu_set_allreduce, so each rank would iterate on its own partial Gram
+    if (param.mpi_size != 1 || collective().nranks > 1)
+      fail(kErrUnsupported, "Kolmogorov-Nagumo on static scratch: one rank only (MPI size %d, %d joined ranks)",
+           (int)param.mpi_size, collective().nranks);
     require_single_rank(param);
     const int m = param.nrow_proc, l = param.dim_sketch, N = param.num_sketch, Nl = param.dim_sketch_total;
     REQUIRE(ldyst >= Nl);

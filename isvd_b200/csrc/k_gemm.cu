@@ -295,6 +295,22 @@ void gemm_fixed(const Gemm<T, Tout> &g, int num_sms, T *partial, size_t cap, cud
 
 template void gemm_fixed<double, double>(const Gemm<double, double> &, int, double *, size_t, cudaStream_t);
 
+void gemm_fixed_preload() {
+  cudaFuncAttributes fa;
+#define ISVD_PRELOAD(BM_, BN_, AK, BNC)                                                         \
+  CK(cudaFuncGetAttributes(&fa, gemm_kernel<double, double, BM_, BN_, 16, AK, BNC>));
+  ISVD_PRELOAD(64, 64, true, true)
+  ISVD_PRELOAD(64, 64, true, false)
+  ISVD_PRELOAD(64, 64, false, true)
+  ISVD_PRELOAD(64, 64, false, false)
+  ISVD_PRELOAD(128, 128, true, true)
+  ISVD_PRELOAD(128, 128, true, false)
+  ISVD_PRELOAD(128, 128, false, true)
+  ISVD_PRELOAD(128, 128, false, false)
+#undef ISVD_PRELOAD
+  CK(cudaFuncGetAttributes(&fa, splitk_reduce_kernel<double, double>));
+}
+
 template void gemm<double, double>(const Gemm<double, double> &, cudaStream_t);
 template void gemm<float, float>(const Gemm<float, float> &, cudaStream_t);
 template void gemm<float, double>(const Gemm<float, double> &, cudaStream_t);

@@ -953,6 +953,11 @@ void svd_jacobi_batched(int n, int batch, const double *B, double *U, double *s,
   KLAUNCHED();
 }
 
+void kn_step_fixed_preload() {
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, kn_step_kernel));
+}
+
 void kn_step_fixed(const KnStep &a, int num_sms, cudaStream_t st) {
   if (a.l > 160) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > 160", a.l);
   const int nr = (a.l + 15) / 16;

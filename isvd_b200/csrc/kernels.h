@@ -162,5 +162,11 @@ void recip_affine(const double *lam, int n, double num, double half, double add,
 template <class T, class Tout>
 void gemm_fixed(const Gemm<T, Tout> &g, int num_sms, T *partial, size_t cap, cudaStream_t st);
 void kn_step_fixed(const KnStep &a, int num_sms, cudaStream_t st);
+// Resolve every kernel that gemm_fixed<double, double> / kn_step_fixed can launch (all operand
+// layouts and tile sizes, the split-K reduction, the cooperative step) on the current device, so
+// that with lazy module loading no later launch is the first use of a kernel (which loads code and
+// may allocate device memory).  Throws on a CUDA error.
+void gemm_fixed_preload();
+void kn_step_fixed_preload();
 
 }  // namespace isvdb

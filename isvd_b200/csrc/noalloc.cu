@@ -51,8 +51,14 @@ struct ScratchSlot {
 std::mutex g_slot_mu;
 ScratchSlot g_slot[kMaxDevices];
 
+__global__ void kn_start_kernel(const double *__restrict__ G, int Nl, int l, double *__restrict__ Bc,
+                                double *__restrict__ Mc);
+
 // First use on a device (that device current): the array's address (looking it up loads the
-// module that holds it, when modules load lazily) and the SM count.  Later calls reuse both.
+// module that holds it, when modules load lazily), the SM count, and every kernel this entry point
+// can launch resolved once, so that with lazy module loading no later call (another shape, another
+// tile size, split-K) is the first launch of a kernel, which would load code and could allocate.
+// Later calls reuse all of it.
 ScratchSlot slot_for_current_device(int dev) {
   if (dev < 0 || dev >= kMaxDevices) fail(kErrUnsupported, "static scratch: device ordinal %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_slot_mu);
@@ -64,6 +70,10 @@ ScratchSlot slot_for_current_device(int dev) {
       fail(kErrCuda, "static scratch: cudaGetSymbolAddress failed on device %d: %s", dev, cudaGetErrorString(e));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, kn_start_kernel));
+    gemm_fixed_preload();
+    kn_step_fixed_preload();
     s.sms = sms;
     s.base = static_cast<double *>(p);
   }

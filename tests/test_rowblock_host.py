@@ -111,3 +111,31 @@ def test_exchange_algebra_over_gloo(oracle, alg):
         assert np.abs(sr - whole["s"]).max() <= 1e-12 * whole["s"].max()
         assert oracle.column_angles(vr, whole["v"]).max() < 1e-10
     assert oracle.column_angles(u, whole["u"]).max() < 1e-10
+
+
+def test_noalloc_kn_refuses_joined_ranks(lib):
+    """The static-scratch Kolmogorov-Nagumo entry point runs on one rank only: it never sums the
+    Gram over ranks, so with ranks joined through isvd_gpu_set_allreduce (or an isvd_Param whose MPI
+    size is not 1) it returns ISVD_GPU_ERROR_UNSUPPORTED before touching any operand or device."""
+    from isvd_b200.capi import Param, c_int_t
+    fn = lib.lib.isvd_dIntegrateKolmogorovNagumo_noalloc
+    fn.argtypes = [Param, ctypes.c_void_p, c_int_t, ctypes.c_void_p, c_int_t, ctypes.c_void_p, c_int_t,
+                   ctypes.c_void_p, c_int_t, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    unsupported = 6  # ISVD_GPU_ERROR_UNSUPPORTED
+    noop = lambda buf, count, dtype, stream, user: None  # noqa: E731
+    try:
+        lib.set_allreduce(noop, 2, 1)
+        prm = lib.create_param(1000, 1000, 8, 4, 4)
+        assert prm.mpi_size == 2
+        lib.clear_error()
+        assert fn(prm, None, 0, None, 0, None, 48, None, 12, None) == unsupported
+        code, msg = lib.last_error()
+        assert code == unsupported and "one rank only" in msg
+    finally:
+        lib.set_allreduce(None, 1, 0)
+    prm = lib.create_param(1000, 1000, 8, 4, 4)
+    prm.mpi_size = 2
+    lib.clear_error()
+    assert fn(prm, None, 0, None, 0, None, 48, None, 12, None) == unsupported
+    assert lib.last_error()[0] == unsupported

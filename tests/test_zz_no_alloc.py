@@ -6,10 +6,14 @@ other test of the suite; the first test makes the first library call when the fi
 in a fresh process, which is when the per-device set-up of the scratch happens.
 """
 import ctypes
+import json
+import subprocess
+import sys
 
 import numpy as np
 import pytest
 
+from conftest import REPO
 from isvd_b200.capi import Param, c_int_t
 
 pytestmark = pytest.mark.gpu
@@ -128,3 +132,75 @@ def test_noalloc_rejects(lib):
     r0 = lib.integrate("d", "KN", prm, ys_h, N * l, qt_h, l, argv=[256, 1e-4])
     assert int(r[0]) == int(r0[0])
     assert np.abs(qt.cpu().numpy() - qt_h).max() < TOL
+
+
+# Run in a fresh process (a fresh CUDA context, no earlier library call): the first call has a
+# small shape (64 x 64 product tiles, no split-K), the second a larger one (128 x 128 tiles and a
+# split-K reduction for the l x l products), so the second call is the first to need those
+# kernels.  Free device memory must not move across the second and third calls.
+_FRESH = r"""
+import ctypes, json, sys
+import numpy as np
+import torch
+sys.path.insert(0, sys.argv[1])
+import isvd_b200
+from isvd_b200.capi import Param, c_int_t
+lib = isvd_b200.load()
+fn = lib.lib.isvd_dIntegrateKolmogorovNagumo_noalloc
+fn.argtypes = [Param, ctypes.c_void_p, c_int_t, ctypes.c_void_p, c_int_t, ctypes.c_void_p, c_int_t,
+               ctypes.c_void_p, c_int_t, ctypes.c_void_p]
+fn.restype = ctypes.c_int
+
+def blocks(seed, m, l, N):
+    rng = np.random.default_rng(seed)
+    base = np.linalg.qr(rng.standard_normal((m, l)))[0]
+    return np.concatenate([np.linalg.qr(base + 0.5 / np.sqrt(m) * rng.standard_normal((m, l)))[0]
+                           for _ in range(N)], axis=1)
+
+shapes = [(120, 32, 3), (60000, 128, 4)]
+cases = []
+for i, (m, l, N) in enumerate(shapes):
+    ys = torch.from_numpy(blocks(7 + i, m, l, N)).cuda()
+    qs = [torch.full((m, l), float("nan"), dtype=torch.float64, device="cuda") for _ in range(2)]
+    cases.append((lib.create_param(m, m, l, 0, N), ys, qs, m, l, N))
+argv = np.asarray([256, 1e-4])
+stream = torch.cuda.current_stream().cuda_stream
+torch.cuda.synchronize()
+out = {"status": [], "free": [], "iters": []}
+
+def call(c, j):
+    prm, ys, qs, m, l, N = c
+    rv = np.zeros(2)
+    st = fn(prm, argv.ctypes.data, 2, rv.ctypes.data, 2, ys.data_ptr(), N * l, qs[j].data_ptr(), l, stream)
+    out["status"].append(int(st))
+    out["iters"].append(int(rv[0]))
+    out["free"].append(int(torch.cuda.mem_get_info()[0]))
+
+call(cases[0], 0)
+call(cases[1], 0)
+call(cases[1], 1)
+# the ordinary stage on the same operands (it allocates; only after the checks above)
+out["diff"] = []
+out["iters_stage"] = []
+for prm, ys, qs, m, l, N in cases:
+    q0 = torch.zeros((m, l), dtype=torch.float64, device="cuda")
+    r0 = lib.integrate("d", "KN", prm, ys, N * l, q0, l, argv=[256, 1e-4])
+    out["iters_stage"].append(int(r0[0]))
+    out["diff"].append(max(float((q - q0).abs().max().item()) for q in qs if not torch.isnan(q).any()))
+print(json.dumps(out))
+"""
+
+
+def test_noalloc_fresh_process_shapes():
+    """In a fresh process: a small call, then two calls of a larger shape that needs other kernel
+    variants (tile size, split-K); free device memory is the same before and after the larger calls,
+    every call succeeds, and the results equal the ordinary stage's within TOL with the same
+    iteration counts."""
+    r = subprocess.run([sys.executable, "-c", _FRESH, REPO], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["status"] == [OK, OK, OK]
+    assert out["free"][1] == out["free"][0] and out["free"][2] == out["free"][0], out["free"]
+    assert out["iters"][0] == out["iters_stage"][0] > 1
+    assert out["iters"][1] == out["iters"][2] == out["iters_stage"][1] > 1
+    assert max(out["diff"]) < TOL, out["diff"]
