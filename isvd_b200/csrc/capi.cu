@@ -115,7 +115,46 @@ const char *arg2str(const char *name, const char *arg, const char *const *opts, 
   arg_error("%s.\n", msg.c_str());
 }
 
+#if !defined(ISVD_MPI_SHIM)
+// Built against a real MPI (isvd_b200/build.py --mpi-include): the ranks of the communicator in
+// isvd_Param join as row blocks without isvd_gpu_set_allreduce, each exchange an in-place
+// MPI_Allreduce (MPI_SUM) on the library's pinned host staging buffer, as the reference's stages
+// reduce on that communicator.  A reduction installed by the program takes precedence.
+MPI_Comm g_param_comm;
+
+void mpi_param_allreduce(void *buf, size_t count, int dtype, void *stream, void *user) {
+  (void)stream; (void)user;
+  const size_t esz = dtype == ISVD_GPU_DTYPE_F64 ? sizeof(double) : sizeof(float);
+  const size_t chunk = (size_t)1 << 30;  // MPI counts are int
+  for (size_t off = 0; off < count; off += chunk) {
+    const int n = (int)std::min(chunk, count - off);
+    if (MPI_Allreduce(MPI_IN_PLACE, static_cast<char *>(buf) + off * esz, n,
+                      dtype == ISVD_GPU_DTYPE_F64 ? MPI_DOUBLE : MPI_FLOAT, MPI_SUM, g_param_comm) != MPI_SUCCESS)
+      fail(kErrUnsupported, "MPI_Allreduce failed on the communicator of isvd_Param");
+  }
+}
+
+void join_param_comm(const isvd_Param &p) {
+  Collective &c = collective();
+  if (c.fn && !c.from_comm) return;  // the program's own reduction
+  if (p.mpi_size > 1) {
+    g_param_comm = p.mpi_comm;
+    c.fn = mpi_param_allreduce;
+    c.user = nullptr;
+    c.nranks = p.mpi_size;
+    c.rank = p.mpi_rank;
+    c.on_device = 0;
+    c.from_comm = true;
+  } else if (c.from_comm) {
+    c = Collective();
+  }
+}
+#endif
+
 void require_single_rank(const isvd_Param &p) {
+#if !defined(ISVD_MPI_SHIM)
+  join_param_comm(p);
+#endif
   // several ranks: only through the caller's AllReduce (isvd_gpu_set_allreduce), row blocks
   const Collective &cl = collective();
   if (p.mpi_size != 1 && !(cl.nranks == p.mpi_size && cl.rank == p.mpi_rank))
@@ -780,13 +819,14 @@ int isvd_gpu_profile_get(const char *tag, double *ms, unsigned long long *launch
 
 // ---------------------------------------------------------------- utilities
 mpi_int_t isvd_getMpiSize(const isvd_MpiComm comm) {
-  if (collective().nranks > 1) return collective().nranks;  // ranks joined by isvd_gpu_set_allreduce
+  // ranks joined by isvd_gpu_set_allreduce (a join from a communicator defers to that communicator)
+  if (collective().nranks > 1 && !collective().from_comm) return collective().nranks;
   int s = 0;
   MPI_Comm_size(comm, &s);
   return s;
 }
 mpi_int_t isvd_getMpiRank(const isvd_MpiComm comm) {
-  if (collective().nranks > 1) return collective().rank;
+  if (collective().nranks > 1 && !collective().from_comm) return collective().rank;
   int r = 0;
   MPI_Comm_rank(comm, &r);
   return r;
@@ -804,6 +844,7 @@ void isvd_gpu_set_allreduce(isvd_gpu_allreduce_fn fn, void *user, int nranks, in
     c.nranks = nranks;
     c.rank = rank;
     c.on_device = on_device ? 1 : 0;
+    c.from_comm = false;
   });
 }
 

@@ -31,19 +31,30 @@ __device__ double block_sum(double v, double *red) {
 // A pivot that is not above piv_rel times its starting diagonal value (or is not finite) stops
 // the CTA and sets *status = kStatusNotPD.  Output: X with zeros below the diagonal (kCholFactor)
 // or out_scale X X' = out_scale A^-1 (kCholInverse).
+// null_mask (kCholFactor only; n ints per matrix): a finite pivot at or below the threshold marks
+// its column as numerically dependent on the ones before it instead of failing -- the column's row
+// of R becomes e_k' (its Schur complement row is zero to rounding) and column k of X is zeroed, so
+// Y X has an exact zero column there and the later columns are orthogonalized against the others
+// only.  Each newly marked column adds 1 to *null_count.
+// perm (n ints per matrix): factor P A P' instead (row / column i of the factored matrix is
+// row / column perm[i] of A) and store X at the original positions, out[perm[i], perm[j]] = X[i, j].
 __global__ void __launch_bounds__(kCholThreads)
     chol_inv_kernel(int n, const double *__restrict__ W, double alpha, double shift_abs, double shift_rel,
-                    double piv_rel, double *__restrict__ out, double out_scale, int mode, int *status) {
+                    double piv_rel, double *__restrict__ out, double out_scale, int mode, int *status,
+                    int *__restrict__ null_mask, int *__restrict__ null_count, const int *__restrict__ perm) {
   extern __shared__ double sm[];
   __shared__ double red[kCholThreads / 32];
   const int ld = n + 1, tid = threadIdx.x, nt = blockDim.x;
   double *R = sm;                       // n x ld
   double *aux = sm + (size_t)n * ld;    // n: starting diagonal, then the column being inverted
   const double *w = W + (size_t)blockIdx.x * n * n;
+  const int *pm = perm ? perm + (size_t)blockIdx.x * n : nullptr;
+  int *mask = null_mask ? null_mask + (size_t)blockIdx.x * n : nullptr;
   double tr = 0.0;
   for (int e = tid; e < n * n; e += nt) {
     const int i = e / n, j = e - i * n;
-    const double v = alpha * ((i <= j) ? w[(size_t)i * n + j] : w[(size_t)j * n + i]);
+    const int pi = pm ? pm[i] : i, pj = pm ? pm[j] : j;
+    const double v = alpha * ((pi <= pj) ? w[(size_t)pi * n + pj] : w[(size_t)pj * n + pi]);
     R[i * ld + j] = v;
     if (i == j) tr += v;
   }
@@ -56,6 +67,19 @@ __global__ void __launch_bounds__(kCholThreads)
   for (int k = 0; k < n; ++k) {
     const double d = R[k * ld + k];
     if (!(d > piv_rel * aux[k]) || !(d > 0.0) || !(d < INFINITY)) {  // same decision in every thread
+      if (mask && d == d && d < INFINITY) {  // a dependent column: null, not a failure
+        __syncthreads();
+        if (tid == 0) {
+          R[k * ld + k] = 1.0;
+          if (!mask[k]) {
+            mask[k] = 1;
+            atomicAdd(null_count, 1);
+          }
+        }
+        for (int j = k + 1 + tid; j < n; j += nt) R[k * ld + j] = 0.0;
+        __syncthreads();
+        continue;  // row k of R is e_k': the Schur update it would make is zero
+      }
       if (tid == 0) atomicExch(status, kStatusNotPD);
       return;
     }
@@ -93,7 +117,9 @@ __global__ void __launch_bounds__(kCholThreads)
   if (mode == kCholFactor) {
     for (int e = tid; e < n * n; e += nt) {
       const int i = e / n, j = e - i * n;
-      o[e] = (j >= i) ? out_scale * R[i * ld + j] : 0.0;
+      const double v = (j >= i && !(mask && mask[j])) ? out_scale * R[i * ld + j] : 0.0;
+      if (pm) o[(size_t)pm[i] * n + pm[j]] = v;
+      else o[e] = v;
     }
   } else {
     for (int e = tid; e < n * n; e += nt) {
@@ -260,8 +286,11 @@ size_t chol_smem(int n) { return ((size_t)n * (n + 1) + n) * sizeof(double); }
 }  // namespace
 
 void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
-                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st) {
+                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st,
+                      int *null_mask, int *null_count, const int *perm) {
   if (n <= 0 || batch <= 0) return;
+  if ((null_mask || perm) && mode != kCholFactor) fail(kErrArgument, "Cholesky: null columns / permutation need kCholFactor");
+  if (null_mask && !null_count) fail(kErrArgument, "Cholesky: a null-column mask needs its counter");
   if (mode == kCholInverse && shift_rel == 0.0) {  // the full inverse: sweep operator, fewer dependent steps
     const size_t smem = ((size_t)n * (n + 1) + 2 * n) * sizeof(double);
     if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "SPD inverse: l = %d exceeds on-chip capacity", n);
@@ -274,7 +303,7 @@ void chol_inv_batched(int n, int batch, const double *W, double alpha, double sh
   if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "Cholesky: l = %d exceeds on-chip capacity", n);
   CK(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   chol_inv_kernel<<<batch, kCholThreads, smem, st>>>(n, W, alpha, shift_abs, shift_rel, piv_rel, out, out_scale,
-                                                     mode, status);
+                                                     mode, status, null_mask, null_count, perm);
   KLAUNCHED();
 }
 

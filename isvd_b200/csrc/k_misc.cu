@@ -114,7 +114,57 @@ __global__ void scale_cols_kernel(const Ts *__restrict__ src, long long lds, Td 
   }
 }
 
+// Null columns of a TS factorization get values uniform in [-1/2, 1/2): one Philox block per
+// element, counter (row, column), key seed.
+template <class T>
+__global__ void fill_null_columns_kernel(T *__restrict__ y, long long ld, long long rows, int cols,
+                                         const int *__restrict__ mask, uint64_t seed, long long row_offset) {
+  const long long total = rows * cols;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e / cols;
+    const int c = (int)(e - i * cols);
+    if (!mask[c]) continue;
+    const uint64_t row = (uint64_t)(row_offset + i);
+    const uint4 x = philox4x32_10(make_uint4((uint32_t)row, (uint32_t)(row >> 32), (uint32_t)c, 0u), (uint32_t)seed,
+                                  (uint32_t)(seed >> 32));
+    y[i * ld + c] = (T)((double)(x.x >> 8) * 0x1.0p-24 - 0.5);
+  }
+}
+
+// Per block of l columns: kept columns first, then the null ones, each in increasing order.
+__global__ void kept_first_perm_kernel(const int *__restrict__ mask, int l, int N, int *__restrict__ perm) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= N) return;
+  const int *m = mask + (size_t)b * l;
+  int *p = perm + (size_t)b * l;
+  int pos = 0;
+  for (int j = 0; j < l; ++j)
+    if (!m[j]) p[pos++] = j;
+  for (int j = 0; j < l; ++j)
+    if (m[j]) p[pos++] = j;
+}
+
 }  // namespace
+
+template <class T>
+void fill_null_columns(T *y, long long ld, long long rows, int cols, const int *mask, uint64_t seed,
+                       long long row_offset, cudaStream_t st) {
+  if (rows <= 0 || cols <= 0) return;
+  fill_null_columns_kernel<T><<<grid_for(rows * cols, 256), 256, 0, st>>>(y, ld, rows, cols, mask, seed, row_offset);
+  KLAUNCHED();
+}
+
+void kept_first_perm(const int *mask, int l, int N, int *perm, cudaStream_t st) {
+  if (l <= 0 || N <= 0) return;
+  kept_first_perm_kernel<<<(N + 127) / 128, 128, 0, st>>>(mask, l, N, perm);
+  KLAUNCHED();
+}
+
+template void fill_null_columns<double>(double *, long long, long long, int, const int *, uint64_t, long long,
+                                        cudaStream_t);
+template void fill_null_columns<float>(float *, long long, long long, int, const int *, uint64_t, long long,
+                                       cudaStream_t);
 
 template <class T>
 void rng_gaussian(T *out, long long rows, long long cols, long long ld, uint64_t seed, uint64_t offset,

@@ -119,9 +119,21 @@ constexpr int kStatusNotPD = 7;  // status word: a Cholesky pivot was not positi
 // Per n x n matrix (row-major, batch stride n^2; upper triangle read):
 //   A = alpha W + (shift_abs + shift_rel trace(alpha W)) I = R' R,  X = R^-1 (upper);
 //   out = X (kCholFactor) or out_scale X X' = out_scale A^-1 (kCholInverse).
-// A pivot not above piv_rel times its starting diagonal value sets *status = kStatusNotPD.
+// A pivot not above piv_rel times its starting diagonal value sets *status = kStatusNotPD, unless
+// null_mask is given (kCholFactor; batch x n ints, zero on the first use): then such a finite pivot
+// marks the column as dependent (mask = 1, *null_count += 1 per newly marked column) and zeroes
+// column k of X, instead of failing.  perm (batch x n ints): factor P A P' (row i = row perm[i] of
+// A), X stored back at the original positions.
 void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
-                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st);
+                      double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st,
+                      int *null_mask = nullptr, int *null_count = nullptr, const int *perm = nullptr);
+// Null columns of a TS factorization: y's columns c < cols with mask[c] set (cols = N l) are filled
+// with Philox4x32-10 uniform values in [-1/2, 1/2) keyed by (seed, row_offset + row, c); perm gets,
+// per block of l columns, the kept columns first and then the null ones, each in order.
+template <class T>
+void fill_null_columns(T *y, long long ld, long long rows, int cols, const int *mask, uint64_t seed,
+                       long long row_offset, cudaStream_t st);
+void kept_first_perm(const int *mask, int l, int N, int *perm, cudaStream_t st);
 // X_b := X_b diag(s_b) with the Householder signs of the QR factor whose top n x n block is
 // Qtop_b X_b (Qtop_b = rows 0..n-1 of Q + b q_bs, row stride q_ld).
 template <class T>

@@ -112,6 +112,9 @@ struct Collective {
   void (*fn)(void *, size_t, int, void *, void *) = nullptr;
   void *user = nullptr;
   int nranks = 1, rank = 0, on_device = 0;
+  // installed by the library itself from the communicator of an isvd_Param (real-MPI builds), not
+  // by isvd_gpu_set_allreduce
+  bool from_comm = false;
 };
 Collective &collective();
 // In-place sum over the ranks of `count` values at the device pointer p, ordered on st (no-op on

@@ -49,10 +49,56 @@ constexpr double unit_roundoff() {
   return std::is_same<T, float>::value ? 0x1p-24 : 0x1p-53;
 }
 
+// Orthonormal completion of the null columns of a TS factor (src: rows x N l, null columns zero,
+// the others orthonormal): the null columns are filled with pseudo-random values and then
+// orthogonalized against the kept columns of their block and each other by two CholeskyQR passes
+// in the column order "kept columns first, then the null ones" (a permuted Cholesky), which leaves
+// the span of every leading set of kept columns unchanged.  Householder QR (the reference's
+// gelqf / orglq) also returns some orthonormal completion for a rank-deficient block; which one
+// depends on the rounding of the dependent columns, so only the kept columns are comparable.
+// Products in the stage's own type on CUDA cores.  Result in src (dst is scratch).
+template <class T>
+void complete_null_columns(const StageCtx &c, long long rows, int l, int N, T *&src, long long &lds, T *&dst,
+                           long long &ldd, const int *mask) {
+  const int Nl = N * l;
+  const size_t ll = (size_t)l * l;
+  const uint64_t seed = 0x5EEDC0DEull + (uint64_t)collective().rank;  // each rank fills its own rows
+  fill_null_columns<T>(src, lds, rows, Nl, mask, seed, 0, c.st);
+  DBuf<int> perm((size_t)N * l);
+  kept_first_perm(mask, l, N, perm.p, c.st);
+  DBuf<double> W(N * ll), X(N * ll);
+  DBuf<T> Xt(N * ll);
+  for (int pass = 0; pass < 2; ++pass) {
+    Gemm<T, double> g;
+    g.M = l; g.N = l; g.K = (int)rows; g.batch = N;
+    g.A = src; g.a_rs = 1; g.a_cs = lds; g.a_bs = l;
+    g.B = src; g.b_rs = lds; g.b_cs = 1; g.b_bs = l;
+    g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
+    gemm(g, c.st);
+    allreduce_sum(W.p, N * ll, c.st);
+    chol_inv_batched(l, N, W.p, 1.0, 0.0, 0.0, l * unit_roundoff<T>(), X.p, 1.0, kCholFactor, c.status, c.st,
+                     nullptr, nullptr, perm.p);
+    copy2d<double, T>(X.p, l, 1, Xt.p, l, 1, (long long)N * l, l, c.st);
+    Gemm<T, T> a;
+    a.M = (int)rows; a.N = l; a.K = l; a.batch = N;
+    a.A = src; a.a_rs = lds; a.a_cs = 1; a.a_bs = l;
+    a.B = Xt.p; a.b_rs = l; a.b_cs = 1; a.b_bs = (long long)ll;
+    a.C = dst; a.c_rs = ldd; a.c_cs = 1; a.c_bs = l;
+    gemm(a, c.st);
+    std::swap(src, dst);
+    std::swap(lds, ldd);
+  }
+}
+
 // Householder-signed Q factor of each of the N column blocks (rows x l) of y, in place.
 //   pass 0: W = Y'Y,  R'R = W + s I with s = (sqrt(rows) + l + 1) u trace(W),  Y := Y R^-1
 //   pass 1, 2: the same without shift (CholeskyQR2 on the now well-conditioned panels); the last
 //   R^-1 carries the Householder column signs.
+// A block of numerical rank r < l (a Cholesky pivot at rounding level: the column depends on the
+// ones before it) does not fail: its dependent columns are marked null, left out of the factor
+// (exact zeros, the later columns orthogonalized against the others only) and finally replaced by
+// an orthonormal completion (complete_null_columns), so that the result is orthonormal and its
+// leading independent columns are the Householder factor's, as Householder QR is total.
 // MIXED precision takes the Gram matrices and products from the bf16 split-product tensor-core engine.
 template <class T>
 void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long long ldy) {
@@ -62,6 +108,8 @@ void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long 
   const double u = mixed ? 0x1p-24 : unit_roundoff<T>();
   DBuf<double> W(N * ll), X(N * ll);
   DBuf<T> Xt(N * ll), tmp((size_t)rows * Nl);
+  DBuf<int> nmask((size_t)Nl + 1);  // null-column flags, then their count
+  CK(cudaMemsetAsync(nmask.p, 0, ((size_t)Nl + 1) * sizeof(int), c.st));
   T *src = y, *dst = tmp.p;
   long long lds = ldy, ldd = Nl;
   for (int pass = 0; pass < 3; ++pass) {
@@ -81,7 +129,8 @@ void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long 
     const double mrows = c.m_total > 0 ? (double)c.m_total : (double)rows;
     const double shift_rel = (pass == 0) ? (std::sqrt(mrows) + l + 1) * u : 0.0;
     const double piv_rel = (pass == 0) ? 0.0 : l * u;
-    chol_inv_batched(l, N, W.p, 1.0, 0.0, shift_rel, piv_rel, X.p, 1.0, kCholFactor, c.status, c.st);
+    chol_inv_batched(l, N, W.p, 1.0, 0.0, shift_rel, piv_rel, X.p, 1.0, kCholFactor, c.status, c.st, nmask.p,
+                     nmask.p + Nl);
     if (pass == 2) {
       if (collective().nranks > 1) {
         // the sign rule reads the first l rows of each block, held by rank 0: every rank takes
@@ -114,7 +163,11 @@ void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long 
     std::swap(src, dst);
     std::swap(lds, ldd);
   }
-  // three passes: y -> tmp -> y -> tmp
+  int nulls = 0;
+  CK(cudaMemcpyAsync(&nulls, nmask.p + Nl, sizeof(int), cudaMemcpyDeviceToHost, c.st));
+  CK(cudaStreamSynchronize(c.st));
+  if (nulls > 0) complete_null_columns<T>(c, rows, l, N, src, lds, dst, ldd, nmask.p);
+  // three passes: y -> tmp -> y -> tmp (two more for a completion: -> y -> tmp)
   CK(cudaMemcpy2DAsync(y, ldy * sizeof(T), src, lds * sizeof(T), (size_t)Nl * sizeof(T), rows,
                        cudaMemcpyDeviceToDevice, c.st));
 }

@@ -179,3 +179,82 @@ def test_driver_qr_wy_mixed(lib, oracle, algs):
     assert np.abs(s1[:k] - s0[:k]).max() <= 1e-5 * s0.max()
     assert oracle.max_principal_angle(u1[:, :k], u0[:, :k]) < 1e-3
     assert oracle.projector_err(v1, v0) < 1e-3
+
+
+def _rank5(seed=17):
+    """A 101 x 1001 matrix of rank 5 (the golden shape), sigma 1 .. 0.2."""
+    rng = np.random.default_rng(seed)
+    u = np.linalg.qr(rng.standard_normal((101, 5)))[0]
+    v = np.linalg.qr(rng.standard_normal((1001, 5)))[0]
+    return (u * np.array([1.0, 0.8, 0.6, 0.4, 0.2])) @ v.T
+
+
+@pytest.mark.parametrize("x", ["d", "s"])
+def test_orthogonalize_tsqr_rank_deficient(lib, reflib, x):
+    """Blocks of rank 5 < l = 11 (Y = A Omega with A of rank 5), a block whose third column repeats
+    its first, and a zero block: the factor is orthonormal and contains span(Y_i), as Householder QR
+    (gelqf / orglq) gives, and its leading independent columns are the reference's.  The completing
+    columns are any orthonormal completion, in the reference as here."""
+    a = _rank5()
+    om = np.random.default_rng(3).standard_normal((1001, L * N))
+    ys = a @ om
+    ys[:, 4 * L + 2] = ys[:, 4 * L]          # block 4: column 2 = column 0
+    ys[:, 7 * L:8 * L] = 0.0                  # block 7: zero
+    q = _ts(lib, x, ys, L, N).astype(np.float64)
+    q_ref = _ts(reflib, x, ys, L, N).astype(np.float64)
+    orth, lead = (1e-13, 1e-10) if x == "d" else (1e-5, 1e-3)
+    for i in range(N):
+        blk = slice(i * L, (i + 1) * L)
+        qi = q[:, blk]
+        assert np.abs(qi.T @ qi - np.eye(L)).max() < orth, i
+        yi = ys[:, blk]
+        if np.abs(yi).max() > 0:
+            assert np.linalg.norm(yi - qi @ (qi.T @ yi)) <= orth * 10 * np.linalg.norm(yi), i
+        nlead = {4: 2, 7: 0}.get(i, 5)
+        assert np.abs(qi[:, :nlead] - q_ref[:, blk][:, :nlead]).max() < lead, i
+
+
+def test_driver_ts_rank_deficient_matches_reference(lib, reflib, oracle):
+    """GP / TS / KN / GR on a rank-5 A with l = 11 (the golden shape), Omega passed in: the five
+    nonzero singular values and their U, V columns equal the reference's; the others are zero."""
+    a = _rank5()
+    m, n = a.shape
+    k, p = 8, 3
+    l = k + p
+    om = np.random.default_rng(9).standard_normal((n, l * N))
+    s_r, u_r, v_r, _ = reference_pipeline(reflib, a, om, k, p, N, "TS", "KN", "GR")
+    for prec, x in ((0, "d"), (1, "s")):
+        dt = DT[x]
+        prm = lib.create_param(m, n, k, p, N)
+        s, ut, vt = np.zeros(l, dt), np.zeros((m, l), dt), np.zeros((n, l), dt)
+        retv, _, status = lib.isvd(x, prm, ("GP", "TS", "KN", "GR"), np.ascontiguousarray(a.astype(dt)), n, s, ut,
+                                   l, vt, l, argv=[None, None, [256, 1e-4], None], retc=(0, 0, 2, 0),
+                                   omega=np.ascontiguousarray(om.astype(dt)), ldomega=l * N, precision=prec)
+        assert status == 0, lib.last_error()
+        assert 1 <= int(retv[2][0]) <= 256
+        tol = 1e-10 if x == "d" else 1e-5
+        s = s.astype(np.float64)
+        assert np.abs(s[:5] - s_r[:5]).max() <= tol * s_r[0]
+        assert np.abs(s[5:k]).max() <= (1e-12 if x == "d" else 1e-5) * s_r[0]
+        assert oracle.max_principal_angle(ut[:, :5].astype(np.float64), u_r[:, :5]) < (1e-8 if x == "d" else 1e-3)
+        assert oracle.max_principal_angle(vt[:, :5].astype(np.float64), v_r[:, :5]) < (1e-8 if x == "d" else 1e-3)
+
+
+@pytest.mark.parametrize("x", ["d", "s"])
+def test_postprocess_tsqr_rank_deficient(lib, reflib, oracle, x):
+    """TS postprocessing of Z = A' Qbar of rank 5 < l (reference gelqf of Z' is total): five
+    singular values and U columns equal the reference's, the other singular values are zero."""
+    a = _rank5().astype(DT[x])
+    m, n = a.shape
+    q = np.linalg.qr(np.random.default_rng(6).standard_normal((m, L)))[0].astype(DT[x])
+    prm = lib.create_param(m, n, L, 0, 1)
+    out = {}
+    for name, lb in (("gpu", lib), ("ref", reflib)):
+        s, ut, vt = np.zeros(L, DT[x]), np.zeros((m, L), DT[x]), np.zeros((n, L), DT[x])
+        lb.postprocess(x, "TS", prm, np.ascontiguousarray(a), n, q, L, s, ut, L, vt, L)
+        out[name] = (s.astype(np.float64), ut.astype(np.float64))
+    (s, ut), (s_r, ut_r) = out["gpu"], out["ref"]
+    tol = 1e-10 if x == "d" else 1e-5
+    assert np.abs(s[:5] - s_r[:5]).max() <= tol * s_r[0]
+    assert np.abs(s[5:]).max() <= (1e-12 if x == "d" else 1e-5) * s_r[0]
+    assert oracle.column_angles(ut[:, :5], ut_r[:, :5]).max() < (1e-8 if x == "d" else 1e-3)
