@@ -211,7 +211,8 @@ def test_orthogonalize_tsqr_rank_deficient(lib, reflib, x):
         if np.abs(yi).max() > 0:
             assert np.linalg.norm(yi - qi @ (qi.T @ yi)) <= orth * 10 * np.linalg.norm(yi), i
         nlead = {4: 2, 7: 0}.get(i, 5)
-        assert np.abs(qi[:, :nlead] - q_ref[:, blk][:, :nlead]).max() < lead, i
+        if nlead:
+            assert np.abs(qi[:, :nlead] - q_ref[:, blk][:, :nlead]).max() < lead, i
 
 
 def test_driver_ts_rank_deficient_matches_reference(lib, reflib, oracle):
