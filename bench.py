@@ -1,9 +1,16 @@
 #!/usr/bin/env python3
 """Benchmark: rank-k iSVD (Gaussian projection / Gramian / Kolmogorov-Nagumo / Gramian) of a
-200000 x 20000 FP32 matrix, k = 100, p = 28 (l = 128), N = 32 sketches, on one B200 (N GPUs:
-N independent replicas, one per rank).  Prints one JSON line.
+200000 x 20000 FP32 matrix, k = 100, p = 28 (l = 128), N = 32 sketches, on one B200.  Prints one
+JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size full|small]
+                    [--parallel rowblock|replicas] [--dist-backend nccl|gloo]
+
+On N GPUs (torchrun, one rank per GPU) the default is one solve of the same matrix split by rows
+over the N ranks (the reference's dista = 'R' decomposition): each rank holds the rows
+isvd_createParam gives it and the exchanges (block Grams, G = Qs'Qs, Z = A'Qbar) run as an NCCL
+AllReduce on the library's stream through isvd_gpu_set_allreduce (strong scaling, value = solves/s
+of the whole job).  --parallel replicas runs one independent solve per rank instead (weak scaling).
 
 Inputs are synthetic and seeded: A = U diag(sigma) V' + 1e-4 G with Haar-random U (m x 2000),
 V (n x 2000), sigma geometric from 1 to 1e-3 over 2000 values, G standard normal; generated on
@@ -125,6 +132,28 @@ def make_matrix(torch, w, dev, seed):
     return a
 
 
+def make_row_block(torch, w, dev, seed, prm):
+    """This rank's rows [rowidxbegin, rowidxend) of A = U diag(sigma) V' + noise * G for a solve split
+    by rows: U's row block is the orthonormal factor of a local Gaussian block scaled by
+    sqrt(rows / m), so that the stacked U is exactly orthonormal (U'U = sum_j (m_j / m) I = I); V (the
+    same on every rank) and sigma as make_matrix; the noise is drawn per rank."""
+    m, n, r = w["m"], w["n"], w["rank"]
+    rows = int(prm.nrow_proc)
+    gv = torch.Generator(device=dev)
+    gv.manual_seed(seed)
+    v = torch.linalg.qr(torch.randn(n, r, generator=gv, device=dev, dtype=torch.float32))[0]
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed + 7919 * (int(prm.mpi_rank) + 1))
+    u = torch.linalg.qr(torch.randn(rows, r, generator=g, device=dev, dtype=torch.float32))[0]
+    u.mul_((rows / m) ** 0.5)
+    sig = torch.logspace(0.0, -3.0, r, device=dev, dtype=torch.float32)
+    a = torch.randn(rows, n, generator=g, device=dev, dtype=torch.float32)
+    a.mul_(w["noise"])
+    a.addmm_(u * sig, v.t())
+    del u, v
+    return a
+
+
 def solve(lib, x, prm, a, lda, s, ut, vt, l, seed, precision, retc=(0, 0, 2, 0)):
     retv, times, status = lib.isvd(x, prm, ("GP", "GR", "KN", "GR"), a, lda, s, ut, l, vt, l, seed=seed,
                                    retc=retc, argv=[None, None, [256, 1e-4], None], precision=precision)
@@ -134,11 +163,28 @@ def solve(lib, x, prm, a, lda, s, ut, vt, l, seed, precision, retc=(0, 0, 2, 0))
 
 
 # ------------------------------------------------------------------------------ CPU reference
+# The row-sample extrapolation over-estimates the full solve: on 8192 rows every stage costs more
+# per row than on 200000 (cache reuse, fixed costs).  Measured once on this pool's host (16 cores,
+# OpenBLAS; tests/test_gpu_parity_full.py case "cal"): the reference's isvd_sIsvd on the full
+# 200000 x 20000 matrix took 51.6 / 3.9 / 91.2 / 4.0 s per stage (150.6 s, 77 KN iterations)
+# against 58.0 / 6.7 / 113.0 / 4.5 s extrapolated from the 8192-row sample (182.2 s, 78): these
+# per-stage ratios scale the extrapolation of that shape.
+REF_CAL_SHAPE = (200000, 20000, 8192)
+REF_CAL = (51.573 / 58.023, 3.922 / 6.748, 91.186 / 112.977, 3.967 / 4.455)
+
+
+def reference_calibrated(w, stage_t, rows):
+    """Stage seconds of the full solve from the sample's extrapolation (calibrated when measured)."""
+    if (w["m"], w["n"], rows) == REF_CAL_SHAPE:
+        return np.asarray(stage_t) * np.asarray(REF_CAL), True
+    return np.asarray(stage_t), False
+
+
 def reference_sample(w, steps, warmup, threads):
     """The reference's own CPU pipeline (oracle/_ref, OpenBLAS, 1 MPI rank, `threads` OpenMP
     threads) on a row sample of the workload; each stage time is scaled to the full row count
-    (every stage's cost is linear in m) and the integration time also to the full problem's
-    iteration count when known.  Returns (seconds per full solve, sample description, KN its)."""
+    (every stage's cost is linear in m).  Returns (stage seconds of a full solve, sample
+    description, KN iterations of the sample, seconds per sample solve)."""
     os.environ["OMP_NUM_THREADS"] = str(threads)
     os.environ["OPENBLAS_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -172,38 +218,64 @@ def reference_sample(w, steps, warmup, threads):
     t = np.mean(np.array(per), axis=0) * scale
     desc = ("reference isvd_sIsvd (GP/GR/KN/GR, OpenBLAS, %d threads) on a %d x %d row sample, stage times "
             "scaled by m / %d" % (threads, ms, n, ms))
-    return t, desc, int(np.median(its))
+    t_cal, cal = reference_calibrated(w, t, ms)
+    if cal:
+        desc += " and by the per-stage ratios full / extrapolated measured once at full size (%.3f %.3f %.3f %.3f)" % REF_CAL
+    return t_cal, desc, int(np.median(its)), float(np.mean(np.sum(np.array(per), axis=1))), t
+
+
+def physical_cores():
+    """Physical cores of this host (logical CPUs when the count is unavailable)."""
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+        if n:
+            return int(n)
+    except ImportError:
+        pass
+    return os.cpu_count() or 1
 
 
 def reference_arm(args, w):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    threads = os.cpu_count() or 1
+    threads = physical_cores()
     t0 = time.time()
-    stage_t, desc, its = reference_sample(w, args.steps, args.warmup, threads)
+    stage_t, desc, its, step_s, raw_t = reference_sample(w, args.steps, args.warmup, threads)
     total = float(np.sum(stage_t))
     val = 1.0 / total
     out = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": "solve/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded row sample)",
-        "config": config_dict(w),
+        # a step is one solve of the row sample (what was timed); value is the full solve's rate
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
+        "ms_per_solve_extrapolated": 1e3 * total, "higher_is_better": True,
+        "scaling": "weak" if (args.gpus > 1 and args.parallel == "replicas") else "strong",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic (seeded row sample)",
+        "config": config_dict(w, args.gpus, args.parallel),
         "cpu_baseline": {"value": val, "unit": "solve/s", "cores": threads, "kind": "reference", "sample": desc,
-                         "stage_s": [float(x) for x in stage_t], "kn_iterations_sample": its},
+                         "stage_s": [float(x) for x in stage_t], "kn_iterations_sample": its,
+                         "stage_s_uncalibrated": [float(x) for x in raw_t]},
         "e2e": {"value": val, "unit": "solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
     print(json.dumps(out), flush=True)
 
 
-def config_dict(w):
+def config_dict(w, world=1, parallel="rowblock"):
+    if world == 1:
+        par, ranks = "one GPU", "1 MPI rank"
+    elif parallel == "rowblock":
+        par = "row blocks over %d GPUs (NCCL AllReduce of the block Grams, G and Z)" % world
+        ranks = "%d ranks" % world
+    else:
+        par, ranks = "replicas (one independent solve per GPU)", "1 MPI rank each"
     return {"workload": "iSVD %dx%d FP32, rank-%d Haar factors, sigma 1..1e-3 geometric, +%.0e noise; "
-                        "k=%d p=%d N=%d; GP/GR/KN(1e-4,256)/GR, row block, 1 MPI rank"
-                        % (w["m"], w["n"], w["rank"], w["noise"], w["k"], w["p"], w["N"]),
+                        "k=%d p=%d N=%d; GP/GR/KN(1e-4,256)/GR, row block, %s"
+                        % (w["m"], w["n"], w["rank"], w["noise"], w["k"], w["p"], w["N"], ranks),
             "m": w["m"], "n": w["n"], "k": w["k"], "p": w["p"], "N": w["N"], "seed": w["seed"],
-            "l2_flush": "none needed: A (%.1f GB) is larger than L2" % (w["m"] * w["n"] * 4 / 1e9),
-            "parallelism": "replicas (one independent solve per GPU)"}
+            "l2_flush": "none needed: A (%.1f GB) is larger than L2" % (w["m"] * w["n"] * 4 / 1e9 / world),
+            "parallelism": par}
 
 
 # ------------------------------------------------------------------------------ B200 arm
@@ -291,9 +363,14 @@ def batch_main(args):
     one after another through isvd_sIsvd_ex (NATIVE FP32, one pass)."""
     import torch
     import isvd_b200
+    out = run_batched(torch, isvd_b200.load(), args.steps, args.warmup)
+    print(json.dumps(out), flush=True)
+
+
+def run_batched(torch, lib, steps, warmup):
+    """The batched-solves workload (batch_main); returns its JSON record."""
     from isvd_b200.capi import c_int_t
     dev = torch.device("cuda", 0)
-    lib = isvd_b200.load()
     rng = np.random.default_rng(BATCH["seed"])
     gen = torch.Generator(device=dev).manual_seed(BATCH["seed"])
     mats = []
@@ -330,18 +407,18 @@ def batch_main(args):
                            arr([d["s"].data_ptr() for d in mats], vp), arr([d["ut"].data_ptr() for d in mats], vp),
                            arr([d["ut"].shape[1] for d in mats]), arr([d["vt"].data_ptr() for d in mats], vp),
                            arr([d["vt"].shape[1] for d in mats]), arr(seeds), argv.ctypes.data, 2, its, None)
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         assert call() == 0, lib.last_error()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = lib.lib.isvd_gpu_kernel_launch_count()
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         assert call() == 0, lib.last_error()
     e1.record()
     torch.cuda.synchronize()
-    launches = (lib.lib.isvd_gpu_kernel_launch_count() - l0) // args.steps
-    ms_batch = e0.elapsed_time(e1) / args.steps
+    launches = (lib.lib.isvd_gpu_kernel_launch_count() - l0) // steps
+    ms_batch = e0.elapsed_time(e1) / steps
     s_batch = [d["s"].clone() for d in mats]
     it_batch = list(its)
     # the same matrices, one single solve each
@@ -361,7 +438,7 @@ def batch_main(args):
     lib.lib.isvd_gpu_batch_destroy(ctypes.c_void_p(batch))
     out = {
         "metric": "batched iSVD matrices/s (256 uneven FP32 matrices)", "value": B / (ms_batch / 1e3),
-        "unit": "matrix/s", "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup),
+        "unit": "matrix/s", "n_gpus": 1, "steps": steps, "warmup": max(3, warmup),
         "ms_per_step": ms_batch, "higher_is_better": True, "dtype": "fp32 (fp64 l x l)", "data": "synthetic",
         "config": {"workload": "256 matrices, m log-uniform [512, 8192], n log-uniform [256, 4096] (n <= m), "
                                "rank 4k geometric 1..1e-3 + 1e-4 noise, k in {8,16,32,64}, p = k/2, N = 8, GP/GR/KN/GR",
@@ -372,7 +449,103 @@ def batch_main(args):
         "sigma_rel_diff_max": err,
         "kn_iterations_equal": sum(int(a == b) for a, b in zip(it_batch, it_seq)),
     }
-    print(json.dumps(out), flush=True)
+    return out
+
+
+DIFF = dict(m=16384, n=4096, rank=512, k=64, p=32, N=16, noise=1e-4, xcols=32, seed=5)
+
+
+def run_differentiated(torch, lib, steps, warmup):
+    """The differentiated solve: A 16384 x 4096 FP32, rank 512 (sigma 1 .. 1e-2 geometric) + 1e-4
+    noise, k = 64, l = 96, N = 16; loss sum_i w_i s_i + ||U U' X||_F^2 with w and X (16384 x 32)
+    seeded Gaussian.  Timed (CUDA events, K steps after W warm-up steps): the MIXED forward
+    (isvd_sIsvd_ex, GP/GR/KN/GR) and the MIXED FP32 adjoint (isvd_sSvdAdjoint: ds = w,
+    dU = 2 X X' U).  Accuracy: the adjoint from the FP64 dense factors against the FP64 dense-SVD
+    gradient (torch autograd through torch.linalg.svd), max abs error over max abs gradient."""
+    import ctypes as ct
+    from isvd_b200.capi import c_int_t, ptr
+    w = DIFF
+    dev = torch.device("cuda", 0)
+    m, n, r, k, p, N = w["m"], w["n"], w["rank"], w["k"], w["p"], w["N"]
+    l = k + p
+    g = torch.Generator(device=dev).manual_seed(w["seed"])
+    uu = torch.linalg.qr(torch.randn(m, r, device=dev, dtype=torch.float64, generator=g))[0]
+    vv = torch.linalg.qr(torch.randn(n, r, device=dev, dtype=torch.float64, generator=g))[0]
+    sig = torch.logspace(0, -2, r, device=dev, dtype=torch.float64)
+    a64 = (uu * sig) @ vv.T + w["noise"] * torch.randn(m, n, device=dev, dtype=torch.float64, generator=g)
+    del uu, vv
+    wt = torch.randn(k, device=dev, dtype=torch.float64, generator=g)
+    xx = torch.randn(m, w["xcols"], device=dev, dtype=torch.float64, generator=g)
+    f32 = lambda t: t.to(torch.float32).contiguous()  # noqa: E731
+    a = f32(a64)
+    fn = lib.lib.isvd_sSvdAdjoint
+    vp = ct.c_void_p
+    fn.argtypes = [c_int_t, c_int_t, c_int_t, ct.c_char, vp, c_int_t, vp, vp, c_int_t, vp, c_int_t, vp, vp,
+                   c_int_t, vp, c_int_t, vp, c_int_t, ct.c_int, ct.c_double, ct.POINTER(ct.c_int)]
+    fn.restype = ct.c_int
+    its = ct.c_int(0)
+
+    def adjoint(s_, u_, v_, ds_, du_, da_):
+        st = fn(m, n, k, b"R", ptr(a), n, ptr(s_), ptr(u_), k, ptr(v_), k, ptr(ds_), ptr(du_), k, None, k, ptr(da_),
+                n, 300, 1e-6, ct.byref(its))
+        if st != 0:
+            raise RuntimeError("isvd_sSvdAdjoint failed: %s" % (lib.last_error(),))
+
+    prm = lib.create_param(m, n, k, p, N)
+    s = torch.zeros(l, device=dev)
+    ut = torch.zeros((m, l), device=dev)
+    vt = torch.zeros((n, l), device=dev)
+    ds = f32(wt)
+    da = torch.zeros_like(a)
+    lib.lib.isvd_gpu_set_precision(1)
+    try:
+        def forward():
+            retv, _, st = lib.isvd("s", prm, ("GP", "GR", "KN", "GR"), a, n, s, ut, l, vt, l, seed=w["seed"],
+                                   argv=[None, None, [256, 1e-4], None], retc=(0, 0, 2, 0), precision=1)
+            if st != 0:
+                raise RuntimeError("isvd_sIsvd_ex failed: %s" % (lib.last_error(),))
+            return int(retv[2][0])
+
+        def backward():
+            u_ = ut[:, :k].contiguous()
+            v_ = vt[:, :k].contiguous()
+            du_ = (2.0 * xx @ (xx.T @ u_.double())).to(torch.float32).contiguous()
+            adjoint(s[:k].contiguous(), u_, v_, ds, du_, da)
+
+        for _ in range(max(3, warmup)):
+            forward()
+            backward()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        t_fwd = t_bwd = 0.0
+        for _ in range(steps):
+            ev[0].record()
+            kn = forward()
+            ev[1].record()
+            backward()
+            ev[2].record()
+            torch.cuda.synchronize()
+            t_fwd += ev[0].elapsed_time(ev[1])
+            t_bwd += ev[1].elapsed_time(ev[2])
+        cg_its = its.value
+        # accuracy of the adjoint: from the FP64 dense factors, against the FP64 dense gradient
+        at = a64.clone().requires_grad_(True)
+        U, S, Vh = torch.linalg.svd(at, full_matrices=False)
+        L = (wt * S[:k]).sum() + ((U[:, :k] @ (U[:, :k].T @ xx)) ** 2).sum()
+        L.backward()
+        gref = at.grad
+        u0, s0, v0 = U[:, :k].detach(), S[:k].detach(), Vh[:k].T.detach()
+        adjoint(f32(s0), f32(u0), f32(v0), ds, f32(2.0 * xx @ (xx.T @ u0)), da)
+        torch.cuda.synchronize()
+        err = float((da.double() - gref).abs().max() / gref.abs().max())
+        sig_err = float(((s[:k].double() - s0).abs() / s0).max())
+    finally:
+        lib.lib.isvd_gpu_set_precision(0)
+    return {"workload": "A 16384x4096 FP32 rank 512 + 1e-4 noise, k=64 l=96 N=16; loss sum w_i s_i + ||U U' X||^2",
+            "forward_ms": t_fwd / steps, "adjoint_ms": t_bwd / steps, "kn_iterations": kn,
+            "adjoint_cg_iterations": cg_its, "adjoint_rel_err_vs_fp64_dense": err,
+            "forward_sigma_rel_err_vs_fp64_dense": sig_err, "precision": "MIXED forward and adjoint",
+            "steps": steps, "warmup": max(3, warmup)}
 
 
 def main():
@@ -385,12 +558,19 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-extra", action="store_true",
+                    help="leave out the batched (256 uneven matrices) and differentiated-solve legs")
     ap.add_argument("--single", action="store_true",
                     help="one MIXED solve and its stage times, nothing else (for ncu launch lists / captures)")
     ap.add_argument("--batched", action="store_true",
                     help="the batched-solves workload (256 uneven matrices) instead of the single large solve")
     ap.add_argument("--square50k", action="store_true",
                     help="the 50000 x 50000 TS / WY / column-block parity case, MIXED beside FP64")
+    ap.add_argument("--parallel", default="rowblock", choices=["rowblock", "replicas"],
+                    help="N > 1: one solve split by rows over the ranks (default) or one solve per rank")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process-group backend (gloo: device buffers staged through the host, e.g. "
+                         "several ranks sharing one GPU for a functional check)")
     args = ap.parse_args()
     if args.batched:
         return batch_main(args)
@@ -406,25 +586,37 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    gpu = local % max(1, torch.cuda.device_count())
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    dev = torch.device("cuda", local)
+        torch.cuda.set_device(gpu)
+        dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", gpu)
     torch.cuda.set_device(dev)
     lib = isvd_b200.load()
     stream = torch.cuda.current_stream(dev)
     lib.lib.isvd_gpu_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    rowblock = world > 1 and args.parallel == "rowblock"
+    if rowblock:  # the ranks join as row blocks; every exchange is an AllReduce on the library stream
+        from isvd_b200.capi import torch_device_allreduce
+        lib.set_allreduce(torch_device_allreduce(), world, rank, on_device=True)
 
     m, n, k, p, N = w["m"], w["n"], w["k"], w["p"], w["N"]
     l = k + p
-    a = make_matrix(torch, w, dev, w["seed"] + 1000 * rank)
-    torch.cuda.synchronize()
     prm = lib.create_param(m, n, k, p, N)
+    if rowblock:
+        a = make_row_block(torch, w, dev, w["seed"], prm)
+    else:
+        a = make_matrix(torch, w, dev, w["seed"] + 1000 * rank)
+    torch.cuda.synchronize()
+    if not rowblock:
+        prm = lib.create_param(m, n, k, p, N)
+    mloc = int(prm.nrow_proc) if rowblock else m
+    nloc = int(prm.ncol_proc) if rowblock else n
     s = torch.zeros(l, dtype=torch.float32, device=dev)
-    ut = torch.zeros((m, l), dtype=torch.float32, device=dev)
-    vt = torch.zeros((n, l), dtype=torch.float32, device=dev)
+    ut = torch.zeros((mloc, l), dtype=torch.float32, device=dev)
+    vt = torch.zeros((nloc, l), dtype=torch.float32, device=dev)
     seed = w["seed"]
     if args.single:
         retv, times = solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
@@ -463,7 +655,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
     ms_per = ms_total / args.steps
-    value = world * args.steps / (ms_total / 1e3)
+    solves_per_step = 1 if (rowblock or world == 1) else world
+    value = solves_per_step * args.steps / (ms_total / 1e3)
     s_mixed = s.double().cpu().numpy()
 
     # per-kernel timing of the dominant kernel (separate, untimed run)
@@ -479,7 +672,7 @@ def main():
     # launch time = total algorithmic flops / total kernel time
     sketch_ms_total = sk[0] if sk else None
     sketch_launches = sk[1] if sk else 0
-    alg_flops = 2.0 * m * n * (l * N)
+    alg_flops = 2.0 * mloc * n * (l * N)  # this rank's rows
     achieved = alg_flops / (sketch_ms_total * 1e-3) / 1e12 if sketch_ms_total else None
     # bf16 plane products per algorithmic product, from the executed flops the library records
     nprod = int(round(sk[2] / alg_flops)) if sk else 2
@@ -493,7 +686,7 @@ def main():
                 "peak_burst": peak3_burst, "frac_burst": (achieved / peak3_burst) if achieved else None,
                 "traffic": SKETCH_LAUNCH_TRAFFIC if headline_shape and sketch_launches == 1 else None,
                 "traffic_unit": "bytes per launch (one launch over all m rows; ncu, dram read + write)",
-                "alg_bytes_per_launch": float(m * n * 4 + m * l * N * 4 + n * l * N * 2),
+                "alg_bytes_per_launch": float(mloc * n * 4 + mloc * l * N * 4 + n * l * N * 2),
                 "convention": "algorithmic 2 m n Nl flops per solve / kernel time; peak = %s bf16 dense "
                               "sustained %.1f TFLOP/s / %d products (burst %.1f / %d also given)"
                               % (peak_kind, bf16_sus, nprod, bf16, nprod),
@@ -501,14 +694,15 @@ def main():
                 "other_tcgen05_ms": {t: (v[0] / v[1] if v else None) for t, v in prof.items() if t != "sketch"}}
 
     out = {"metric": METRIC, "value": value, "unit": "solve/s", "n_gpus": world, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms_per, "higher_is_better": True, "scaling": "weak",
+           "warmup": args.warmup, "ms_per_step": ms_per, "higher_is_better": True,
+           "scaling": "weak" if (world > 1 and not rowblock) else "strong",
            "vs_baseline": None, "dtype": "f32 via bf16 split planes (sketch: 2 A planes x exact bf16 Omega; fp32 accumulate; fp64 l x l)",
-           "data": "synthetic (seeded, generated on GPU)", "config": config_dict(w),
+           "data": "synthetic (seeded, generated on GPU)", "config": config_dict(w, world, args.parallel),
            "stage_ms": [1e3 * x / args.steps for x in stage], "kn_iterations": kn_its,
            "gpu_launches": int(launches), "roofline": roofline}
 
-    # FP64 path on the same matrix and Omega
-    if not args.skip_fp64:
+    # FP64 path on the same matrix and Omega (one GPU)
+    if not args.skip_fp64 and not rowblock:
         a64 = a.double()
         s64 = torch.zeros(l, dtype=torch.float64, device=dev)
         ut64 = torch.zeros((m, l), dtype=torch.float64, device=dev)
@@ -535,12 +729,12 @@ def main():
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
     if not args.skip_e2e:
-        ah = torch.empty((m, n), dtype=torch.float32, pin_memory=True)
+        ah = torch.empty((mloc, n), dtype=torch.float32, pin_memory=True)
         ah.copy_(a)
         sh = torch.zeros(l, dtype=torch.float32, pin_memory=True)
-        uh = torch.zeros((m, l), dtype=torch.float32, pin_memory=True)
-        vh = torch.zeros((n, l), dtype=torch.float32, pin_memory=True)
-        del a
+        uh = torch.zeros((mloc, l), dtype=torch.float32, pin_memory=True)
+        vh = torch.zeros((nloc, l), dtype=torch.float32, pin_memory=True)
+        a = None
         torch.cuda.synchronize()
         solve(lib, "s", prm, ah, n, sh, uh, vh, l, seed, 1)  # warm
         torch.cuda.synchronize()
@@ -560,22 +754,32 @@ def main():
             t = torch.tensor([te], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             te = float(t.item())
-        out["e2e"] = {"value": world / te, "unit": "solve/s", "ms_per_solve": 1e3 * te,
-                      "h2d_bytes_per_step": m * n * 4, "d2h_bytes_per_step": (l + m * k + n * k) * 4,
+        reps_job = 1 if rowblock else world  # whole-job bytes: every rank's copies
+        out["e2e"] = {"value": solves_per_step / te, "unit": "solve/s", "ms_per_solve": 1e3 * te,
+                      "h2d_bytes_per_step": reps_job * m * n * 4,
+                      "d2h_bytes_per_step": reps_job * (l * (world if rowblock else 1) + m * k + n * k) * 4,
                       "path": "isvd_sIsvd_ex with pinned host A, s, U, V (H2D of A and D2H of s, U, V timed)"}
     out["clocks"] = clk.summary()
+    if world == 1 and not args.skip_extra:
+        a = None  # the headline matrix
+        torch.cuda.empty_cache()
+        out["batched_256_uneven"] = run_batched(torch, lib, args.steps, args.warmup)
+        out["differentiated_16384x4096"] = run_differentiated(torch, lib, args.steps, args.warmup)
     if rank == 0 and world == 1 and not args.skip_cpu:
+        cores = physical_cores()
         try:
-            stage_t, desc, its = reference_sample(w, 1, 0, os.cpu_count() or 1)
+            stage_t, desc, its, _, _ = reference_sample(w, 1, 0, cores)
             tot = float(np.sum(stage_t))
-            out["cpu_baseline"] = {"value": 1.0 / tot, "unit": "solve/s", "cores": os.cpu_count(),
+            out["cpu_baseline"] = {"value": 1.0 / tot, "unit": "solve/s", "cores": cores,
                                    "kind": "reference", "sample": desc, "stage_s": [float(x) for x in stage_t]}
         except Exception as e:  # the checker library may be absent on a fresh box
-            out["cpu_baseline"] = {"value": None, "unit": "solve/s", "cores": os.cpu_count(), "kind": "reference",
+            out["cpu_baseline"] = {"value": None, "unit": "solve/s", "cores": cores, "kind": "reference",
                                    "sample": "unavailable: %s" % e}
     if rank == 0:
         print(json.dumps(out), flush=True)
     lib.lib.isvd_gpu_set_stream(None)
+    if rowblock:
+        lib.set_allreduce(None, 1, 0)
     if dist is not None:
         dist.destroy_process_group()
 

@@ -149,8 +149,10 @@ void isvd_gpu_batch_destroy( isvd_gpu_batch *batch );
  *   Lam S^2 - Aperp Aperp' Lam = (I - UU') dU,   Gam S^2 - Aperp' Aperp Gam = (I - VV') dV,
  * the last two solved column by column by conjugate gradients (at most cg_iters iterations each,
  * relative residual tol); cg_iters = 0 uses Lam = (I - UU') dU S^-2 (exact when rank(A) = k).
- * *iterations (may be NULL) receives the CG iterations used.  Buffers may be host or device memory.
- * Returns an ISVD_GPU_* status. */
+ * *iterations (may be NULL) receives the CG iterations used (both systems together).  Buffers may
+ * be host or device memory.  In MIXED precision (isvd_gpu_set_precision) isvd_sSvdAdjoint runs the
+ * products by A and A' on the tensor cores (A in two bf16 planes, the other operand in three);
+ * NATIVE keeps them in FP32 on CUDA cores.  Returns an ISVD_GPU_* status. */
 int isvd_sSvdAdjoint(
     const isvd_int_t m, const isvd_int_t n, const isvd_int_t k, const char ordera,
     const isvd_s_val_t *a, const isvd_int_t lda, const isvd_s_val_t *s,

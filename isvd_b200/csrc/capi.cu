@@ -766,7 +766,7 @@ int adjoint_api(isvd_int_t m, isvd_int_t n, isvd_int_t k, char ordera, const T *
     if (dut) REQUIRE(lddut >= k);
     if (dvt) REQUIRE(lddvt >= k);
     REQUIRE(cg_iters >= 0 && tol >= 0);
-    Ctx c(kNative);
+    Ctx c(-1);  // the library precision mode: MIXED puts the FP32 products by A on tensor cores
     cudaStream_t sst = c.sc.st;
     View<T> A, S, U, V, dS, dU, dV, dA;
     if (ordera_ == 'R') {

@@ -13,6 +13,7 @@
 //   G = Qs' Qs   2 x 2 planes, 3 products      (errors average over the m-long inner products)
 //   Z = A' Qbar  Qbar': 2 planes x A: 2 planes, 3 products
 #include <algorithm>
+#include <cstdio>
 #include <cstdlib>
 
 #include "kernels.h"
@@ -77,6 +78,22 @@ int sketch_planes() {
   return np;
 }
 
+// L2 policy of the sketch's tile loads: A (16 GB at the headline shape) streams through once per
+// 16 N tiles running side by side, Omega' (N l x n, 164 MB) is re-read by every row panel.
+// ISVD_GPU_SKETCH_L2 = "a,b" (0 normal, 1 evict-first, 2 evict-last) overrides the default.
+static void sketch_l2_hints(UmmaGemm &g) {
+  static int h[2] = {-1, -1};
+  if (h[0] < 0) {
+    h[0] = 0;
+    h[1] = 0;
+    if (const char *e = getenv("ISVD_GPU_SKETCH_L2")) {
+      if (sscanf(e, "%d,%d", &h[0], &h[1]) != 2 || h[0] < 0 || h[0] > 2 || h[1] < 0 || h[1] > 2) h[0] = h[1] = 0;
+    }
+  }
+  g.l2_a = h[0];
+  g.l2_b = h[1];
+}
+
 // Sketch Y = A Omega with A processed in row panels: each panel is split into A's bf16 planes
 // (kept for the postprocess) and multiplied by Omega' on the tensor cores.  When A is in host
 // memory, panel p + 1 is copied to the device on the copy stream while panel p is split and
@@ -125,6 +142,7 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
   g.status = c.status;
   g.chunk_k = 512;  // 5e-7 relative tensor-core chain error per chunk, below the 2^-17 split level
   g.tag = "sketch";
+  sketch_l2_hints(g);
   if (a_dev) {
     // A on the device: split every row, then one launch over all m rows (no per-panel wave tail)
     for (long long r0 = 0; r0 < m; r0 += P) {

@@ -31,6 +31,9 @@ def test_reference_arm_json_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # ms_per_step is the timed sample step: the steps fit in the run's own wall clock
+    assert d["ms_per_step"] * d["steps"] <= 1e3 * d["wall_s"]
+    assert d["ms_per_solve_extrapolated"] == 1e3 / d["value"]
 
 
 def test_reference_arm_other_ranks_exit_quietly():

@@ -87,6 +87,37 @@ def test_adjoint_matches_dense_svd_gradient(lib, ordera):
     assert np.abs(da - g).max() < 1e-8 * np.abs(g).max()
 
 
+@pytest.mark.parametrize("ordera", [b"R", b"C"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["native", "mixed"])
+def test_adjoint_fp32_u_and_v_terms(lib, ordera, precision):
+    """FP32 adjoint with both complement systems (dU and dV), A row- and column-major, NATIVE and
+    MIXED (products by A on the tensor cores), against the FP64 dense gradient of
+    L = w's + ||U U' X||_F^2 + ||V V' Y||_F^2."""
+    torch = pytest.importorskip("torch")
+    a, k, w, xx = slice_case(11)
+    yy = np.random.default_rng(12).standard_normal((a.shape[1], 8))
+    at = torch.tensor(a, dtype=torch.float64, requires_grad=True)
+    uu, ss, vh = torch.linalg.svd(at, full_matrices=False)
+    uk, vk = uu[:, :k], vh[:k].T
+    L = (torch.tensor(w) * ss[:k]).sum() + ((uk @ (uk.T @ torch.tensor(xx))) ** 2).sum() + \
+        ((vk @ (vk.T @ torch.tensor(yy))) ** 2).sum()
+    L.backward()
+    g = at.grad.numpy()
+    _, u, s, v = loss_parts(a, k, w, xx)
+    du = 2.0 * xx @ (xx.T @ u)
+    dv = 2.0 * yy @ (yy.T @ v)
+    f32 = lambda x_: np.ascontiguousarray(x_, dtype=np.float32)  # noqa: E731
+    aa = f32(a) if ordera == b"R" else np.asfortranarray(a, dtype=np.float32)
+    lib.lib.isvd_gpu_set_precision(precision)
+    try:
+        da, its = adjoint(lib, aa, f32(s), f32(u), f32(v), ds=f32(w), du=f32(du), dv=f32(dv), cg_iters=300,
+                          tol=1e-6, x="s", ordera=ordera)
+    finally:
+        lib.lib.isvd_gpu_set_precision(0)
+    assert its > 0
+    assert np.abs(da.astype(np.float64) - g).max() < 1e-3 * np.abs(g).max()
+
+
 def test_adjoint_finite_differences(lib):
     """Central differences, h = 1e-3 in FP64, along random directions of the 512 x 256 slice."""
     a, k, w, xx = slice_case(7)
@@ -177,9 +208,11 @@ def test_autograd_function_end_to_end(lib):
     assert np.abs(got - g).max() < 5e-4 * np.abs(g).max()
 
 
-def test_adjoint_differentiated_solve_fp32(lib):
+@pytest.mark.parametrize("precision", [0, 1], ids=["native", "mixed"])
+def test_adjoint_differentiated_solve_fp32(lib, precision):
     """The differentiated-solve shape: A 16384 x 4096 FP32, rank 512 plus noise, k = 64, X 16384 x 32.
-    The FP32 adjoint (device buffers) from the FP64 dense factors, against the FP64 dense gradient."""
+    The FP32 adjoint (device buffers) from the FP64 dense factors, against the FP64 dense gradient;
+    NATIVE (CUDA-core FP32 products) and MIXED (products by A on the tensor cores)."""
     torch = pytest.importorskip("torch")
     dev = torch.device("cuda:0")
     m, n, k, r = 16384, 4096, 64, 512
@@ -198,7 +231,11 @@ def test_adjoint_differentiated_solve_fp32(lib):
     u, s, v = U[:, :k].detach(), S[:k].detach(), Vh[:k].T.detach()
     du = 2.0 * xx @ (xx.T @ u)
     f32 = lambda t: t.to(torch.float32).contiguous()
-    da, its = adjoint(lib, f32(a), f32(s), f32(u), f32(v), ds=f32(w), du=f32(du), cg_iters=300, tol=1e-6, x="s")
+    lib.lib.isvd_gpu_set_precision(precision)
+    try:
+        da, its = adjoint(lib, f32(a), f32(s), f32(u), f32(v), ds=f32(w), du=f32(du), cg_iters=300, tol=1e-6, x="s")
+    finally:
+        lib.lib.isvd_gpu_set_precision(0)
     assert its > 0
     err = (da.double() - gref).abs().max().item() / gref.abs().max().item()
     assert err < 1e-3
