@@ -363,12 +363,13 @@ def batch_main(args):
     one after another through isvd_sIsvd_ex (NATIVE FP32, one pass)."""
     import torch
     import isvd_b200
-    out = run_batched(torch, isvd_b200.load(), args.steps, args.warmup)
+    out = run_batched(torch, isvd_b200.load(), args.steps, args.warmup, single=args.single)
     print(json.dumps(out), flush=True)
 
 
-def run_batched(torch, lib, steps, warmup):
-    """The batched-solves workload (batch_main); returns its JSON record."""
+def run_batched(torch, lib, steps, warmup, single=False):
+    """The batched-solves workload (batch_main); returns its JSON record.  single: one batch call
+    and nothing else (for launch lists)."""
     from isvd_b200.capi import c_int_t
     dev = torch.device("cuda", 0)
     rng = np.random.default_rng(BATCH["seed"])
@@ -407,6 +408,12 @@ def run_batched(torch, lib, steps, warmup):
                            arr([d["s"].data_ptr() for d in mats], vp), arr([d["ut"].data_ptr() for d in mats], vp),
                            arr([d["ut"].shape[1] for d in mats]), arr([d["vt"].data_ptr() for d in mats], vp),
                            arr([d["vt"].shape[1] for d in mats]), arr(seeds), argv.ctypes.data, 2, its, None)
+    if single:
+        l0 = lib.lib.isvd_gpu_kernel_launch_count()
+        assert call() == 0, lib.last_error()
+        torch.cuda.synchronize()
+        lib.lib.isvd_gpu_batch_destroy(ctypes.c_void_p(batch))
+        return {"batch_launches": int(lib.lib.isvd_gpu_kernel_launch_count() - l0), "kn_iterations": list(its)}
     for _ in range(max(3, warmup)):
         assert call() == 0, lib.last_error()
     torch.cuda.synchronize()
@@ -638,7 +645,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stage = np.zeros(4)
     kn_its = 0
-    with ClockSampler(local) as clk:
+    with ClockSampler(gpu) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             retv, times = solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
@@ -664,7 +671,8 @@ def main():
     lib.lib.isvd_gpu_profile_enable(1)
     solve(lib, "s", prm, a, n, s, ut, vt, l, seed, 1)
     lib.lib.isvd_gpu_profile_enable(0)
-    prof = {t: lib.profile(t) for t in ("sketch", "block_gram", "gram_full", "project")}
+    prof = {t: lib.profile(t) for t in ("sketch", "block_gram", "block_apply", "gram_full", "kn_product",
+                                        "coeff_apply", "project")}
 
     hbm, bf16, bf16_sus, peak_kind = peaks()
     sk = prof["sketch"]
