@@ -52,19 +52,7 @@ struct KParams {
   int stage_out;  // epilogue stages its rows through shared memory (C rows contiguous)
   int bloop;      // one CTA runs every batch of its tile in turn (grid z = 1, no split-K)
   int vec_out;    // direct epilogue stores as 16-byte vectors (C rows contiguous and aligned)
-  int l2_a, l2_b; // L2 eviction priority of the A / B tile loads (kL2Normal / kL2First / kL2Last)
 };
-
-enum L2Hint : int { kL2Normal = 0, kL2First = 1, kL2Last = 2 };
-
-// 64-bit L2 cache policy for cp.async.bulk loads: every line the load brings in gets the given
-// eviction priority (createpolicy.fractional, fraction 1).  kL2Normal: no policy is passed.
-__device__ __forceinline__ uint64_t l2_policy(int hint) {
-  uint64_t pol = 0;
-  if (hint == kL2First) asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-  else if (hint == kL2Last) asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-  return pol;
-}
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -114,20 +102,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::
           "r"(su32(dst)),
       "l"((uint64_t)map), "r"(su32(bar)), "r"(x), "r"(y), "r"(z)
-      : "memory");
-}
-// As tma_load_3d with an L2 cache policy (l2_policy) for the loaded lines; hint kL2Normal loads
-// without one.
-__device__ __forceinline__ void tma_load_3d_hint(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y,
-                                                 int z, int hint, uint64_t pol) {
-  if (hint == kL2Normal) {
-    tma_load_3d(dst, map, bar, x, y, z);
-    return;
-  }
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%3, "
-      "%4, %5}], [%2], %6;" ::"r"(su32(dst)),
-      "l"((uint64_t)map), "r"(su32(bar)), "r"(x), "r"(y), "r"(z), "l"(pol)
       : "memory");
 }
 
@@ -252,7 +226,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------------- TMA producer
     int issued = 0, s = 0;
     uint32_t ph = 1;  // parity of the empty phase to wait for (first pass: none)
-    const uint64_t pol_a = l2_policy(p.l2_a), pol_b = l2_policy(p.l2_b);
     for (int seg = 0; seg < nseg && !*abort_flag; ++seg) {
     const int b = bloop ? seg : bz;
     const int a_row = (int)(b * p.a_mn_step) + m0;
@@ -268,23 +241,21 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int ka = k0 + (int)(b * p.a_k_step), kbb = k0 + (int)(b * p.b_k_step);
       for (int q = 0; q < p.na; ++q) {
         if (!AMN) {
-          tma_load_3d_hint(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q, p.l2_a, pol_a);
+          tma_load_3d(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q);
         } else {
 #pragma unroll
           for (int j = 0; j < BM / 64; ++j)
-            tma_load_3d_hint(st + q * C::A_TILE + j * (BK * 128), &mapA, &full[s], a_row + 64 * j, ka, q, p.l2_a,
-                             pol_a);
+            tma_load_3d(st + q * C::A_TILE + j * (BK * 128), &mapA, &full[s], a_row + 64 * j, ka, q);
         }
       }
       uint8_t *bt = st + p.na * C::A_TILE;
       for (int q = 0; q < p.nb; ++q) {
         if (!BMN) {
-          tma_load_3d_hint(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q, p.l2_b, pol_b);
+          tma_load_3d(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q);
         } else {
 #pragma unroll
           for (int j = 0; j < BN / 64; ++j)
-            tma_load_3d_hint(bt + q * C::B_TILE + j * (BK * 128), &mapB, &full[s], b_row + 64 * j, kbb, q, p.l2_b,
-                             pol_b);
+            tma_load_3d(bt + q * C::B_TILE + j * (BK * 128), &mapB, &full[s], b_row + 64 * j, kbb, q);
         }
       }
       ++issued;
@@ -1048,8 +1019,6 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;
   p.status = status;
-  p.l2_a = g.l2_a;
-  p.l2_b = g.l2_b;
   p.total_kb = (g.K + BK - 1) / BK;
   const int gx = (g.N + BN - 1) / BN, gy = (g.M + BM - 1) / BM;
   const long long tiles = (long long)gx * gy * g.batch;
@@ -1150,8 +1119,6 @@ void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;
   p.status = status;
-  p.l2_a = g.l2_a;
-  p.l2_b = g.l2_b;
   p.total_kb = (g.K + BK - 1) / BK;
   p.kbps = p.total_kb;
   p.chunk_kb = chunk_kblocks(BK, g.chunk_k);

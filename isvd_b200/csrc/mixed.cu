@@ -13,9 +13,7 @@
 //   G = Qs' Qs   2 x 2 planes, 3 products      (errors average over the m-long inner products)
 //   Z = A' Qbar  Qbar': 2 planes x A: 2 planes, 3 products
 #include <algorithm>
-#include <cstdio>
 #include <cstdlib>
-#include <vector>
 
 #include "kernels.h"
 #include "mixed.h"
@@ -79,33 +77,6 @@ int sketch_planes() {
   return np;
 }
 
-// L2 policy of the sketch's tile loads: A (16 GB at the headline shape) streams through once per
-// 16 N tiles running side by side, Omega' (N l x n, 164 MB) is re-read by every row panel.
-// ISVD_GPU_SKETCH_L2 = "a,b" (0 normal, 1 evict-first, 2 evict-last) overrides the default.
-// Row panels of a device-resident A whose plane split overlaps the sketch of the previous panel
-// (1: split all rows, then one sketch launch).  ISVD_GPU_SKETCH_PANELS overrides the default.
-static int sketch_overlap_panels() {
-  static const int np = [] {
-    const char *e = getenv("ISVD_GPU_SKETCH_PANELS");
-    const int v = e ? atoi(e) : 1;
-    return v >= 1 && v <= 64 ? v : 1;
-  }();
-  return np;
-}
-
-static void sketch_l2_hints(UmmaGemm &g) {
-  static int h[2] = {-1, -1};
-  if (h[0] < 0) {
-    h[0] = 0;
-    h[1] = 0;
-    if (const char *e = getenv("ISVD_GPU_SKETCH_L2")) {
-      if (sscanf(e, "%d,%d", &h[0], &h[1]) != 2 || h[0] < 0 || h[0] > 2 || h[1] < 0 || h[1] > 2) h[0] = h[1] = 0;
-    }
-  }
-  g.l2_a = h[0];
-  g.l2_b = h[1];
-}
-
 // Sketch Y = A Omega with A processed in row panels: each panel is split into A's bf16 planes
 // (kept for the postprocess) and multiplied by Omega' on the tensor cores.  When A is in host
 // memory, panel p + 1 is copied to the device on the copy stream while panel p is split and
@@ -154,53 +125,7 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
   g.status = c.status;
   g.chunk_k = 512;  // 5e-7 relative tensor-core chain error per chunk, below the 2^-17 split level
   g.tag = "sketch";
-  sketch_l2_hints(g);
-  const int overlap = sketch_overlap_panels();
-  if (a_dev && overlap > 1 && m >= 128LL * overlap) {
-    // A on the device, split while the sketch runs: the rows form `overlap` panels (multiples of
-    // 128 rows); every panel's split is enqueued on the copy stream and each panel's sketch launch
-    // on c.st waits only for its own split, so that panel p + 1 is split (HBM-bound, 40 registers
-    // a thread: its CTAs fit beside a sketch CTA on an SM) while panel p is multiplied
-    Runtime &rt = Runtime::get();
-    const long long Pp = ((m + overlap - 1) / overlap + 127) / 128 * 128;
-    std::vector<cudaEvent_t> done;
-    cudaEvent_t start = nullptr;
-    auto destroy = [&] {
-      for (cudaEvent_t e : done) cudaEventDestroy(e);
-      if (start) cudaEventDestroy(start);
-    };
-    try {
-      CK(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
-      CK(cudaEventRecord(start, c.st));  // the plane buffer (allocated and padded on c.st) is ready
-      CK(cudaStreamWaitEvent(rt.copy_stream, start, 0));
-      for (long long r0 = 0; r0 < m; r0 += Pp) {
-        const long long rows = std::min<long long>(Pp, m - r0);
-        __nv_bfloat16 *dst = mc->buf.p + (size_t)r0 * ld;
-        if (ordera == 'R') split_rows<T>(a + r0 * lda, lda, 1, rows, n, na, false, dst, ld, ps, rt.copy_stream);
-        else split_rows<T>(a + r0, lda, 1, n, rows, na, true, dst, ld, ps, rt.copy_stream);
-        done.push_back(nullptr);
-        CK(cudaEventCreateWithFlags(&done.back(), cudaEventDisableTiming));
-        CK(cudaEventRecord(done.back(), rt.copy_stream));
-      }
-      int p = 0;
-      for (long long r0 = 0; r0 < m; r0 += Pp, ++p) {
-        CK(cudaStreamWaitEvent(c.st, done[p], 0));
-        Planes pp = all;
-        pp.ptr = mc->buf.p + (size_t)r0 * ld;
-        pp.rows = std::min<long long>(Pp, m - r0);
-        g.M = (int)pp.rows;
-        g.A = pp;
-        g.C = y + r0 * ldy;
-        umma_gemm(g, c.st);
-      }
-    } catch (...) {
-      cudaStreamSynchronize(rt.copy_stream);
-      cudaStreamSynchronize(c.st);
-      destroy();
-      throw;
-    }
-    destroy();
-  } else if (a_dev) {
+  if (a_dev) {
     // A on the device: split every row, then one launch over all m rows (no per-panel wave tail)
     for (long long r0 = 0; r0 < m; r0 += P) {
       const long long rows = std::min<long long>(P, m - r0);

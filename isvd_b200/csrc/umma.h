@@ -44,9 +44,6 @@ struct UmmaGemm {
   int chunk_k = 0;     // K depth of one tensor-memory accumulation chunk (0: 128)
   const char *tag = "gemm";  // name under which launches are recorded when profiling is enabled
   int *status = nullptr;     // device status word: set, the call returns without a host synchronisation
-  // L2 eviction priority of the A and B tile loads (0 normal, 1 evict-first, 2 evict-last): an
-  // operand that many CTAs re-read while a larger one streams through once can be kept in L2
-  int l2_a = 0, l2_b = 0;
 };
 
 // Geometry of a plane buffer for a rows x cols matrix: ld = cols rounded up to 64, rows padded to
