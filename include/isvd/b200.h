@@ -84,7 +84,9 @@ int isvd_dIsvd_ex(
 
 /* Stream on which the library enqueues its work (a cudaStream_t of the current device; NULL
  * restores the library's own non-blocking stream).  Every entry point still returns only after
- * its work on that stream has completed. */
+ * its work on that stream has completed.  Device-memory operands are read in that stream's order:
+ * when another stream produced them, either that work has completed before the call (e.g.
+ * cudaStreamSynchronize) or the library runs on the producing stream (isvd_gpu_set_stream). */
 void  isvd_gpu_set_stream( void *stream );
 void *isvd_gpu_get_stream( void );
 

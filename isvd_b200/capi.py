@@ -44,12 +44,17 @@ _CH = ctypes.c_char
 
 
 def ptr(x):
-    """Raw address of a NumPy array / CUDA tensor / int / None."""
+    """Raw address of a NumPy array / CUDA tensor / int / None.  A CUDA tensor's producing work on
+    torch's current stream is completed first: the library reads device operands in the order of
+    its own stream, which need not be torch's (isvd_gpu_set_stream)."""
     if x is None:
         return None
     if isinstance(x, int):
         return x
     if hasattr(x, "data_ptr"):
+        if getattr(x, "is_cuda", False):
+            import torch
+            torch.cuda.current_stream(x.device).synchronize()
         return x.data_ptr()
     if isinstance(x, np.ndarray):
         return x.ctypes.data

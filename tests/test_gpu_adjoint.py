@@ -34,6 +34,9 @@ def adjoint(lib, a, s, u, v, ds=None, du=None, dv=None, cg_iters=500, tol=1e-13,
         da = np.zeros_like(a)
     lda = n if ordera == b"R" else m
     its = ctypes.c_int(0)
+    if hasattr(a, "data_ptr"):  # the operands were produced on torch's stream; the library uses its own
+        import torch
+        torch.cuda.synchronize()
     st = _adjoint_fn(lib, x)(m, n, k, ordera, ptr(a), lda, ptr(s), ptr(u), k, ptr(v), k, ptr(ds), ptr(du), k, ptr(dv),
                              k, ptr(da), lda, cg_iters, tol, ctypes.byref(its))
     assert st == 0, lib.last_error()
