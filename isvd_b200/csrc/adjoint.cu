@@ -195,6 +195,7 @@ struct AProducts {
   long long lda;
   bool mixed;
   PlaneBuf ap;
+  PlaneBuf xpn, xpm;  // the other operand's planes (n or m rows), kept across products
   AProducts(const StageCtx &c_, int m_, int n_, char ordera_, const T *a_, long long lda_)
       : c(c_), m(m_), n(n_), ordera(ordera_), a(a_), lda(lda_),
         mixed(c_.precision == kMixed && sizeof(T) == sizeof(float)) {
@@ -209,7 +210,7 @@ struct AProducts {
       return;
     }
     UmmaGemm g;
-    PlaneBuf xp;
+    PlaneBuf &xp = transpose ? xpm : xpn;
     if (!transpose) {  // Y (m x k) = A X: A planes M x K (K-major), X' planes N x K
       make_planes<T>(xp, X, k, n, k, 3, true, c.st);
       g.M = m; g.N = k; g.K = n;
@@ -309,6 +310,19 @@ int complement_cg(const StageCtx &c, AProducts<T> &A, int k, const T *u, long lo
     coldot<T>(st, y.b, y.b, y.rows, k, y.part.p, y.bb);
     coldot<T>(st, y.r.p, y.r.p, y.rows, k, y.part.p, y.rr);
   }
+  // One CG iteration of one system; after two eager iterations (which size every buffer) each
+  // system's iteration is captured as a CUDA graph and replayed.
+  auto body = [&](CgSystem<T> &y) {
+    apply(y, y.p.p, y.q.p);
+    coldot<T>(st, y.p.p, y.q.p, y.rows, k, y.part.p, y.pq.p);
+    cg_step1_kernel<T><<<egrid(y.rows * k), 256, 0, st>>>(y.x, y.r.p, y.p.p, y.q.p, y.rows, k, y.rr, y.pq.p);
+    KLAUNCHED();
+    coldot<T>(st, y.r.p, y.r.p, y.rows, k, y.part.p, y.rn.p);
+    cg_step2_kernel<T><<<egrid(y.rows * k), 256, 0, st>>>(y.p.p, y.r.p, y.rows, k, y.rr, y.rn.p);
+    KLAUNCHED();
+    CK(cudaMemcpyAsync(y.rr, y.rn.p, k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  };
+  GraphPair graphs(st);
   std::vector<double> h((size_t)4 * k);
   for (int it = 0; it < maxit; ++it) {
     CK(cudaMemcpyAsync(h.data(), scal.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -325,17 +339,12 @@ int complement_cg(const StageCtx &c, AProducts<T> &A, int k, const T *u, long lo
       any = any || y.active;
     }
     if (!any) break;
-    for (CgSystem<T> &y : sys) {
+    for (int i = 0; i < 2; ++i) {
+      CgSystem<T> &y = sys[i];
       if (!y.active) continue;
       ++y.its;
-      apply(y, y.p.p, y.q.p);
-      coldot<T>(st, y.p.p, y.q.p, y.rows, k, y.part.p, y.pq.p);
-      cg_step1_kernel<T><<<egrid(y.rows * k), 256, 0, st>>>(y.x, y.r.p, y.p.p, y.q.p, y.rows, k, y.rr, y.pq.p);
-      KLAUNCHED();
-      coldot<T>(st, y.r.p, y.r.p, y.rows, k, y.part.p, y.rn.p);
-      cg_step2_kernel<T><<<egrid(y.rows * k), 256, 0, st>>>(y.p.p, y.r.p, y.rows, k, y.rr, y.rn.p);
-      KLAUNCHED();
-      CK(cudaMemcpyAsync(y.rr, y.rn.p, k * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      if (graphs.usable && it >= 2) graphs.run(i, [&] { body(y); });
+      else body(y);
     }
   }
   return sys[0].its + sys[1].its;
