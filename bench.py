@@ -352,6 +352,9 @@ def square50k_main(args):
                       "mixed_wy_iterations": wy_mixed, "fp64_ms": fp64_ms,
                       "fp64_stage_ms": [1e3 * t for t in times64], "fp64_wy_iterations": int(retv64[2][0]),
                       "sigma_rel_err_max": err, "steps": args.steps, "warmup": args.warmup,
+                      "note": "on this input Wen-Yin's stopping point (mu < tol^2) depends on rounding: the "
+                              "reference's own result moves by 1.2e-4 in sigma (219 -> 157 iterations) under a "
+                              "last-bit change of Y, so MIXED and FP64 differ by that order as well",
                       "clocks": clk.summary()}), flush=True)
 
 

@@ -155,12 +155,15 @@ __global__ void __launch_bounds__(kColdotThreads)
   }
 }
 
+// One warp per column: lane j adds the slices j, j + 32, ... in order, then a fixed shuffle tree.
 __global__ void coldot_final_kernel(const double *__restrict__ partial, int nb, int k, double *__restrict__ out) {
-  for (int c = threadIdx.x; c < k; c += blockDim.x) {
-    double s = 0.0;
-    for (int b = 0; b < nb; ++b) s += partial[(size_t)b * k + c];
-    out[c] = s;
-  }
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  if (c >= k) return;  // whole warps leave together
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += partial[(size_t)b * k + c];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) out[c] = s;
 }
 
 inline int egrid(long long n) {
@@ -180,7 +183,7 @@ void coldot(cudaStream_t st, const T *x, const T *y, long long rows, int k, doub
   const int nb = (int)std::max<long long>(1, std::min<long long>(kColdotBlocks, (rows + 63) / 64));
   coldot_kernel<T><<<nb, kColdotThreads, kColdotThreads * sizeof(double), st>>>(x, y, rows, k, partial);
   KLAUNCHED();
-  coldot_final_kernel<<<1, 128, 0, st>>>(partial, nb, k, out);
+  coldot_final_kernel<<<(k + 7) / 8, 256, 0, st>>>(partial, nb, k, out);
   KLAUNCHED();
 }
 

@@ -128,29 +128,41 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// C = alpha * (sum of the split partials) + beta * C.  Eight lanes per output: lane u adds the
+// partials of splits u, u + 8, u + 16, ... in increasing order (eight loads in flight per output
+// across the lanes, several outputs per warp), then the eight sums are combined by shuffles as
+// ((s0 + s1) + (s2 + s3)) + ((s4 + s5) + (s6 + s7)) -- a fixed order, the same in every launch.
 template <class T, class Tout>
 __global__ void splitk_reduce_kernel(const Gemm<T, Tout> g, const int splits, const T *__restrict__ partial) {
   const long long MN = (long long)g.M * g.N;
   const long long total = MN * g.batch;
-  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
-       e += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(e / MN);
-    const long long r = e - (long long)b * MN;
-    const int gm = (int)(r / g.N), gn = (int)(r - (long long)gm * g.N);
-    const T *p = partial + ((long long)b * splits) * MN + r;
-    // eight independent partial sums, so that eight loads are in flight
-    double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    int sp = 0;
-    for (; sp + 8 <= splits; sp += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; ++u) acc[u] += (double)p[(long long)(sp + u) * MN];
+  const int u = threadIdx.x & 7;
+  const long long groups0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const long long gstride = ((long long)gridDim.x * blockDim.x) >> 3;
+  // every lane of a warp runs the same number of loop trips (the shuffles need all 32)
+  const long long trips = (total + gstride - 1) / gstride;
+  for (long long t = 0; t < trips; ++t) {
+    const long long e = groups0 + t * gstride;
+    const bool live = e < total;
+    double acc = 0.0;
+    long long r = 0;
+    int b = 0;
+    if (live) {
+      b = (int)(e / MN);
+      r = e - (long long)b * MN;
+      const T *p = partial + ((long long)b * splits) * MN + r;
+      for (int sp = u; sp < splits; sp += 8) acc += (double)p[(long long)sp * MN];
     }
-    for (int u = 0; sp < splits; ++sp, ++u) acc[u] += (double)p[(long long)sp * MN];
-    const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
-    Tout *c = g.C + (long long)b * g.c_bs + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
-    double v = g.alpha * s;
-    if (g.beta != 0.0) v += g.beta * (double)(*c);
-    *c = (Tout)v;
+    acc += __shfl_down_sync(0xffffffffu, acc, 1);
+    acc += __shfl_down_sync(0xffffffffu, acc, 2);
+    acc += __shfl_down_sync(0xffffffffu, acc, 4);
+    if (live && u == 0) {
+      const int gm = (int)(r / g.N), gn = (int)(r - (long long)gm * g.N);
+      Tout *c = g.C + (long long)b * g.c_bs + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+      double v = g.alpha * acc;
+      if (g.beta != 0.0) v += g.beta * (double)(*c);
+      *c = (Tout)v;
+    }
   }
 }
 
@@ -188,7 +200,7 @@ void launch(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, cudaStream_t st) {
 #undef ISVD_GEMM_CASE
   if (splits > 1) {
     const long long total = (long long)g.M * g.N * g.batch;
-    int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * rt.num_sms);
+    int blocks = (int)std::min<long long>((8 * total + 255) / 256, 16LL * rt.num_sms);  // 8 lanes per output
     splitk_reduce_kernel<T, Tout><<<blocks, 256, 0, st>>>(g, splits, part.p);
     KLAUNCHED();
   }
@@ -231,7 +243,7 @@ void launch_fixed(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, int sms, T *part
 #undef ISVD_GEMM_CASE
   if (splits > 1) {
     const long long total = (long long)g.M * g.N * g.batch;
-    int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * sms);
+    int blocks = (int)std::min<long long>((8 * total + 255) / 256, 16LL * sms);  // 8 lanes per output
     splitk_reduce_kernel<T, Tout><<<blocks, 256, 0, st>>>(g, splits, part);
     KLAUNCHED();
   }
@@ -241,7 +253,7 @@ void launch_fixed(const Gemm<T, Tout> &g, bool a_kc, bool b_nc, int sms, T *part
 
 void splitk_reduce(const Gemm<double, double> &g, int splits, const double *partial, cudaStream_t st) {
   const long long total = (long long)g.M * g.N * g.batch;
-  const int blocks = (int)std::min<long long>((total + 255) / 256, 8LL * Runtime::get().num_sms);
+  const int blocks = (int)std::min<long long>((8 * total + 255) / 256, 16LL * Runtime::get().num_sms);
   splitk_reduce_kernel<double, double><<<blocks, 256, 0, st>>>(g, splits, partial);
   KLAUNCHED();
 }

@@ -1284,6 +1284,9 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
     fail(kErrUnsupported, "tcgen05 GEMM: MN-major A needs MN-major B");
   } else if (bmn) {
     launch_t<128, 64, false, true>(g, st, status);
+  } else if (g.N <= 64) {
+    // narrow outputs (N <= 64, e.g. products with k or l columns): 64-wide tiles, no half-empty MMAs
+    launch_t<64, 64, false, false>(g, st, status);
   } else if (small_n) {
     // six or more planes: 32-deep k-blocks give four pipeline stages instead of two, which pays
     // when there are many tiles; for a few split-K tiles (the Kolmogorov-Nagumo G B product,
