@@ -290,12 +290,12 @@ int complement_cg(const StageCtx &c, AProducts<T> &A, int k, const T *u, long lo
     y.active = maxit > 0;
   }
   if (maxit <= 0 || (!sys[0].active && !sys[1].active)) return 0;
-  // op(X) = X S^2 - P_perp A_ Q_perp A_' P_perp X,  A_ = A (left) or A' (right)
+  // op(X) = X S^2 - P_perp A_ Q_perp A_' X,  A_ = A (left) or A' (right).  Every X this is
+  // applied to (b S^-2, the CG directions) lies in the complement of P already (b does, and op
+  // ends with P_perp), so the projection before A_' is left out: P_perp A_' X = A_' X - ... would
+  // only remove rounding-level components, which the final P_perp removes from the result.
   auto apply = [&](CgSystem<T> &y, const T *X, T *Y) {
-    const size_t rk = (size_t)y.rows * k;
-    CK(cudaMemcpyAsync(y.z.p, X, rk * sizeof(T), cudaMemcpyDeviceToDevice, st));
-    project_out<T>(st, y.rows, k, y.P, y.ldp, y.z.p, y.tk.p);
-    A.mul(y.left, k, y.z.p, y.w.p);
+    A.mul(y.left, k, X, y.w.p);
     project_out<T>(st, y.other, k, y.Qb, y.ldq, y.w.p, y.tk.p);
     A.mul(!y.left, k, y.w.p, y.z.p);
     project_out<T>(st, y.rows, k, y.P, y.ldp, y.z.p, y.tk.p);
