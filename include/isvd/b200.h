@@ -204,8 +204,10 @@ int isvd_dMtxWrite( const char *path, const isvd_int_t m, const isvd_int_t n, co
  *     this rank's rows of A, yst and qt, and exchange through fn: the N block Grams (Gramian
  *     orthogonalization; each CholeskyQR pass and the top rows for the sign rule of the
  *     tall-skinny QR), G = Qs'Qs (KN, WY: one exchange per solve
- *     instead of two per iteration; every rank then runs the same iterations on the same G) and
- *     Z = A'Qbar (Gramian postprocessing);
+ *     instead of two per iteration; every rank then runs the same iterations on the same G), the
+ *     products Q(i)'Q(i+h) of each level of the hierarchical reduction, Z = A'Qbar (Gramian,
+ *     tall-skinny QR and symmetric postprocessing; every rank then factors the same Z) and the
+ *     l x l W = Qbar'AQbar (symmetric postprocessing);
  *   - outputs as the reference's: ut_root = -1 leaves this rank's rows of U in ut, ut_root >= 0
  *     gathers all m rows on that rank; vt_root = -1 leaves this rank's column block of V
  *     (rows [colidxbegin, colidxend)) in vt, vt_root >= 0 all n rows on that rank (the other
@@ -214,8 +216,8 @@ int isvd_dMtxWrite( const char *path, const isvd_int_t m, const isvd_int_t n, co
  *     ISVD_GPU_DTYPE_F64) at buf over the ranks, in place.  on_device = 1: buf is device memory
  *     and fn enqueues the reduction on `stream` (a cudaStream_t); on_device = 0: buf is pinned host
  *     memory (the library copies through it and synchronises around the call);
- *   - with nranks > 1, dista 'C', HR integration, TS / SY postprocessing and the postprocessing
- *     stage called on its own return ISVD_GPU_ERROR_UNSUPPORTED.
+ *   - with nranks > 1, dista 'C' and the postprocessing stage called on its own return
+ *     ISVD_GPU_ERROR_UNSUPPORTED.
  * nranks = 1 or fn = NULL returns to single-process execution.  Every rank must make the same
  * calls in the same order. */
 #define ISVD_GPU_DTYPE_F32 0

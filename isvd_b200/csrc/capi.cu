@@ -509,12 +509,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   const bool root = p.mpi_rank == p.mpi_root;
   // several ranks (isvd_gpu_set_allreduce): this rank holds rows [rowidxbegin, rowidxend) of A
   const bool multi = p.mpi_size > 1;
-  if (multi) {
-    if (dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
-    if (bi == "HR" || bp != "GR")
-      fail(kErrUnsupported, "several ranks: Gramian or TS orthogonalization, KN or WY integration and Gramian "
-                            "postprocessing only");
-  }
+  if (multi && dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
   const int ml = multi ? (int)p.nrow_proc : m;  // rows of A held here
   if (stream && root) {
     const char *tn = TypeName<T>::name;
@@ -538,7 +533,10 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   cudaStream_t st = c.sc.st;
   MixedCache mcache;  // A's bf16 planes, shared by the sketch and the postprocess
   c.sc.cache = &mcache;
-  if (multi) c.sc.m_total = m;
+  if (multi) {
+    c.sc.m_total = m;
+    c.sc.row_begin = p.rowidxbegin;
+  }
   StageTimer tm;
   auto progress = [&](const char *what) {
     if (stream && root) { fprintf(stream, "%s", what); fflush(stream); }
@@ -627,7 +625,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   progress("Postprocessing ................ ");
   View<T> S, U, V;
   S.bind(s, l, 1, l, false, st);
-  if (bp == "SY") {
+  if (bp == "SY" && !multi) {
     const bool wu = ut_root >= -1 || vt_root >= -1;
     T *u = (ut_root >= -1) ? ut : vt;
     const isvd_int_t ld = (ut_root >= -1) ? ldut : ldvt;
@@ -645,40 +643,56 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
       sync();
     }
   } else if (multi) {
-    // row blocks: U rows of this rank; V (all n rows) is the same on every rank
-    const bool wu = ut_root >= -1, wv = vt_root >= -1;
+    // row blocks: U rows of this rank; V (all n rows) is the same on every rank.  Symmetric: U and
+    // V are the same matrix (reference @x@_postprocess_symmetric.c:101-104, 170-191)
+    const bool sy = bp == "SY";
+    const bool wu = ut_root >= -1 || (sy && vt_root >= -1), wv = !sy && vt_root >= -1;
+    const int vcols = (bp == "TS") ? l : k;  // TS: all l columns of V (@x@_postprocess_tall_skinny_qr.c:286)
     DBuf<T> Ul((size_t)ml * l), Vf((size_t)n * l);
-    post_gramian_dev<T>(c.sc, ml, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, Ul.p, l, Vf.p, l, wu, wv);
+    if (bp == "GR")
+      post_gramian_dev<T>(c.sc, ml, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, Ul.p, l, Vf.p, l, wu, wv);
+    else if (bp == "TS")
+      post_tsqr_dev<T>(c.sc, ml, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, Ul.p, l, Vf.p, l, wu, wv);
+    else
+      post_symmetric_dev<T>(c.sc, ml, n, k, l, ordera_, a_use, lda, Q.p, l, S.d, Ul.p, l, wu);
     tm.mark(4, st);
     S.back(st);
-    const bool me_u = ut_root < 0 || ut_root != p.mpi_rank;  // this rank's rows only
-    if (wu && me_u) {
-      U.bind(ut, k, ml, ldut, false, st);
-      CK(cudaMemcpy2DAsync(U.d, ldut * sizeof(T), Ul.p, l * sizeof(T), k * sizeof(T), ml, cudaMemcpyDeviceToDevice,
-                           st));
-      U.back(st, k);
-    }
-    if (ut_root >= 0) {  // gather (reference MPI_Gather, @x@_postprocess_gramian.c:162-165): a sum of
-      DBuf<T> Ug((size_t)m * l);  // zero-padded copies of the ranks' rows
-      CK(cudaMemsetAsync(Ug.p, 0, (size_t)m * l * sizeof(T), st));
-      CK(cudaMemcpyAsync(Ug.p + (size_t)p.rowidxbegin * l, Ul.p, (size_t)ml * l * sizeof(T), cudaMemcpyDeviceToDevice,
-                         st));
-      allreduce_sum(Ug.p, (size_t)m * l, st);
-      if (ut_root == p.mpi_rank) {
-        U.bind(ut, k, m, ldut, false, st);
-        CK(cudaMemcpy2DAsync(U.d, ldut * sizeof(T), Ug.p, l * sizeof(T), k * sizeof(T), m, cudaMemcpyDeviceToDevice,
+    // U: this rank's rows, and all rows at the root (reference MPI_Gather,
+    // @x@_postprocess_gramian.c:162-165) through a sum of zero-padded copies of the ranks' rows
+    auto emit_u = [&](T *out, isvd_int_t ld, mpi_int_t root) {
+      View<T> Uo;
+      if (root < 0 || root != p.mpi_rank) {  // this rank's rows only
+        Uo.bind(out, k, ml, ld, false, st);
+        CK(cudaMemcpy2DAsync(Uo.d, ld * sizeof(T), Ul.p, l * sizeof(T), k * sizeof(T), ml, cudaMemcpyDeviceToDevice,
                              st));
-        U.back(st, k);
+        Uo.back(st, k);
       }
-    }
+      if (root >= 0) {
+        DBuf<T> Ug((size_t)m * l);
+        CK(cudaMemsetAsync(Ug.p, 0, (size_t)m * l * sizeof(T), st));
+        CK(cudaMemcpyAsync(Ug.p + (size_t)p.rowidxbegin * l, Ul.p, (size_t)ml * l * sizeof(T),
+                           cudaMemcpyDeviceToDevice, st));
+        allreduce_sum(Ug.p, (size_t)m * l, st);
+        if (root == p.mpi_rank) {
+          View<T> Ua;
+          Ua.bind(out, k, m, ld, false, st);
+          CK(cudaMemcpy2DAsync(Ua.d, ld * sizeof(T), Ug.p, l * sizeof(T), k * sizeof(T), m, cudaMemcpyDeviceToDevice,
+                               st));
+          Ua.back(st, k);
+        }
+      }
+      sync();
+    };
+    if (ut_root >= -1) emit_u(ut, ldut, ut_root);
+    if (sy && vt_root >= -1) emit_u(vt, ldvt, vt_root);
     if (wv) {  // this rank's column block; all rows at the root (reference MPI_Gather, :176-183)
       const bool all = vt_root >= 0 && vt_root == p.mpi_rank;
       const long long v0 = all ? 0 : (long long)p.colidxbegin;
       const long long vn = all ? (long long)n : (long long)p.ncol_proc;
-      V.bind(vt, k, vn, ldvt, false, st);
-      CK(cudaMemcpy2DAsync(V.d, ldvt * sizeof(T), Vf.p + v0 * l, l * sizeof(T), k * sizeof(T), vn,
+      V.bind(vt, vcols, vn, ldvt, false, st);
+      CK(cudaMemcpy2DAsync(V.d, ldvt * sizeof(T), Vf.p + v0 * l, l * sizeof(T), vcols * sizeof(T), vn,
                            cudaMemcpyDeviceToDevice, st));
-      V.back(st, k);
+      V.back(st, vcols);
     }
   } else {
     const bool wu = ut_root >= -1, wv = vt_root >= -1;

@@ -346,7 +346,6 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
 // Hierarchical reduction (reference @x@_integrate_hierarchical_reduction.c:90-130).
 template <class T>
 void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long ldq, T *qt, long long ldqt) {
-  if (collective().nranks > 1) fail(kErrUnsupported, "hierarchical reduction: one rank only");
   const size_t ll = (size_t)l * l;
   const int hmax = N / 2 > 0 ? N / 2 : 1;
   DBuf<double> Bs(hmax * ll), W(hmax * ll), Vv(hmax * ll), s((size_t)hmax * l);
@@ -361,7 +360,8 @@ void integrate_hr_dev(const StageCtx &c, int m, int l, int N, T *qs, long long l
       g.C = Bs.p; g.c_rs = l; g.c_cs = 1; g.c_bs = ll;
       gemm(g, c.st);
     }
-    // svd(B(i)) = W S T'
+    allreduce_sum(Bs.p, (size_t)h * ll, c.st);  // row blocks on several ranks: a sum (:100)
+    // svd(B(i)) = W S T' (the same B on every rank: the same factors)
     svd_jacobi_batched(l, h, Bs.p, W.p, s.p, Vv.p, c.status, c.st);
     // Q(i) := (Q(i) W + Q(i+h) T) / sqrt(2 (1 + s))
     scale_cols_batched<double, T>(W.p, l, Wt.p, l, (long long)h * l, l, l, s.p, kScaleHr, c.st);
@@ -446,23 +446,26 @@ void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera
 }
 
 // Symmetric postprocessing (reference @x@_postprocess_symmetric.c:139-157): W = Qbar' A Qbar,
-// syev (ascending), U = Qbar W[:, :k].
+// syev (ascending), U = Qbar W[:, :k].  Row blocks on several ranks (this rank: rows
+// [row_begin, row_begin + m) of A and Qbar, n = all rows): Z = A' Qbar summed over the ranks, then
+// W = sum of Z(own rows)' Qbar_j (the reference's MPI_Allreduce of W, :147).
 template <class T>
 void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                         const T *qt, long long ldqt, T *s, T *ut, long long ldut, bool wu) {
-  if (collective().nranks > 1) fail(kErrUnsupported, "symmetric postprocessing: one rank only");
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l);
   project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
+  allreduce_sum(Z.p, (size_t)n * l, c.st);
   DBuf<double> W(ll), V(ll), w(l);
   {
     Gemm<T, double> g;
-    g.M = l; g.N = l; g.K = n;
-    g.A = Z.p; g.a_rs = 1; g.a_cs = l;
+    g.M = l; g.N = l; g.K = m;
+    g.A = Z.p + (size_t)c.row_begin * l; g.a_rs = 1; g.a_cs = l;
     g.B = qt; g.b_rs = ldqt; g.b_cs = 1;
     g.C = W.p; g.c_rs = l; g.c_cs = 1;
     gemm(g, c.st);
   }
+  allreduce_sum(W.p, ll, c.st);
   sym_eig_batched(l, 1, W.p, V.p, w.p, -1, false, c.status, c.st);
   copy2d<double, T>(w.p, 1, 1, s, 1, 1, l, 1, c.st);
   if (wu) {

@@ -22,8 +22,12 @@ struct StageCtx {
   // instead of the eigenbasis): set by the driver when the rest of the pipeline is basis-invariant
   bool chol_basis = false;
   // rows of the whole matrix when this process holds a row block of it (multi-rank; 0: the
-  // stage's own rows are all of them)
+  // stage's own rows are all of them), and the first of this process's rows
   long long m_total = 0;
+  long long row_begin = 0;
+  // the stage's matrix is whole and the same on every rank (an n x l factor formed after a sum over
+  // the ranks): no exchange between ranks, and every rank computes the same result
+  bool replicated = false;
   // out-of-core A: a host A is streamed through the device in row panels of this many rows by the
   // sketch and the projection (0: A is on the device, or copied there whole)
   long long a_panel_rows = 0;

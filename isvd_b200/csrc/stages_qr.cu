@@ -62,7 +62,8 @@ void complete_null_columns(const StageCtx &c, long long rows, int l, int N, T *&
                            long long &ldd, const int *mask) {
   const int Nl = N * l;
   const size_t ll = (size_t)l * l;
-  const uint64_t seed = 0x5EEDC0DEull + (uint64_t)collective().rank;  // each rank fills its own rows
+  // each rank fills its own rows (a replicated matrix: the same values on every rank)
+  const uint64_t seed = 0x5EEDC0DEull + (c.replicated ? 0 : (uint64_t)collective().rank);
   fill_null_columns<T>(src, lds, rows, Nl, mask, seed, 0, c.st);
   DBuf<int> perm((size_t)N * l);
   kept_first_perm(mask, l, N, perm.p, c.st);
@@ -75,7 +76,7 @@ void complete_null_columns(const StageCtx &c, long long rows, int l, int N, T *&
     g.B = src; g.b_rs = lds; g.b_cs = 1; g.b_bs = l;
     g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
     gemm(g, c.st);
-    allreduce_sum(W.p, N * ll, c.st);
+    if (!c.replicated) allreduce_sum(W.p, N * ll, c.st);
     chol_inv_batched(l, N, W.p, 1.0, 0.0, 0.0, l * unit_roundoff<T>(), X.p, 1.0, kCholFactor, c.status, c.st,
                      nullptr, nullptr, perm.p);
     copy2d<double, T>(X.p, l, 1, Xt.p, l, 1, (long long)N * l, l, c.st);
@@ -125,14 +126,14 @@ void cholqr3_blocks(const StageCtx &c, long long rows, int l, int N, T *y, long 
       g.C = W.p; g.c_rs = l; g.c_cs = 1; g.c_bs = (long long)ll;
       gemm(g, c.st);
     }
-    allreduce_sum(W.p, N * ll, c.st);  // row blocks on several ranks: the Grams are sums
+    if (!c.replicated) allreduce_sum(W.p, N * ll, c.st);  // row blocks on several ranks: the Grams are sums
     const double mrows = c.m_total > 0 ? (double)c.m_total : (double)rows;
     const double shift_rel = (pass == 0) ? (std::sqrt(mrows) + l + 1) * u : 0.0;
     const double piv_rel = (pass == 0) ? 0.0 : l * u;
     chol_inv_batched(l, N, W.p, 1.0, 0.0, shift_rel, piv_rel, X.p, 1.0, kCholFactor, c.status, c.st, nmask.p,
                      nmask.p + Nl);
     if (pass == 2) {
-      if (collective().nranks > 1) {
+      if (collective().nranks > 1 && !c.replicated) {
         // the sign rule reads the first l rows of each block, held by rank 0: every rank takes
         // them from a sum in which the other ranks contribute zeros
         DBuf<T> top((size_t)l * Nl);
@@ -361,20 +362,25 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   return res;
 }
 
-// Tall-skinny QR postprocessing (reference @x@_postprocess_tall_skinny_qr.c:195-294 at P = 1):
+// Tall-skinny QR postprocessing (reference @x@_postprocess_tall_skinny_qr.c:195-294):
 //   Z = A' Qbar;  Z' = L Qlq (gelqf, :199), i.e. Z = Qz R with L = R';  svd(L) = U_L S V_L';
 //   U = Qbar V_L[:, 0:k]  (:270);  V = Qz U_L'  (all l columns, :286);  s = S (l values).
 template <class T>
 void post_tsqr_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                    const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
                    bool wv) {
-  if (collective().nranks > 1) fail(kErrUnsupported, "tall-skinny QR postprocessing: one rank only");
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l), Qz((size_t)n * l);
   project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
+  // row blocks on several ranks: Z = sum of A_j' Qbar_j, whole on every rank, which then factors
+  // it as one rank would (the reference factors its row-distributed Z by a TSQR tree, :199-241;
+  // both give the QR factorization of the same Z, up to rounding and column signs)
+  allreduce_sum(Z.p, (size_t)n * l, c.st);
   CK(cudaMemcpyAsync(Qz.p, Z.p, (size_t)n * l * sizeof(T), cudaMemcpyDeviceToDevice, c.st));
   StageCtx cn = c;
   cn.precision = kNative;  // the n x l factorization: the stage's own type on CUDA cores
+  cn.replicated = true;
+  cn.m_total = 0;
   cholqr3_blocks<T>(cn, n, l, 1, Qz.p, l);
   DBuf<double> R(ll), L(ll), Ul(ll), Vl(ll), sv(l);
   {  // R = Qz' Z (upper triangular to rounding)

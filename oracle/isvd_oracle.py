@@ -172,18 +172,21 @@ def integrate_wen_yin(qs, l, N, maxit=256, tol=1e-3, tau0=1.0, taumax=1e14, taum
     return qp, it, float(mu)
 
 
-def integrate_hierarchical_reduction(qs, l, N):
+def integrate_hierarchical_reduction(qs, l, N, allreduce=None):
     """Hierarchical reduction, core/stage/@x@_integrate_hierarchical_reduction.c:90-130.
 
-    Q(i) := (Q(i) W + Q(i+h) T) / sqrt(2 (1 + s)) with B(i) = Q(i)' Q(i+h) = W S T'.
+    Q(i) := (Q(i) W + Q(i+h) T) / sqrt(2 (1 + s)) with B(i) = Q(i)' Q(i+h) = W S T'; with row
+    blocks the h products B(i) of a level are summed over the ranks in one reduction (:100).
     Works on a copy; the reference overwrites yst (the returned ``qs_out``)."""
+    red = allreduce or _local
     q = np.array(qs, np.float64)
     h2 = N
     while h2 > 1:
         h = h2 // 2
+        bs = red(np.stack([q[:, i * l:(i + 1) * l].T @ q[:, (i + h) * l:(i + h + 1) * l] for i in range(h)]))
         for i in range(h):
             qi, qih = q[:, i * l:(i + 1) * l], q[:, (i + h) * l:(i + h + 1) * l]
-            w, s, tt = np.linalg.svd(qi.T @ qih)
+            w, s, tt = np.linalg.svd(bs[i])
             q[:, i * l:(i + 1) * l] = (qi @ w + qih @ tt.T) / np.sqrt(2.0 * (1.0 + s))
         h2 = (h2 + 1) // 2
     return q[:, :l].copy(), q
@@ -257,17 +260,20 @@ def row_block(m, P, rank):
     return min(rank * each, m), min(rank * each + each, m)
 
 
-def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None):
-    """The Gramian / KN-or-WY / Gramian driver on one rank's rows of a row-distributed A
-    (dista 'R'), with every reduction over the ranks done by ``allreduce(x)`` (an in-place sum of a
-    float64 array, the reference's MPI_Allreduce with MPI_SUM):
+def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None, alg_p="GR", row_begin=0):
+    """The Gramian / KN, WY or HR / GR, TS or SY driver on one rank's rows [row_begin, ...) of a
+    row-distributed A (dista 'R'), with every reduction over the ranks done by ``allreduce(x)`` (an
+    in-place sum of a float64 array, the reference's MPI_Allreduce with MPI_SUM):
       * orthogonalization W_i = sum_ranks Y_i' Y_i, core/stage/@x@_orthogonalize_gramian.c:82-85;
       * integration as the reference's integrate stages with ``allreduce`` (Bc, Bgc and, for WY,
-        the step-size sums);
+        the step-size sums; for HR the products B(i) of each level);
       * postprocessing Z = A' Qbar (projectBlockRow, core/stage/@x@_postprocess.h:96-162, whose
         MPI_Reduce_scatter_block leaves each rank its column block of the sum; here every rank keeps
-        the whole sum) and W = Z' Z (core/stage/@x@_postprocess_gramian.c:145-146).
-    Returns (s, U rows of this rank, V (all n rows), iterations, error or mu)."""
+        the whole sum), then GR: W = Z' Z (core/stage/@x@_postprocess_gramian.c:145-146); TS: the
+        QR factorization of the whole Z on every rank (the reference's TSQR tree over the ranks,
+        @x@_postprocess_tall_skinny_qr.c:199-241, factors the same Z); SY: W = sum_ranks of
+        Z(own rows)' Qbar_j (@x@_postprocess_symmetric.c:146-147).
+    Returns (s, U rows of this rank, V (all n rows; SY: None), iterations, error or mu)."""
     a_rows = np.asarray(a_rows, np.float64)
     l = k + p
     y = a_rows @ np.asarray(omega, np.float64)
@@ -280,9 +286,19 @@ def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None):
     argv_i = dict(argv_i or {})
     if alg_i == "KN":
         qp, it, err = integrate_kolmogorov_nagumo(q, l, N, allreduce=allreduce, **argv_i)
-    else:
+    elif alg_i == "WY":
         qp, it, err = integrate_wen_yin(q, l, N, allreduce=allreduce, **argv_i)
+    else:
+        qp, it, err = integrate_hierarchical_reduction(q, l, N, allreduce=allreduce)[0], 0, 0.0
     z = allreduce(a_rows.T @ qp)
+    if alg_p == "TS":
+        qz, r = np.linalg.qr(z)
+        uu, s, vvt = np.linalg.svd(r.T)
+        return s, qp @ vvt.T[:, :k], qz @ uu.T, it, err
+    if alg_p == "SY":
+        w = allreduce(z[row_begin:row_begin + qp.shape[0]].T @ qp)
+        lam, ev = np.linalg.eigh(_sym_upper(w))
+        return lam, qp @ ev[:, :k], None, it, err
     w, s, _ = np.linalg.svd(z.T @ z)
     sig = np.sqrt(s)
     return sig, qp @ w[:, :k], (z @ w[:, :k]) / sig[:k], it, err

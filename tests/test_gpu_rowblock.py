@@ -1,6 +1,7 @@
 """Row blocks over two processes on one GPU, joined by a caller-supplied AllReduce
 (isvd_gpu_set_allreduce with a gloo host reduction): each process holds the rows
-[rowidxbegin, rowidxend) that isvd_createParam gives it, and the solve matches the one-process
+[rowidxbegin, rowidxend) that isvd_createParam gives it, and the solve -- every orthogonalization,
+integration and postprocessing selector -- matches the one-process
 solve of the whole matrix with the same Omega -- singular values within 1e-10 (FP64) / 1e-5
 (MIXED), the same iteration counts, U and V column angles within 1e-8 (FP64) / 1e-4 (MIXED), for
 the gathered outputs (ut_root = vt_root = 0) and for each rank's own blocks (roots -1).  The
@@ -76,10 +77,21 @@ def free_port():
 @pytest.mark.parametrize("x,precision,algs,on_device", [
     ("d", 0, ("GP", "GR", "KN", "GR"), False), ("s", 1, ("GP", "GR", "KN", "GR"), False),
     ("d", 0, ("GP", "TS", "WY", "GR"), False), ("s", 1, ("GP", "TS", "WY", "GR"), False),
-    ("d", 0, ("GP", "GR", "KN", "GR"), True), ("s", 1, ("GP", "TS", "KN", "GR"), True)])
+    ("d", 0, ("GP", "GR", "KN", "GR"), True), ("s", 1, ("GP", "TS", "KN", "GR"), True),
+    ("d", 0, ("GP", "GR", "HR", "GR"), False), ("s", 1, ("GP", "GR", "HR", "GR"), True),
+    ("d", 0, ("GP", "GR", "KN", "TS"), False), ("s", 1, ("GP", "TS", "KN", "TS"), True),
+    ("d", 0, ("GP", "GR", "KN", "SY"), False), ("s", 1, ("GP", "GR", "WY", "SY"), True)])
 def test_two_row_blocks_match_one_process(lib, oracle, x, precision, algs, on_device):
-    m, n, k, p, N = 1201, 700, 16, 8, 8
-    a = lowrank(m, n, 300, 0.97, 1e-6, 11)
+    """Every selector the driver takes with row blocks: GR or TS orthogonalization, KN, WY or HR
+    integration, GR, TS or SY postprocessing (SY: a symmetric A)."""
+    if algs[3] == "SY":
+        m = n = 700
+        a = lowrank(m, n, 300, 0.97, 1e-6, 11)
+        a = 0.5 * (a + a.T)
+    else:
+        m, n = 1201, 700
+        a = lowrank(m, n, 300, 0.97, 1e-6, 11)
+    k, p, N = 16, 8, 8
     om = np.random.default_rng(12).standard_normal((n, (k + p) * N))
     prm1 = lib.create_param(m, n, k, p, N)
     s1, u1, v1, r1 = solve(lib, x, prm1, a, om, k, p, N, algs, precision, -1, -1)
@@ -103,7 +115,7 @@ def test_two_row_blocks_match_one_process(lib, oracle, x, precision, algs, on_de
     for rank in (0, 1):
         (rb, re, cb, ce), own, gathered = out[rank]
         for res in (own, gathered):
-            assert np.abs(res[0].astype(np.float64) - s1).max() <= ts * s1.max()
+            assert np.abs(res[0].astype(np.float64) - s1).max() <= ts * np.abs(s1).max()
             assert abs(res[3][2][0] - r1[2][0]) <= it_tol
         uo = own[1][:, :k].astype(np.float64)
         vo = own[2][:, :k].astype(np.float64)

@@ -46,7 +46,7 @@ def test_set_allreduce_rejects_bad_ranks(lib):
     assert lib.create_param(10, 10, 2, 1, 2).mpi_size == 1
 
 
-def _rank(rank, port, a, om, k, p, N, alg, q):
+def _rank(rank, port, a, om, k, p, N, alg, alg_p, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     import sys
@@ -69,27 +69,31 @@ def _rank(rank, port, a, om, k, p, N, alg, q):
         f32 = np.arange(5, dtype=np.float32) * (rank + 1)
         fn(f32.ctypes.data, 5, 0, None, None)
         rb, re = orc.row_block(a.shape[0], 2, rank)
-        s, u, v, it, err = orc.isvd_row_block(a[rb:re], om, k, p, N, allreduce, alg_i=alg)
+        s, u, v, it, err = orc.isvd_row_block(a[rb:re], om, k, p, N, allreduce, alg_i=alg, alg_p=alg_p,
+                                              row_begin=rb)
         q.put((rank, (rb, re), s, u, v, it, count[0], f32))
         dist.destroy_process_group()
     except BaseException as e:
         q.put((rank, "error", repr(e), None, None, None, None, None))
 
 
-@pytest.mark.parametrize("alg", ["KN", "WY"])
-def test_exchange_algebra_over_gloo(oracle, alg):
+@pytest.mark.parametrize("alg,alg_p", [("KN", "GR"), ("WY", "GR"), ("HR", "GR"), ("KN", "TS"), ("KN", "SY")])
+def test_exchange_algebra_over_gloo(oracle, alg, alg_p):
     m, n, k, p, N = 301, 120, 6, 4, 5
     rng = np.random.default_rng(3)
     a = (np.linalg.qr(rng.standard_normal((m, 40)))[0] * 0.9 ** np.arange(40)) @ rng.standard_normal((40, n))
+    if alg_p == "SY":  # a symmetric A
+        a = a[:n] + a[:n].T
+        m = n
     om = rng.standard_normal((n, (k + p) * N))
-    whole = oracle.isvd(a, om, k, p, N, alg_i=alg)
+    whole = oracle.isvd(a, om, k, p, N, alg_i=alg, alg_p=alg_p)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
     port = s.getsockname()[1]
     s.close()
-    procs = [ctx.Process(target=_rank, args=(r, port, a, om, k, p, N, alg, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, port, a, om, k, p, N, alg, alg_p, q)) for r in range(2)]
     for pr in procs:
         pr.start()
     res = {}
@@ -104,12 +108,18 @@ def test_exchange_algebra_over_gloo(oracle, alg):
     for r in (0, 1):
         _, (rb, re), sr, ur, vr, it, calls, f32 = res[r]
         assert np.array_equal(f32, np.arange(5, dtype=np.float32) * 3)
-        # KN: the block Grams, Bc, one Bgc per iteration, Z; WY: also the first Bgc and the two
-        # step-size sums of every iteration but the last
-        expected = N + 1 + it + 1 if alg == "KN" else N + 2 + it + (it - 1) + 1
+        # the block Grams; KN: Bc, one Bgc per iteration; WY: also the first Bgc and the two
+        # step-size sums of every iteration but the last; HR: one sum per level; then Z (and for
+        # SY the l x l W)
+        levels, h2 = 0, N
+        while h2 > 1:
+            levels, h2 = levels + 1, (h2 + 1) // 2
+        integ = {"KN": 1 + it, "WY": 2 + it + (it - 1), "HR": levels}[alg]
+        expected = N + integ + (2 if alg_p == "SY" else 1)
         assert it == whole["iters"] and calls == expected
-        assert np.abs(sr - whole["s"]).max() <= 1e-12 * whole["s"].max()
-        assert oracle.column_angles(vr, whole["v"]).max() < 1e-10
+        assert np.abs(sr - whole["s"]).max() <= 1e-12 * np.abs(whole["s"]).max()
+        if alg_p != "SY":
+            assert oracle.column_angles(vr, whole["v"]).max() < 1e-10
     assert oracle.column_angles(u, whole["u"]).max() < 1e-10
 
 
