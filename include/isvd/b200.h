@@ -216,7 +216,11 @@ int isvd_dMtxWrite( const char *path, const isvd_int_t m, const isvd_int_t n, co
  *     ISVD_GPU_DTYPE_F64) at buf over the ranks, in place.  on_device = 1: buf is device memory
  *     and fn enqueues the reduction on `stream` (a cudaStream_t); on_device = 0: buf is pinned host
  *     memory (the library copies through it and synchronises around the call);
- *   - with nranks > 1, dista 'C' and the postprocessing stage called on its own return
+ *   - with dista 'C' (column blocks) each rank passes all m rows of its columns
+ *     [colidxbegin, colidxend) of A (and, to the _ex driver, all n rows of Omega): Y = sum of the
+ *     ranks' A_j Omega_j is exchanged once (m x Nl) and each rank keeps its rows of Y; the
+ *     projection gathers Qbar (m x l) and Z (n x l) through fn as sums of zero-padded copies;
+ *   - with nranks > 1 the postprocessing stage called on its own returns
  *     ISVD_GPU_ERROR_UNSUPPORTED.
  * nranks = 1 or fn = NULL returns to single-process execution.  Every rank must make the same
  * calls in the same order. */

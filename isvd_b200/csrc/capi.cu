@@ -240,11 +240,13 @@ void sketch_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, is
   const char dista_ = arg2char("DISTA", dista, "CR");
   const char ordera_ = arg2char("ORDERA", ordera, "CR");
   require_single_rank(p);
-  if (p.mpi_size > 1 && dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
-  // several ranks: this rank's rows [rowidxbegin, rowidxend) of A and Y
+  // several ranks: row blocks hold rows [rowidxbegin, rowidxend) of A, column blocks (dista 'C') all
+  // rows and columns [colidxbegin, colidxend); either way this rank's rows of Y are returned
+  const bool colblk = p.mpi_size > 1 && dista_ == 'C';
   const int m = p.mpi_size > 1 ? (int)p.nrow_proc : (int)p.nrow, n = p.ncol, Nl = p.dim_sketch_total;
+  const int arows = colblk ? (int)p.nrow : m, acols = colblk ? (int)p.ncol_proc : n;
   if (dista_ == 'C') {
-    REQUIRE(ordera_ == 'C' ? lda >= m : lda >= p.ncol_proc);
+    REQUIRE(ordera_ == 'C' ? lda >= p.nrow : lda >= p.ncol_proc);
     REQUIRE(ldyst == Nl);
   } else {
     REQUIRE(ordera_ == 'C' ? lda >= p.nrow_proc : lda >= n);
@@ -252,16 +254,32 @@ void sketch_api(const isvd_Param &p, const T *argv, isvd_int_t argc, T *retv, is
   }
   if (omega) REQUIRE(ldomega >= Nl);
   Ctx c(precision);
-  View<T> A, Om, Y;
-  c.sc.a_panel_rows = plan_a_panels<T>(a, m, n, Nl, p.dim_sketch, c.sc.precision == kMixed);
-  if (c.sc.a_panel_rows == 0) {  // otherwise a host A is streamed in row panels by the sketch
-    if (ordera_ == 'R') A.bind(a, n, m, lda, true, c.sc.st);
-    else A.bind(a, m, n, lda, true, c.sc.st);
+  if (colblk) {
+    c.sc.col_begin = p.colidxbegin;
+    c.sc.a_cols = acols;
   }
-  if (omega) Om.bind(omega, Nl, n, ldomega, true, c.sc.st);
+  View<T> A, Om, Y;
+  c.sc.a_panel_rows = plan_a_panels<T>(a, arows, acols, Nl, p.dim_sketch, c.sc.precision == kMixed);
+  if (c.sc.a_panel_rows == 0) {  // otherwise a host A is streamed in row panels by the sketch
+    if (ordera_ == 'R') A.bind(a, acols, arows, lda, true, c.sc.st);
+    else A.bind(a, arows, acols, lda, true, c.sc.st);
+  }
+  if (omega) Om.bind(omega + (colblk ? (size_t)p.colidxbegin * ldomega : 0), Nl, acols, ldomega, true, c.sc.st);
   Y.bind(yst, Nl, m, ldyst, false, c.sc.st);
-  sketch_dev<T>(c.sc, m, n, Nl, ordera_, c.sc.a_panel_rows ? a : A.d, lda, omega ? Om.d : nullptr, ldomega,
-                (uint64_t)(uint32_t)seed, Y.d, ldyst);
+  const T *a_use = c.sc.a_panel_rows ? a : A.d;
+  if (colblk) {  // Y = sum over the ranks of A_j Omega_j, then this rank's rows (@x@_sketch.h:82)
+    DBuf<T> Yf((size_t)arows * Nl);
+    sketch_dev<T>(c.sc, arows, acols, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega,
+                  (uint64_t)(uint32_t)seed, Yf.p, Nl);
+    allreduce_sum(Yf.p, (size_t)arows * Nl, c.sc.st);
+    CK(cudaMemcpyAsync(Y.d, Yf.p + (size_t)p.rowidxbegin * Nl, (size_t)m * Nl * sizeof(T), cudaMemcpyDeviceToDevice,
+                       c.sc.st));
+    Y.back(c.sc.st);
+    sync();
+    return;
+  }
+  sketch_dev<T>(c.sc, m, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.d,
+                ldyst);
   Y.back(c.sc.st);
   sync();
 }
@@ -509,7 +527,6 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   const bool root = p.mpi_rank == p.mpi_root;
   // several ranks (isvd_gpu_set_allreduce): this rank holds rows [rowidxbegin, rowidxend) of A
   const bool multi = p.mpi_size > 1;
-  if (multi && dista_ != 'R') fail(kErrUnsupported, "several ranks: row blocks (dista 'R') only");
   const int ml = multi ? (int)p.nrow_proc : m;  // rows of A held here
   if (stream && root) {
     const char *tn = TypeName<T>::name;
@@ -533,9 +550,18 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   cudaStream_t st = c.sc.st;
   MixedCache mcache;  // A's bf16 planes, shared by the sketch and the postprocess
   c.sc.cache = &mcache;
+  // column blocks over several ranks (dista 'C'): A holds all m rows and this rank's columns; Y is
+  // summed over the ranks and each keeps its row block, so that the orthogonalization and the
+  // integration run on row blocks as with dista 'R'
+  const bool colblk = multi && dista_ == 'C';
+  const int arows = colblk ? m : ml, acols = colblk ? (int)p.ncol_proc : n;  // A held here
   if (multi) {
     c.sc.m_total = m;
     c.sc.row_begin = p.rowidxbegin;
+  }
+  if (colblk) {
+    c.sc.col_begin = p.colidxbegin;
+    c.sc.a_cols = acols;
   }
   StageTimer tm;
   auto progress = [&](const char *what) {
@@ -553,17 +579,28 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   const bool mixed = c.sc.precision == kMixed;
   // out of core: a host A that does not fit beside the solve's buffers is streamed in row panels
   // by the sketch and again by the projection
-  c.sc.a_panel_rows = plan_a_panels<T>(a, ml, n, Nl, l, mixed);
+  c.sc.a_panel_rows = plan_a_panels<T>(a, arows, acols, Nl, l, mixed);
   View<T> A, Om;
   if (!mixed && c.sc.a_panel_rows == 0) {
-    if (ordera_ == 'R') A.bind(a, n, ml, lda, true, st);
-    else A.bind(a, ml, n, lda, true, st);
+    if (ordera_ == 'R') A.bind(a, acols, arows, lda, true, st);
+    else A.bind(a, arows, acols, lda, true, st);
   }
   const T *a_use = (mixed || c.sc.a_panel_rows > 0) ? a : A.d;
-  if (omega) Om.bind(omega, Nl, n, ldomega, true, st);
+  // Omega passed in: all n rows; column blocks use the rows of their own columns
+  if (omega) Om.bind(omega + (colblk ? (size_t)p.colidxbegin * ldomega : 0), Nl, acols, ldomega, true, st);
   DBuf<T> Y((size_t)ml * Nl), Q((size_t)ml * l);
-  sketch_dev<T>(c.sc, ml, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed, Y.p,
-                Nl);
+  if (colblk) {  // Y = sum over the ranks of A_j Omega_j, then this rank's rows (reference
+    DBuf<T> Yf((size_t)m * Nl);  // MPI_Reduce_scatter_block, @x@_sketch.h:82)
+    sketch_dev<T>(c.sc, m, acols, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed,
+                  Yf.p, Nl);
+    allreduce_sum(Yf.p, (size_t)m * Nl, st);
+    CK(cudaMemcpyAsync(Y.p, Yf.p + (size_t)p.rowidxbegin * Nl, (size_t)ml * Nl * sizeof(T), cudaMemcpyDeviceToDevice,
+                       st));
+    sync();
+  } else {
+    sketch_dev<T>(c.sc, ml, n, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed,
+                  Y.p, Nl);
+  }
   tm.mark(1, st);
   sync();
   done();

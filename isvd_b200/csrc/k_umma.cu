@@ -925,13 +925,15 @@ __device__ __forceinline__ uint4 philox(uint4 c, uint32_t k0, uint32_t k1) {
 }
 
 __global__ void rng_bf16_t_kernel(__nv_bfloat16 *__restrict__ dst, long long n, long long Nl, long long ld,
-                                  long long rows_pad, uint64_t seed) {
-  // one thread per (c, j-pair): value indices j*Nl + c; pairs in value space (2p, 2p + 1) hold
-  // consecutive c for even Nl, so each thread produces one pair and writes two rows of dst.
+                                  long long rows_pad, uint64_t seed, long long pair0) {
+  // one thread per (c, j-pair): value indices offset + j*Nl + c (offset = 2 pair0); pairs in value
+  // space (2p, 2p + 1) hold consecutive c for even Nl, so each thread produces one pair and writes
+  // two rows of dst.
   const long long total_pairs = (n * Nl + 1) / 2;
   for (long long pi = blockIdx.x * (long long)blockDim.x + threadIdx.x; pi < total_pairs;
        pi += (long long)gridDim.x * blockDim.x) {
-    const uint4 x = philox(make_uint4((uint32_t)pi, (uint32_t)(pi >> 32), 0u, 0u), (uint32_t)seed,
+    const long long gp = pair0 + pi;
+    const uint4 x = philox(make_uint4((uint32_t)gp, (uint32_t)(gp >> 32), 0u, 0u), (uint32_t)seed,
                            (uint32_t)(seed >> 32));
     const uint64_t a = ((((uint64_t)x.x) << 32) | x.y) >> 11;
     const uint64_t bb = ((((uint64_t)x.z) << 32) | x.w) >> 11;
@@ -1222,7 +1224,8 @@ template void split_rows<double>(const double *, long long, long long, long long
                                  __nv_bfloat16 *, long long, long long, cudaStream_t);
 
 void rng_gaussian_bf16_t(__nv_bfloat16 *dst, long long n, long long Nl, long long ld, long long rows_pad,
-                         uint64_t seed, cudaStream_t st) {
+                         uint64_t seed, cudaStream_t st, long long offset) {
+  if (offset % 2) fail(kErrUnsupported, "bf16 Omega: an odd value offset (odd rows x odd Nl)");
   Runtime &rt = Runtime::get();
   if (rows_pad > Nl)
     CK(cudaMemsetAsync(dst + (size_t)Nl * ld, 0, (size_t)(rows_pad - Nl) * ld * sizeof(__nv_bfloat16), st));
@@ -1230,7 +1233,7 @@ void rng_gaussian_bf16_t(__nv_bfloat16 *dst, long long n, long long Nl, long lon
     CK(cudaMemset2DAsync(dst + n, ld * sizeof(__nv_bfloat16), 0, (ld - n) * sizeof(__nv_bfloat16), Nl, st));
   const long long pairs = (n * Nl + 1) / 2;
   const int blocks = (int)std::min<long long>((pairs + 255) / 256, 32LL * rt.num_sms);
-  rng_bf16_t_kernel<<<blocks, 256, 0, st>>>(dst, n, Nl, ld, Nl, seed);
+  rng_bf16_t_kernel<<<blocks, 256, 0, st>>>(dst, n, Nl, ld, Nl, seed, offset / 2);
   KLAUNCHED();
 }
 

@@ -112,7 +112,7 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
   if (!omega) {
     const long long old = plane_ld(n), orp = plane_rows(Nl);
     om.buf.alloc((size_t)orp * old);
-    rng_gaussian_bf16_t(om.buf.p, n, Nl, old, orp, seed, c.st);
+    rng_gaussian_bf16_t(om.buf.p, n, Nl, old, orp, seed, c.st, c.col_begin * (long long)Nl);
     om.P.ptr = om.buf.p; om.P.np = 1; om.P.rows = Nl; om.P.cols = n; om.P.ld = old; om.P.plane_stride = orp * old;
   } else {
     make_planes<T>(om, omega, ldom, n, Nl, 3, true, c.st);  // Omega' planes (Nl x n)

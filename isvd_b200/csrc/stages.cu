@@ -52,7 +52,7 @@ void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a
   DBuf<T> om;
   if (!omega) {
     om.alloc((size_t)n * Nl);
-    rng_gaussian<T>(om.p, n, Nl, Nl, seed, 0, c.st);
+    rng_gaussian<T>(om.p, n, Nl, Nl, seed, (uint64_t)c.col_begin * Nl, c.st);  // column blocks: own rows
     omega = om.p;
     ldom = Nl;
   }
@@ -406,13 +406,35 @@ void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, lo
 }
 
 template <class T>
+void project_sum(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+                 long long ldqt, T *z) {
+  if (c.a_cols <= 0) {  // one rank, or row blocks: Z = sum of A_j' Qbar_j
+    project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, z);
+    allreduce_sum(z, (size_t)n * l, c.st);
+    return;
+  }
+  // column blocks (reference projectBlockCol, @x@_postprocess.h:19-94): Qbar gathered (its
+  // MPI_Allgather, :78, here a sum of zero-padded copies), Z_j = A_j' Qbar for this rank's
+  // columns, Z gathered likewise
+  const long long M = c.m_total, nj = c.a_cols;
+  DBuf<T> qf((size_t)M * l), zj((size_t)nj * l);
+  CK(cudaMemsetAsync(qf.p, 0, (size_t)M * l * sizeof(T), c.st));
+  CK(cudaMemcpy2DAsync(qf.p + (size_t)c.row_begin * l, (size_t)l * sizeof(T), qt, (size_t)ldqt * sizeof(T),
+                       (size_t)l * sizeof(T), m, cudaMemcpyDeviceToDevice, c.st));
+  allreduce_sum(qf.p, (size_t)M * l, c.st);
+  project<T>(c, (int)M, (int)nj, l, ordera, a, lda, qf.p, l, zj.p);
+  CK(cudaMemsetAsync(z, 0, (size_t)n * l * sizeof(T), c.st));
+  CK(cudaMemcpyAsync(z + (size_t)c.col_begin * l, zj.p, (size_t)nj * l * sizeof(T), cudaMemcpyDeviceToDevice, c.st));
+  allreduce_sum(z, (size_t)n * l, c.st);
+}
+
+template <class T>
 void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,
                       const T *qt, long long ldqt, T *s, T *ut, long long ldut, T *vt, long long ldvt, bool wu,
                       bool wv) {
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l);
-  project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
-  allreduce_sum(Z.p, (size_t)n * l, c.st);  // row blocks on several ranks: Z = sum of A_j' Qbar_j
+  project_sum<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);  // several ranks: the whole Z on each
   DBuf<double> W(ll), V(ll), w(l);
   {  // W = Z' Z  (reference @x@_postprocess_gramian.c:145)
     Gemm<T, double> g;
@@ -454,8 +476,7 @@ void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char orde
                         const T *qt, long long ldqt, T *s, T *ut, long long ldut, bool wu) {
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l);
-  project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
-  allreduce_sum(Z.p, (size_t)n * l, c.st);
+  project_sum<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
   DBuf<double> W(ll), V(ll), w(l);
   {
     Gemm<T, double> g;
@@ -485,6 +506,8 @@ void post_symmetric_dev(const StageCtx &c, int m, int n, int k, int l, char orde
                               uint64_t, T *, long long);                                                        \
   template void orth_gramian_dev<T>(const StageCtx &, int, int, int, T *, long long);                           \
   template void project<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long, T *); \
+  template void project_sum<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *, long long,  \
+                               T *);                                                                               \
   template IterResult integrate_kn_dev<T>(const StageCtx &, int, int, int, const T *, long long, T *, long long, \
                                           int, double);                                                         \
   template void integrate_hr_dev<T>(const StageCtx &, int, int, int, T *, long long, T *, long long);           \

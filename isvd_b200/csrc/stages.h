@@ -25,6 +25,11 @@ struct StageCtx {
   // stage's own rows are all of them), and the first of this process's rows
   long long m_total = 0;
   long long row_begin = 0;
+  // column blocks (dista 'C') on several ranks: this process holds all m_total rows of A and its
+  // columns [col_begin, col_begin + a_cols) (a_cols 0: A holds every column of its rows); the sketch
+  // draws the rows of Omega from col_begin on
+  long long col_begin = 0;
+  long long a_cols = 0;
   // the stage's matrix is whole and the same on every rank (an n x l factor formed after a sum over
   // the ranks): no exchange between ranks, and every rank computes the same result
   bool replicated = false;
@@ -97,6 +102,13 @@ int svd_adjoint_dev(const StageCtx &c, int m, int n, int k, char ordera, const T
 template <class T>
 void project(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
              long long ldqt, T *z);
+
+// Z = A' Qbar (n x l) summed over the ranks, the whole of it on every rank: m and qt are this
+// rank's rows of Qbar; with row blocks A holds the same m rows, with column blocks (a_cols > 0) all
+// m_total rows and a_cols columns.
+template <class T>
+void project_sum(const StageCtx &c, int m, int n, int l, char ordera, const T *a, long long lda, const T *qt,
+                 long long ldqt, T *z);
 
 template <class T>
 void post_gramian_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, const T *a, long long lda,

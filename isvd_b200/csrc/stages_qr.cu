@@ -371,11 +371,10 @@ void post_tsqr_dev(const StageCtx &c, int m, int n, int k, int l, char ordera, c
                    bool wv) {
   const size_t ll = (size_t)l * l;
   DBuf<T> Z((size_t)n * l), Qz((size_t)n * l);
-  project<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
-  // row blocks on several ranks: Z = sum of A_j' Qbar_j, whole on every rank, which then factors
-  // it as one rank would (the reference factors its row-distributed Z by a TSQR tree, :199-241;
-  // both give the QR factorization of the same Z, up to rounding and column signs)
-  allreduce_sum(Z.p, (size_t)n * l, c.st);
+  // several ranks: the whole Z on every rank, which then factors it as one rank would (the
+  // reference factors its distributed Z by a TSQR tree, :199-241; both give the QR factorization of
+  // the same Z, up to rounding and column signs)
+  project_sum<T>(c, m, n, l, ordera, a, lda, qt, ldqt, Z.p);
   CK(cudaMemcpyAsync(Qz.p, Z.p, (size_t)n * l * sizeof(T), cudaMemcpyDeviceToDevice, c.st));
   StageCtx cn = c;
   cn.precision = kNative;  // the n x l factorization: the stage's own type on CUDA cores

@@ -63,10 +63,11 @@ template <class T>
 void split_rows(const T *src, long long s_rs, long long s_cs, long long rows, long long cols, int np, bool transpose,
                 __nv_bfloat16 *dst, long long ld, long long plane_stride, cudaStream_t st);
 
-// Omega' drawn directly in bf16: plane(c, j) = bf16(N(0,1) value with index j * cols_total + c)
-// so that Omega(j, c) matches rng_gaussian's value index convention (rounded).
+// Omega' drawn directly in bf16: plane(c, j) = bf16(N(0,1) value with index offset + j * Nl + c)
+// so that Omega(j, c) matches rng_gaussian's value index convention (rounded); offset even (the
+// first of this process's rows of Omega times Nl).
 void rng_gaussian_bf16_t(__nv_bfloat16 *dst, long long n, long long Nl, long long ld, long long rows_pad,
-                         uint64_t seed, cudaStream_t st);
+                         uint64_t seed, cudaStream_t st, long long offset = 0);
 
 void umma_gemm(const UmmaGemm &g, cudaStream_t st);
 

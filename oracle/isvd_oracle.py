@@ -260,6 +260,37 @@ def row_block(m, P, rank):
     return min(rank * each, m), min(rank * each + each, m)
 
 
+def _distributed(y, project, k, p, N, allreduce, alg_i, argv_i, alg_p, row_begin):
+    """Orthogonalization, integration and postprocessing on this rank's rows y of Y, every sum over
+    the ranks through ``allreduce``; ``project(qbar_rows)`` returns the whole Z = A' Qbar."""
+    l = k + p
+    q = np.empty_like(y)
+    for i in range(N):
+        yi = y[:, i * l:(i + 1) * l]
+        w = allreduce(yi.T @ yi)
+        u, s, _ = np.linalg.svd(w)
+        q[:, i * l:(i + 1) * l] = yi @ (u / np.sqrt(s))
+    argv_i = dict(argv_i or {})
+    if alg_i == "KN":
+        qp, it, err = integrate_kolmogorov_nagumo(q, l, N, allreduce=allreduce, **argv_i)
+    elif alg_i == "WY":
+        qp, it, err = integrate_wen_yin(q, l, N, allreduce=allreduce, **argv_i)
+    else:
+        qp, it, err = integrate_hierarchical_reduction(q, l, N, allreduce=allreduce)[0], 0, 0.0
+    z = project(qp)
+    if alg_p == "TS":
+        qz, r = np.linalg.qr(z)
+        uu, s, vvt = np.linalg.svd(r.T)
+        return s, qp @ vvt.T[:, :k], qz @ uu.T, it, err
+    if alg_p == "SY":
+        w = allreduce(z[row_begin:row_begin + qp.shape[0]].T @ qp)
+        lam, ev = np.linalg.eigh(_sym_upper(w))
+        return lam, qp @ ev[:, :k], None, it, err
+    w, s, _ = np.linalg.svd(z.T @ z)
+    sig = np.sqrt(s)
+    return sig, qp @ w[:, :k], (z @ w[:, :k]) / sig[:k], it, err
+
+
 def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None, alg_p="GR", row_begin=0):
     """The Gramian / KN, WY or HR / GR, TS or SY driver on one rank's rows [row_begin, ...) of a
     row-distributed A (dista 'R'), with every reduction over the ranks done by ``allreduce(x)`` (an
@@ -275,33 +306,32 @@ def isvd_row_block(a_rows, omega, k, p, N, allreduce, alg_i="KN", argv_i=None, a
         Z(own rows)' Qbar_j (@x@_postprocess_symmetric.c:146-147).
     Returns (s, U rows of this rank, V (all n rows; SY: None), iterations, error or mu)."""
     a_rows = np.asarray(a_rows, np.float64)
-    l = k + p
     y = a_rows @ np.asarray(omega, np.float64)
-    q = np.empty_like(y)
-    for i in range(N):
-        yi = y[:, i * l:(i + 1) * l]
-        w = allreduce(yi.T @ yi)
-        u, s, _ = np.linalg.svd(w)
-        q[:, i * l:(i + 1) * l] = yi @ (u / np.sqrt(s))
-    argv_i = dict(argv_i or {})
-    if alg_i == "KN":
-        qp, it, err = integrate_kolmogorov_nagumo(q, l, N, allreduce=allreduce, **argv_i)
-    elif alg_i == "WY":
-        qp, it, err = integrate_wen_yin(q, l, N, allreduce=allreduce, **argv_i)
-    else:
-        qp, it, err = integrate_hierarchical_reduction(q, l, N, allreduce=allreduce)[0], 0, 0.0
-    z = allreduce(a_rows.T @ qp)
-    if alg_p == "TS":
-        qz, r = np.linalg.qr(z)
-        uu, s, vvt = np.linalg.svd(r.T)
-        return s, qp @ vvt.T[:, :k], qz @ uu.T, it, err
-    if alg_p == "SY":
-        w = allreduce(z[row_begin:row_begin + qp.shape[0]].T @ qp)
-        lam, ev = np.linalg.eigh(_sym_upper(w))
-        return lam, qp @ ev[:, :k], None, it, err
-    w, s, _ = np.linalg.svd(z.T @ z)
-    sig = np.sqrt(s)
-    return sig, qp @ w[:, :k], (z @ w[:, :k]) / sig[:k], it, err
+    return _distributed(y, lambda qp: allreduce(a_rows.T @ qp), k, p, N, allreduce, alg_i, argv_i, alg_p,
+                        row_begin)
+
+
+def isvd_col_block(a_cols, omega, k, p, N, allreduce, rows, cols, alg_i="KN", argv_i=None, alg_p="GR"):
+    """The same driver on one rank's columns ``cols`` (a slice) of a column-distributed A (dista
+    'C'; a_cols holds all m rows of them), with Omega's rows of those columns:
+      * sketch Y = sum_ranks A_j Omega_j, each rank keeping its row block ``rows``
+        (sketchBlockCol, core/stage/@x@_sketch.h:21-90: MPI_Reduce_scatter_block at :82);
+      * orthogonalization and integration on the row blocks, as isvd_row_block;
+      * projection: Qbar gathered (MPI_Allgather, core/stage/@x@_postprocess.h:78), Z_j = A_j' Qbar
+        for the rank's columns, Z gathered (here both gathers are sums of zero-padded copies)."""
+    a_cols = np.asarray(a_cols, np.float64)
+    omega = np.asarray(omega, np.float64)
+    m, n, l = a_cols.shape[0], omega.shape[0], k + p
+    y = allreduce(a_cols @ omega[cols])[rows]
+
+    def project(qp):
+        qf = np.zeros((m, l))
+        qf[rows] = qp
+        qf = allreduce(qf)
+        z = np.zeros((n, l))
+        z[cols] = a_cols.T @ qf
+        return allreduce(z)
+    return _distributed(y, project, k, p, N, allreduce, alg_i, argv_i, alg_p, rows.start)
 
 
 # ---------------------------------------------------------------------------------------------

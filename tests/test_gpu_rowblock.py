@@ -26,8 +26,8 @@ def lowrank(m, n, rank, decay, noise, seed):
     return (u * decay ** np.arange(rank)) @ v.T + noise * rng.standard_normal((m, n))
 
 
-def solve(L, x, prm, a, om, k, p, N, algs, precision, ut_root, vt_root):
-    """The driver on this process's rows; returns s, ut, vt, retv."""
+def solve(L, x, prm, a, om, k, p, N, algs, precision, ut_root, vt_root, dista="R"):
+    """The driver on this process's rows (dista 'R') or columns ('C'); returns s, ut, vt, retv."""
     l = k + p
     dt = np.float32 if x == "s" else np.float64
     mloc = prm.nrow_proc if ut_root < 0 or ut_root != prm.mpi_rank else prm.nrow
@@ -38,7 +38,7 @@ def solve(L, x, prm, a, om, k, p, N, algs, precision, ut_root, vt_root):
     n = a.shape[1]
     argv = [None, None, [256, 1e-4] if algs[2] == "KN" else None, None]
     retv, _, st = L.isvd(x, prm, algs, np.ascontiguousarray(a.astype(dt)), n, s, ut, l, vt, l, argv=argv,
-                         retc=(0, 0, 2, 0), ut_root=ut_root, vt_root=vt_root,
+                         retc=(0, 0, 2, 0), ut_root=ut_root, vt_root=vt_root, dista=dista.encode(),
                          omega=np.ascontiguousarray(om.astype(dt)), ldomega=l * N, precision=precision)
     assert st == 0, L.last_error()
     return s, ut, vt, [list(v) for v in retv]
@@ -52,14 +52,14 @@ def _worker(rank, port, args, q):
     from isvd_b200.capi import IsvdLib, torch_device_allreduce, torch_host_allreduce
     try:
         dist.init_process_group("gloo", rank=rank, world_size=2, timeout=datetime.timedelta(seconds=120))
-        x, precision, algs, a, om, k, p, N, on_device = args
+        x, precision, algs, a, om, k, p, N, on_device, dista = args
         L = IsvdLib(LIB_PATH)
         fn = torch_device_allreduce() if on_device else torch_host_allreduce()
         L.set_allreduce(fn, 2, rank, on_device=on_device)
         prm = L.create_param(a.shape[0], a.shape[1], k, p, N)
-        rows = slice(prm.rowidxbegin, prm.rowidxend)
-        own = solve(L, x, prm, a[rows], om, k, p, N, algs, precision, -1, -1)
-        gathered = solve(L, x, prm, a[rows], om, k, p, N, algs, precision, 0, 0)
+        held = a[prm.rowidxbegin:prm.rowidxend] if dista == "R" else a[:, prm.colidxbegin:prm.colidxend]
+        own = solve(L, x, prm, held, om, k, p, N, algs, precision, -1, -1, dista)
+        gathered = solve(L, x, prm, held, om, k, p, N, algs, precision, 0, 0, dista)
         q.put((rank, (prm.rowidxbegin, prm.rowidxend, prm.colidxbegin, prm.colidxend), own, gathered))
         dist.destroy_process_group()
     except BaseException as e:  # report instead of hanging the parent
@@ -74,16 +74,19 @@ def free_port():
     return port
 
 
-@pytest.mark.parametrize("x,precision,algs,on_device", [
-    ("d", 0, ("GP", "GR", "KN", "GR"), False), ("s", 1, ("GP", "GR", "KN", "GR"), False),
-    ("d", 0, ("GP", "TS", "WY", "GR"), False), ("s", 1, ("GP", "TS", "WY", "GR"), False),
-    ("d", 0, ("GP", "GR", "KN", "GR"), True), ("s", 1, ("GP", "TS", "KN", "GR"), True),
-    ("d", 0, ("GP", "GR", "HR", "GR"), False), ("s", 1, ("GP", "GR", "HR", "GR"), True),
-    ("d", 0, ("GP", "GR", "KN", "TS"), False), ("s", 1, ("GP", "TS", "KN", "TS"), True),
-    ("d", 0, ("GP", "GR", "KN", "SY"), False), ("s", 1, ("GP", "GR", "WY", "SY"), True)])
-def test_two_row_blocks_match_one_process(lib, oracle, x, precision, algs, on_device):
+@pytest.mark.parametrize("x,precision,algs,on_device,dista", [
+    ("d", 0, ("GP", "GR", "KN", "GR"), False, "R"), ("s", 1, ("GP", "GR", "KN", "GR"), False, "R"),
+    ("d", 0, ("GP", "TS", "WY", "GR"), False, "R"), ("s", 1, ("GP", "TS", "WY", "GR"), False, "R"),
+    ("d", 0, ("GP", "GR", "KN", "GR"), True, "R"), ("s", 1, ("GP", "TS", "KN", "GR"), True, "R"),
+    ("d", 0, ("GP", "GR", "HR", "GR"), False, "R"), ("s", 1, ("GP", "GR", "HR", "GR"), True, "R"),
+    ("d", 0, ("GP", "GR", "KN", "TS"), False, "R"), ("s", 1, ("GP", "TS", "KN", "TS"), True, "R"),
+    ("d", 0, ("GP", "GR", "KN", "SY"), False, "R"), ("s", 1, ("GP", "GR", "WY", "SY"), True, "R"),
+    ("d", 0, ("GP", "GR", "KN", "GR"), False, "C"), ("s", 1, ("GP", "GR", "KN", "GR"), True, "C"),
+    ("d", 0, ("GP", "TS", "HR", "TS"), False, "C"), ("d", 0, ("GP", "GR", "KN", "SY"), True, "C")])
+def test_two_row_blocks_match_one_process(lib, oracle, x, precision, algs, on_device, dista):
     """Every selector the driver takes with row blocks: GR or TS orthogonalization, KN, WY or HR
-    integration, GR, TS or SY postprocessing (SY: a symmetric A)."""
+    integration, GR, TS or SY postprocessing (SY: a symmetric A); and column blocks (dista 'C':
+    each process holds all rows of its columns, Y summed over the processes)."""
     if algs[3] == "SY":
         m = n = 700
         a = lowrank(m, n, 300, 0.97, 1e-6, 11)
@@ -98,7 +101,7 @@ def test_two_row_blocks_match_one_process(lib, oracle, x, precision, algs, on_de
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = free_port()
-    args = (x, precision, algs, a, om, k, p, N, on_device)
+    args = (x, precision, algs, a, om, k, p, N, on_device, dista)
     procs = [ctx.Process(target=_worker, args=(r, port, args, q)) for r in range(2)]
     for pr in procs:
         pr.start()

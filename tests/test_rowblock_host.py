@@ -46,7 +46,7 @@ def test_set_allreduce_rejects_bad_ranks(lib):
     assert lib.create_param(10, 10, 2, 1, 2).mpi_size == 1
 
 
-def _rank(rank, port, a, om, k, p, N, alg, alg_p, q):
+def _rank(rank, port, a, om, k, p, N, alg, alg_p, dista, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     import sys
@@ -69,16 +69,23 @@ def _rank(rank, port, a, om, k, p, N, alg, alg_p, q):
         f32 = np.arange(5, dtype=np.float32) * (rank + 1)
         fn(f32.ctypes.data, 5, 0, None, None)
         rb, re = orc.row_block(a.shape[0], 2, rank)
-        s, u, v, it, err = orc.isvd_row_block(a[rb:re], om, k, p, N, allreduce, alg_i=alg, alg_p=alg_p,
-                                              row_begin=rb)
+        if dista == "R":
+            s, u, v, it, err = orc.isvd_row_block(a[rb:re], om, k, p, N, allreduce, alg_i=alg, alg_p=alg_p,
+                                                  row_begin=rb)
+        else:
+            cb, ce = orc.row_block(a.shape[1], 2, rank)
+            s, u, v, it, err = orc.isvd_col_block(a[:, cb:ce], om, k, p, N, allreduce, slice(rb, re), slice(cb, ce),
+                                                  alg_i=alg, alg_p=alg_p)
         q.put((rank, (rb, re), s, u, v, it, count[0], f32))
         dist.destroy_process_group()
     except BaseException as e:
         q.put((rank, "error", repr(e), None, None, None, None, None))
 
 
-@pytest.mark.parametrize("alg,alg_p", [("KN", "GR"), ("WY", "GR"), ("HR", "GR"), ("KN", "TS"), ("KN", "SY")])
-def test_exchange_algebra_over_gloo(oracle, alg, alg_p):
+@pytest.mark.parametrize("alg,alg_p,dista", [("KN", "GR", "R"), ("WY", "GR", "R"), ("HR", "GR", "R"),
+                                             ("KN", "TS", "R"), ("KN", "SY", "R"), ("KN", "GR", "C"),
+                                             ("HR", "TS", "C"), ("WY", "SY", "C")])
+def test_exchange_algebra_over_gloo(oracle, alg, alg_p, dista):
     m, n, k, p, N = 301, 120, 6, 4, 5
     rng = np.random.default_rng(3)
     a = (np.linalg.qr(rng.standard_normal((m, 40)))[0] * 0.9 ** np.arange(40)) @ rng.standard_normal((40, n))
@@ -93,7 +100,7 @@ def test_exchange_algebra_over_gloo(oracle, alg, alg_p):
     s.bind(("127.0.0.1", 0))
     port = s.getsockname()[1]
     s.close()
-    procs = [ctx.Process(target=_rank, args=(r, port, a, om, k, p, N, alg, alg_p, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, port, a, om, k, p, N, alg, alg_p, dista, q)) for r in range(2)]
     for pr in procs:
         pr.start()
     res = {}
@@ -108,19 +115,23 @@ def test_exchange_algebra_over_gloo(oracle, alg, alg_p):
     for r in (0, 1):
         _, (rb, re), sr, ur, vr, it, calls, f32 = res[r]
         assert np.array_equal(f32, np.arange(5, dtype=np.float32) * 3)
-        # the block Grams; KN: Bc, one Bgc per iteration; WY: also the first Bgc and the two
-        # step-size sums of every iteration but the last; HR: one sum per level; then Z (and for
-        # SY the l x l W)
+        # column blocks: Y; the block Grams; KN: Bc, one Bgc per iteration; WY: also the first
+        # Bgc and the two step-size sums of every iteration but the last; HR: one sum per level;
+        # then Z (column blocks: Qbar and Z) and for SY the l x l W
         levels, h2 = 0, N
         while h2 > 1:
             levels, h2 = levels + 1, (h2 + 1) // 2
         integ = {"KN": 1 + it, "WY": 2 + it + (it - 1), "HR": levels}[alg]
-        expected = N + integ + (2 if alg_p == "SY" else 1)
+        col = dista == "C"
+        expected = col + N + integ + (2 if col else 1) + (alg_p == "SY")
         assert it == whole["iters"] and calls == expected
-        assert np.abs(sr - whole["s"]).max() <= 1e-12 * np.abs(whole["s"]).max()
+        # column blocks add Y's partial products in another order (last-bit differences); WY stops
+        # at tol 1e-3, short of convergence, where such differences grow to about 1e-8
+        ts, ta = (1e-7, 1e-6) if (col and alg == "WY") else (1e-12, 1e-10)
+        assert np.abs(sr - whole["s"]).max() <= ts * np.abs(whole["s"]).max()
         if alg_p != "SY":
-            assert oracle.column_angles(vr, whole["v"]).max() < 1e-10
-    assert oracle.column_angles(u, whole["u"]).max() < 1e-10
+            assert oracle.column_angles(vr, whole["v"]).max() < ta
+    assert oracle.column_angles(u, whole["u"]).max() < ta
 
 
 def test_noalloc_kn_refuses_joined_ranks(lib):
