@@ -370,6 +370,43 @@ def batch_main(args):
     print(json.dumps(out), flush=True)
 
 
+def kn_loop_main(args):
+    """The MIXED Kolmogorov-Nagumo integration stage (isvd_sIntegrateKolmogorovNagumo) alone, at the
+    loop shapes of the 200000 x 20000 workload (N = 32 blocks of l = 128, so G is 4096 x 4096) but on
+    6000 rows, so that forming G and the final Qbar = Qs M take little of the time: W untimed calls,
+    then K calls timed with CUDA events; the loop's cost per iteration without the sketch before it
+    (which leaves the clock at the power cap in the full solve)."""
+    import torch
+    import isvd_b200
+    lib = isvd_b200.load()
+    lib.lib.isvd_gpu_set_precision(1)
+    m, l, N = 6000, 128, 32
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(3)
+    base = torch.linalg.qr(torch.randn(m, l, device=dev, dtype=torch.float64, generator=g))[0]
+    qs = torch.cat([torch.linalg.qr(base + 0.05 * torch.randn(m, l, device=dev, dtype=torch.float64,
+                                                               generator=g))[0] for _ in range(N)], dim=1)
+    qs = qs.float().contiguous()
+    qt = torch.zeros((m, l), device=dev)
+    prm = lib.create_param(m, m, l, 0, N)
+    stream = torch.cuda.current_stream(dev)
+    lib.lib.isvd_gpu_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    its, ms = [], []
+    for i in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = lib.integrate("s", "KN", prm, qs, l * N, qt, l, argv=[256, 1e-4])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            its.append(int(r[0]))
+            ms.append(e0.elapsed_time(e1))
+    lib.lib.isvd_gpu_set_stream(None)
+    print(json.dumps({"workload": "KN integration, MIXED, N l = 4096, l = 128, 6000 rows", "kn_iterations": its[-1],
+                      "ms_per_stage": float(np.median(ms)), "us_per_iteration": 1e3 * float(np.median(ms)) / its[-1],
+                      "steps": args.steps, "warmup": args.warmup}), flush=True)
+
+
 def run_batched(torch, lib, steps, warmup, single=False):
     """The batched-solves workload (batch_main); returns its JSON record.  single: one batch call
     and nothing else (for launch lists)."""
@@ -576,6 +613,9 @@ def main():
                     help="the batched-solves workload (256 uneven matrices) instead of the single large solve")
     ap.add_argument("--square50k", action="store_true",
                     help="the 50000 x 50000 TS / WY / column-block parity case, MIXED beside FP64")
+    ap.add_argument("--kn-loop", action="store_true",
+                    help="the Kolmogorov-Nagumo integration stage alone at the 200000 x 20000 workload's "
+                         "loop shapes (N l = 4096, l = 128) on 6000 rows: time per iteration")
     ap.add_argument("--parallel", default="rowblock", choices=["rowblock", "replicas"],
                     help="N > 1: one solve split by rows over the ranks (default) or one solve per rank")
     ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
@@ -586,6 +626,8 @@ def main():
         return batch_main(args)
     if args.square50k:
         return square50k_main(args)
+    if args.kn_loop:
+        return kn_loop_main(args)
     w = WORKLOADS[args.size]
     if args.impl == "reference":
         return reference_arm(args, w)
