@@ -20,6 +20,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "batched.h"
@@ -30,26 +31,43 @@ namespace isvdb {
 namespace {
 
 // ------------------------------------------------------------------------- grouped GEMM
-struct GProd {  // C = alpha A B + beta C, A M x K, B K x N (element strides), C M x N
-  int M, N, K;
-  const void *A;
-  long long a_rs, a_cs;
-  const void *B;
-  long long b_rs, b_cs;
-  void *C;
-  long long c_rs, c_cs;
-  double alpha, beta;
-  int tile0, tn;  // first work item of this product, output tiles along N
-};
+using GProd = GroupedProd;  // C = alpha A B + beta C, its work items from tile0 (kernels.h)
 
 constexpr int kGThreads = 256;
 
+// V consecutive elements from 16-byte aligned shared memory as one or two vector loads.
+template <int V, class T>
+__device__ __forceinline__ void lds_vec(const T *p, T (&out)[V]) {
+  constexpr int kPer16 = 16 / (int)sizeof(T);  // elements of one 16-byte load
+  static_assert(V % 2 == 0 && (V <= kPer16 || V % kPer16 == 0), "vector width");
+  if (V >= kPer16) {
+#pragma unroll
+    for (int v = 0; v < V; v += kPer16) {
+      const float4 w = *reinterpret_cast<const float4 *>(p + v);
+      const T *e = reinterpret_cast<const T *>(&w);
+#pragma unroll
+      for (int u = 0; u < kPer16; ++u) out[v + u] = e[u];
+    }
+  } else {  // two floats (8 bytes)
+    const float2 w = *reinterpret_cast<const float2 *>(p);
+    const T *e = reinterpret_cast<const T *>(&w);
+#pragma unroll
+    for (int u = 0; u < V; ++u) out[u] = e[u];
+  }
+}
+
+// Grouped products on CUDA cores: each CTA walks the work items blockIdx.x, blockIdx.x + gridDim.x,
+// ...; a work item is one BM x BN output tile of the product that owns it.  256 threads in a
+// 16 x 16 grid, each accumulating TM x TN outputs: rows ty * TM/2 + [0, TM/2) of both halves of
+// the tile (and columns likewise), so that a thread's operands of one k are two vector loads from
+// shared memory per operand.  Each output is one FMA chain in ascending k.
 template <class T, class Tout, int BM, int BN>
 __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restrict__ prods, int nprod, int total) {
-  constexpr int BK = 16, TM = BM / 16, TN = BN / 16;
+  constexpr int BK = 16, TM = BM / 16, TN = BN / 16, HM = TM / 2, HN = TN / 2;
   constexpr int LA = BM * BK / kGThreads, LB = BK * BN / kGThreads;
-  __shared__ T As[BK][BM + 1];
-  __shared__ T Bs[BK][BN + 1];
+  constexpr int kPad = 16 / (int)sizeof(T);  // rows stay 16-byte aligned; transposing stores spread over banks
+  __shared__ __align__(16) T As[BK][BM + kPad];
+  __shared__ __align__(16) T Bs[BK][BN + kPad];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
     int lo = 0, hi = nprod - 1;  // the product owning work item t
@@ -99,6 +117,7 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
         Bs[kk][nn] = rb[r];
       }
     };
+    __syncthreads();  // the previous work item's reads of As / Bs are done
     if (g.K > 0) load(0);
     for (int k0 = 0; k0 < g.K; k0 += BK) {
       store();
@@ -107,10 +126,12 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
         T av[TM], bv[TN];
-#pragma unroll
-        for (int i = 0; i < TM; ++i) av[i] = As[kk][ty + 16 * i];
-#pragma unroll
-        for (int j = 0; j < TN; ++j) bv[j] = Bs[kk][tx + 16 * j];
+        T (&a0)[HM] = *reinterpret_cast<T(*)[HM]>(av), (&a1)[HM] = *reinterpret_cast<T(*)[HM]>(av + HM);
+        T (&b0)[HN] = *reinterpret_cast<T(*)[HN]>(bv), (&b1)[HN] = *reinterpret_cast<T(*)[HN]>(bv + HN);
+        lds_vec<HM>(&As[kk][ty * HM], a0);
+        lds_vec<HM>(&As[kk][BM / 2 + ty * HM], a1);
+        lds_vec<HN>(&Bs[kk][tx * HN], b0);
+        lds_vec<HN>(&Bs[kk][BN / 2 + tx * HN], b1);
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
@@ -121,11 +142,11 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
     Tout *__restrict__ C = static_cast<Tout *>(g.C);
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
-      const int gm = m0 + ty + 16 * i;
+      const int gm = m0 + (i < HM ? ty * HM + i : BM / 2 + ty * HM + (i - HM));
       if (gm >= g.M) continue;
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
-        const int gn = n0 + tx + 16 * j;
+        const int gn = n0 + (j < HN ? tx * HN + j : BN / 2 + tx * HN + (j - HN));
         if (gn >= g.N) continue;
         Tout *c = C + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
         double v = g.alpha * (double)acc[i][j];
@@ -184,17 +205,40 @@ constexpr int kConfigs = 3;
 constexpr int kBM[kConfigs] = {64, 128, 128}, kBN[kConfigs] = {64, 64, 128};
 std::map<std::string, int> g_tuned;  // product-list signature -> tile shape
 
-// A grouped product list: host descriptors, the device copy for the chosen tile shape.
+// A grouped product list: host descriptors, the device copy for the chosen tile shape.  FP64
+// lists whose products share one operand orientation run on the FP64 tensor cores
+// (dmma_grouped, tile shapes dmma_grouped_bm / _bn); other lists on the CUDA-core ggemm_kernel.
 template <class T, class Tout>
 struct GemmList {
+  static constexpr bool kFp64 = std::is_same<T, double>::value && std::is_same<Tout, double>::value;
   std::vector<GProd> host;
   DevList<GProd> dev;
   int config = -1, total = 0, uploaded = -1;
+  bool dmma = false, a_kc = false, b_nc = false;  // orientation of the tensor-core launch
 
   void clear() {
     host.clear();
     uploaded = -1;
   }
+  // dmma, a_kc, b_nc from the current products
+  void orient() {
+    dmma = false;
+    if (!kFp64 || host.empty() || !dmma_enabled()) return;
+    auto all = [&](auto pred) {
+      for (const auto &g : host)
+        if (!pred(g)) return false;
+      return true;
+    };
+    const bool akc = all([](const GProd &g) { return g.a_cs == 1; }), amc = all([](const GProd &g) { return g.a_rs == 1; });
+    const bool bnc = all([](const GProd &g) { return g.b_cs == 1; }), bkc = all([](const GProd &g) { return g.b_rs == 1; });
+    if ((akc || amc) && (bnc || bkc)) {
+      dmma = true;
+      a_kc = akc;
+      b_nc = bnc;
+    }
+  }
+  int bm(int cfg) const { return dmma ? dmma_grouped_bm(cfg) : kBM[cfg]; }
+  int bn(int cfg) const { return dmma ? dmma_grouped_bn(cfg) : kBN[cfg]; }
   std::string signature() const {
     int bm = 0, bn = 0, bk = 0;
     for (const auto &g : host) {
@@ -207,15 +251,16 @@ struct GemmList {
       while ((1 << b) < v) ++b;
       return b;
     };
-    return std::to_string(sizeof(T)) + std::to_string(sizeof(Tout)) + ":" + std::to_string(host.size()) + ":" +
+    return std::to_string(sizeof(T)) + std::to_string(sizeof(Tout)) + (dmma ? "t" : "c") + ":" +
+           std::to_string(host.size()) + ":" +
            std::to_string(lg(bm)) + "," + std::to_string(lg(bn)) + "," + std::to_string(lg(bk));
   }
   void finalize(int cfg, cudaStream_t st) {  // work items for tile shape cfg, uploaded
     int tot = 0;
     for (auto &g : host) {
-      g.tn = (g.N + kBN[cfg] - 1) / kBN[cfg];
+      g.tn = (g.N + bn(cfg) - 1) / bn(cfg);
       g.tile0 = tot;
-      tot += ((g.M + kBM[cfg] - 1) / kBM[cfg]) * g.tn;
+      tot += ((g.M + bm(cfg) - 1) / bm(cfg)) * g.tn;
     }
     total = tot;
     dev.upload(host, st);
@@ -223,6 +268,10 @@ struct GemmList {
   }
   void launch(int cfg, cudaStream_t st) {  // kernels only (capturable)
     if (host.empty() || total == 0) return;
+    if (dmma) {
+      dmma_grouped(static_cast<const GroupedProd *>(dev.d.p), dev.count, total, cfg, a_kc, b_nc, st);
+      return;
+    }
     const int grid = std::max(1, std::min(total, 4 * Runtime::get().num_sms));
     switch (cfg) {
       case 0: ggemm_kernel<T, Tout, 64, 64><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
@@ -235,6 +284,12 @@ struct GemmList {
   // products overwrite their outputs) and upload the work items.  May run the products.
   void prepare(cudaStream_t st, bool may_measure) {
     if (host.empty()) return;
+    const bool was = dmma;
+    orient();
+    if (dmma != was) {  // another kernel family: its tile shape is chosen afresh
+      config = -1;
+      uploaded = -1;
+    }
     if (config < 0) {
       const std::string key = signature();
       auto it = g_tuned.find(key);
@@ -248,7 +303,7 @@ struct GemmList {
         CK(cudaEventCreate(&e1));
         float best = 1e30f;
         int bestc = 0;
-        for (int cfg = 0; cfg < kConfigs; ++cfg) {
+        for (int cfg = 0; cfg < (dmma ? kDmmaGroupedShapes : kConfigs); ++cfg) {
           finalize(cfg, st);
           CK(cudaEventRecord(e0, st));
           launch(cfg, st);
@@ -341,7 +396,8 @@ struct Plan : BatchPlan {
   GemmList<double, double> l1, l2, l4;
   MapList<double, T> m_scale, m_mt, m_s, m_wk, m_vk;
   MapList<double, double> m_init;
-  DevList<EigDesc> eig1, eig2;
+  DevList<EigDesc> eig1, eig2;  // sorted by n, descending
+  std::vector<std::pair<int, int>> eig1_cls, eig2_cls;  // (first, largest n) of each size class
   DevList<KnStep> steps;
   // graphs of the work before and after the iterations
   cudaGraphExec_t pre = nullptr, post = nullptr;
@@ -388,9 +444,29 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
     P.ul.host.push_back(prod(m, k, l, M.qbar.p, l, 1, M.wk.p, k, 1, P.ut[b], P.ldut[b], 1));
     P.vl.host.push_back(prod(n, k, l, M.z.p, l, 1, M.vk.p, k, 1, P.vt[b], P.ldvt[b], 1));
   }
+  // each eigensolve list sorted by size, largest first, and cut into the size classes of the
+  // eigensolver's CTA shapes (n <= 32, <= 64, <= 96): one launch per class
+  auto classes = [](std::vector<EigDesc> &e, std::vector<std::pair<int, int>> &cls) {
+    std::stable_sort(e.begin(), e.end(), [](const EigDesc &x, const EigDesc &y) { return x.n > y.n; });
+    auto cl = [](int n) { return n <= 32 ? 0 : n <= 64 ? 1 : 2; };
+    cls.clear();
+    for (int i = 0; i < (int)e.size(); ++i)
+      if (i == 0 || cl(e[i].n) != cl(e[i - 1].n)) cls.emplace_back(i, e[i].n);
+  };
+  classes(e1, P.eig1_cls);
+  classes(e2, P.eig2_cls);
   P.eig1.upload(e1, st);
   P.eig2.upload(e2, st);
   P.m_scale.prepare(st); P.m_s.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
+}
+
+// The grouped eigensolves of list d (classes cls: first index and largest n), one launch per class.
+inline void eig_classes(const DevList<EigDesc> &d, const std::vector<std::pair<int, int>> &cls, int *status,
+                        cudaStream_t st) {
+  for (size_t c = 0; c < cls.size(); ++c) {
+    const int first = cls[c].first, end = c + 1 < cls.size() ? cls[c + 1].first : d.count;
+    sym_eig_grouped(d.d.p + first, end - first, cls[c].second, +1, true, status, st);
+  }
 }
 
 template <class T>
@@ -399,7 +475,7 @@ void run_pre(Plan<T> &P, cudaStream_t st, bool measure) {
     rng_gaussian<T>(P.mats[b]->om.p, P.n[b], P.Nl[b], P.Nl[b], P.seeds[b], 0, st);
   P.sketch.run(st, measure);
   P.gram.run(st, measure);
-  sym_eig_grouped(P.eig1.d.p, P.eig1.count, P.max_l, +1, true, P.status.p, st);
+  eig_classes(P.eig1, P.eig1_cls, P.status.p, st);
   P.m_scale.launch(st);
   P.apply.run(st, measure);
   P.gfull.run(st, measure);
@@ -411,7 +487,7 @@ void run_post(Plan<T> &P, cudaStream_t st, bool measure) {
   P.qbar_l.run(st, measure);
   P.proj.run(st, measure);
   P.wzl.run(st, measure);
-  sym_eig_grouped(P.eig2.d.p, P.eig2.count, P.max_l, +1, true, P.status.p, st);
+  eig_classes(P.eig2, P.eig2_cls, P.status.p, st);
   P.m_s.launch(st);
   P.m_wk.launch(st);
   P.m_vk.launch(st);
@@ -557,8 +633,29 @@ void batch_solve(BatchPlan *plan, const T *const *a, const long long *lda, T *co
     }
     P.l1.run(st, true);
     P.l2.run(st, true);
+    // the steps grouped by their number of 32 x 32 product tiles, nt = ceil(l / 32)^2, one launch
+    // per group with the cluster size c that minimises waves x tiles per CTA,
+    // ceil(count c / SMs) ceil(nt / c) (one 1024-thread CTA per SM)
+    auto tiles_of = [](const KnStep &s) { return ((s.l + 31) / 32) * ((s.l + 31) / 32); };
+    std::stable_sort(hsteps.begin(), hsteps.end(),
+                     [&](const KnStep &x, const KnStep &y) { return tiles_of(x) > tiles_of(y); });
     P.steps.upload(hsteps, st);
-    kn_step_grouped(P.steps.d.p, (int)hsteps.size(), P.max_l, st);
+    const int sms = rt.num_sms;
+    for (size_t g0 = 0; g0 < hsteps.size();) {
+      const int nt = tiles_of(hsteps[g0]);
+      size_t g1 = g0;
+      int lmax = 0;
+      while (g1 < hsteps.size() && tiles_of(hsteps[g1]) == nt) lmax = std::max(lmax, hsteps[g1++].l);
+      const long long cnt = (long long)(g1 - g0);
+      int best_c = 1;
+      long long best = -1;
+      for (int c = 1; c <= 8 && c <= nt; c *= 2) {
+        const long long cost = ((cnt * c + sms - 1) / sms) * ((nt + c - 1) / c);
+        if (best < 0 || cost < best) { best = cost; best_c = c; }
+      }
+      kn_step_grouped(P.steps.d.p + g0, (int)cnt, lmax, best_c, st);
+      g0 = g1;
+    }
     P.l4.run(st, true);
     int hstatus = 0;
     CK(cudaMemcpyAsync(herr.data(), P.errs.p, B * sizeof(double), cudaMemcpyDeviceToHost, st));

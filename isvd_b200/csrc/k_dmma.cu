@@ -46,24 +46,22 @@ struct DmmaLayout {
   __device__ static int b_at(int k, int n) { return B_NC ? k * (BN + kPad) + n : n * (kBK + kPad) + k; }
 };
 
+// acc += A[m0 .. m0 + BM, kb .. ke) B[kb .. ke, n0 .. n0 + BN) for one output tile, with A(i, k) =
+// A[i a_rs + k a_cs] and B(k, j) = B[k b_rs + j b_cs]; rows >= M, columns >= N read as zero.  K
+// slices flow through the kStages-deep cp.async ring in smem.  On return every copy has landed,
+// but warps may still read the ring: a caller that refills it must synchronise the block first.
 template <int BM, int BN, int WM, int WN, bool A_KC, bool B_NC>
-__global__ void __launch_bounds__(WM * WN * 32)
-    dmma_gemm_kernel(const Gemm<double, double> g, const int splits, const int kchunk, double *__restrict__ partial) {
+__device__ __forceinline__ void dmma_tile(double *smem, const double *__restrict__ A, long long a_rs, long long a_cs,
+                                          const double *__restrict__ B, long long b_rs, long long b_cs, int M, int N,
+                                          int kb, int ke, int m0, int n0,
+                                          double (&acc)[BM / WM / 8][BN / WN / 8][2]) {
   using L = DmmaLayout<BM, BN, A_KC, B_NC>;
   constexpr int NT = WM * WN * 32;
   constexpr int TM = BM / WM / 8, TN = BN / WN / 8;  // 8 x 8 tiles per warp
   constexpr int LA = BM * kBK / NT, LB = BN * kBK / NT;
   static_assert(LA * NT == BM * kBK && LB * NT == BN * kBK, "tile / thread mismatch");
-  extern __shared__ double smem[];
-
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm0 = (warp / WN) * (BM / WM), wn0 = (warp % WN) * (BN / WN);
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
-  if (g.upper && n0 + BN <= m0) return;  // tile strictly below the diagonal: mirrored by the caller
-  const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
-  const int kb = sp * kchunk, ke = min(g.K, kb + kchunk);
-  const double *__restrict__ A = g.A + (long long)b * g.a_bs;
-  const double *__restrict__ B = g.B + (long long)b * g.b_bs;
   const int nk = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
 
   auto issue = [&](int kt) {  // k slice kt into stage kt % kStages
@@ -74,24 +72,18 @@ __global__ void __launch_bounds__(WM * WN * 32)
       const int e = tid + r * NT;
       const int mm = A_KC ? e / kBK : e % BM, kk = A_KC ? e % kBK : e / BM;
       const int gm = m0 + mm, gk = k0 + kk;
-      const bool ok = gm < g.M && gk < ke;
-      cp_async8(As + L::a_at(mm, kk), ok ? A + (long long)gm * g.a_rs + (long long)gk * g.a_cs : A, ok);
+      const bool ok = gm < M && gk < ke;
+      cp_async8(As + L::a_at(mm, kk), ok ? A + (long long)gm * a_rs + (long long)gk * a_cs : A, ok);
     }
 #pragma unroll
     for (int r = 0; r < LB; ++r) {
       const int e = tid + r * NT;
       const int nn = B_NC ? e % BN : e / kBK, kk = B_NC ? e / BN : e % kBK;
       const int gn = n0 + nn, gk = k0 + kk;
-      const bool ok = gn < g.N && gk < ke;
-      cp_async8(Bs + L::b_at(kk, nn), ok ? B + (long long)gk * g.b_rs + (long long)gn * g.b_cs : B, ok);
+      const bool ok = gn < N && gk < ke;
+      cp_async8(Bs + L::b_at(kk, nn), ok ? B + (long long)gk * b_rs + (long long)gn * b_cs : B, ok);
     }
   };
-
-  double acc[TM][TN][2];
-#pragma unroll
-  for (int i = 0; i < TM; ++i)
-#pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
 #pragma unroll
   for (int s = 0; s < kStages - 1; ++s) {
@@ -119,7 +111,30 @@ __global__ void __launch_bounds__(WM * WN * 32)
     }
   }
   cp_async_wait<0>();
+}
 
+template <int BM, int BN, int WM, int WN, bool A_KC, bool B_NC>
+__global__ void __launch_bounds__(WM * WN * 32)
+    dmma_gemm_kernel(const Gemm<double, double> g, const int splits, const int kchunk, double *__restrict__ partial) {
+  constexpr int TM = BM / WM / 8, TN = BN / WN / 8;  // 8 x 8 tiles per warp
+  extern __shared__ double smem[];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm0 = (warp / WN) * (BM / WM), wn0 = (warp % WN) * (BN / WN);
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  if (g.upper && n0 + BN <= m0) return;  // tile strictly below the diagonal: mirrored by the caller
+  const int b = blockIdx.z / splits, sp = blockIdx.z % splits;
+  const int kb = sp * kchunk, ke = min(g.K, kb + kchunk);
+
+  double acc[TM][TN][2];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  dmma_tile<BM, BN, WM, WN, A_KC, B_NC>(smem, g.A + (long long)b * g.a_bs, g.a_rs, g.a_cs, g.B + (long long)b * g.b_bs,
+                                        g.b_rs, g.b_cs, g.M, g.N, kb, ke, m0, n0, acc);
+
+  const int fr = lane >> 2, fc = lane & 3;
   const bool direct = splits == 1;
   double *__restrict__ C = direct ? g.C + (long long)b * g.c_bs : partial + ((long long)blockIdx.z * g.M) * g.N;
 #pragma unroll
@@ -142,6 +157,70 @@ __global__ void __launch_bounds__(WM * WN * 32)
         }
       }
   }
+}
+
+// Grouped products (dmma_grouped): each CTA walks the work items blockIdx.x, blockIdx.x + gridDim.x,
+// ...; a work item is one BM x BN output tile of the product that owns it (binary search on tile0).
+template <int BM, int BN, int WM, int WN, bool A_KC, bool B_NC>
+__global__ void __launch_bounds__(WM * WN * 32)
+    dmma_grouped_kernel(const GroupedProd *__restrict__ prods, int nprod, int total) {
+  constexpr int TM = BM / WM / 8, TN = BN / WN / 8;
+  extern __shared__ double smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm0 = (warp / WN) * (BM / WM), wn0 = (warp % WN) * (BN / WN);
+  const int fr = lane >> 2, fc = lane & 3;
+  for (int t = blockIdx.x; t < total; t += gridDim.x) {
+    int lo = 0, hi = nprod - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prods[mid].tile0 <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const GroupedProd g = prods[lo];
+    const int tt = t - g.tile0, m0 = (tt / g.tn) * BM, n0 = (tt % g.tn) * BN;
+    double acc[TM][TN][2];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+      for (int j = 0; j < TN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    __syncthreads();  // the previous work item's reads of the ring are done before it is refilled
+    dmma_tile<BM, BN, WM, WN, A_KC, B_NC>(smem, static_cast<const double *>(g.A), g.a_rs, g.a_cs,
+                                          static_cast<const double *>(g.B), g.b_rs, g.b_cs, g.M, g.N, 0, g.K, m0, n0,
+                                          acc);
+    double *__restrict__ C = static_cast<double *>(g.C);
+#pragma unroll
+    for (int i = 0; i < TM; ++i) {
+      const int gm = m0 + wm0 + 8 * i + fr;
+      if (gm >= g.M) continue;
+#pragma unroll
+      for (int j = 0; j < TN; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int gn = n0 + wn0 + 8 * j + 2 * fc + h;
+          if (gn >= g.N) continue;
+          double *c = C + (long long)gm * g.c_rs + (long long)gn * g.c_cs;
+          double v = g.alpha * acc[i][j][h];
+          if (g.beta != 0.0) v += g.beta * *c;
+          *c = v;
+        }
+    }
+  }
+}
+
+template <int BM, int BN, int WM, int WN, bool A_KC, bool B_NC>
+void dmma_grouped_launch(const GroupedProd *prods, int nprod, int total, cudaStream_t st) {
+  auto *k = dmma_grouped_kernel<BM, BN, WM, WN, A_KC, B_NC>;
+  constexpr int NT = WM * WN * 32;
+  const int bytes = kStages * DmmaLayout<BM, BN, A_KC, B_NC>::stage * (int)sizeof(double);
+  static int per_sm = 0;  // resident CTAs per SM, resolved on first use
+  if (per_sm == 0) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, bytes));
+    per_sm = std::max(1, per_sm);
+  }
+  const int grid = std::max(1, std::min(total, per_sm * Runtime::get().num_sms));
+  k<<<grid, NT, bytes, st>>>(prods, nprod, total);
+  KLAUNCHED();
 }
 
 template <int BM, int BN, int WM, int WN>
@@ -216,6 +295,24 @@ void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t
     dmma_launch<64, 64, 2, 2>(g, a_kc, b_nc, st);
   else
     dmma_launch<128, 128, 2, 4>(g, a_kc, b_nc, st);
+}
+
+int dmma_grouped_bm(int shape) { return shape == 2 ? 128 : 64; }
+int dmma_grouped_bn(int shape) { return shape == 0 ? 32 : 64; }
+
+void dmma_grouped(const GroupedProd *prods, int nprod, int total, int shape, bool a_kc, bool b_nc, cudaStream_t st) {
+  if (nprod <= 0 || total <= 0) return;
+#define ISVD_DMMA_GROUPED(BM, BN, WM, WN)                                                              \
+  if (a_kc && b_nc) dmma_grouped_launch<BM, BN, WM, WN, true, true>(prods, nprod, total, st);          \
+  else if (a_kc) dmma_grouped_launch<BM, BN, WM, WN, true, false>(prods, nprod, total, st);            \
+  else if (b_nc) dmma_grouped_launch<BM, BN, WM, WN, false, true>(prods, nprod, total, st);            \
+  else dmma_grouped_launch<BM, BN, WM, WN, false, false>(prods, nprod, total, st);
+  switch (shape) {  // warp tiles of 32 x 32 outputs (4 x 4 mma tiles)
+    case 0: ISVD_DMMA_GROUPED(64, 32, 2, 1) break;
+    case 1: ISVD_DMMA_GROUPED(64, 64, 2, 2) break;
+    default: ISVD_DMMA_GROUPED(128, 64, 4, 2) break;
+  }
+#undef ISVD_DMMA_GROUPED
 }
 
 }  // namespace isvdb

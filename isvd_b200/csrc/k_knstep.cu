@@ -399,7 +399,7 @@ int choose_cluster_size(const KnStep &a, cudaStream_t st) {
 
 }  // namespace
 
-void kn_step_grouped(const KnStep *steps, int count, int max_l, cudaStream_t st) {
+void kn_step_grouped(const KnStep *steps, int count, int max_l, int cluster, cudaStream_t st) {
   if (count <= 0) return;
   if (max_l > kKsMaxL) fail(kErrUnsupported, "Kolmogorov-Nagumo step: l = %d > %d", max_l, kKsMaxL);
   KnStep probe;
@@ -412,7 +412,8 @@ void kn_step_grouped(const KnStep *steps, int count, int max_l, cudaStream_t st)
     CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKsSmem));
     attr = true;
   }
-  cs = std::min(cs, 8);  // many clusters run side by side: eight CTAs each
+  // many clusters run side by side: `cluster` CTAs each (default eight)
+  cs = std::min(cs, cluster > 0 ? cluster : 8);
   static const KnSeries series = make_series();
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(count * cs);

@@ -59,9 +59,17 @@ __device__ __forceinline__ int pk(int i, int j, int n) {
   return i * n - (i * (i - 1)) / 2 + (j - i);
 }
 
-// One CTA per matrix: batch b at Ag + b n^2 (uniform n), or, with desc, the matrix desc[b] (its own n).
-template <bool VS>
-__global__ void __launch_bounds__(kEigThreads)
+// Largest n a CTA of nt threads solves: each thread keeps a fixed list of at most
+// eig_max_mine(nt) of the np (np + 1) / 2 block updates of a round (np = ceil(n / 2)).
+constexpr int eig_max_n(int nt) { return nt >= 1024 ? 160 : nt >= 512 ? 96 : nt >= 256 ? 64 : 32; }
+constexpr int eig_max_mine(int nt) {
+  return ((eig_max_n(nt) / 2) * (eig_max_n(nt) / 2 + 1) / 2 + nt - 1) / nt;
+}
+
+// One CTA of NT threads per matrix: batch b at Ag + b n^2 (uniform n), or, with desc, the matrix
+// desc[b] (its own n <= eig_max_n(NT)).
+template <bool VS, int NT = kEigThreads>
+__global__ void __launch_bounds__(NT)
     sym_eig_kernel(int n_uniform, const double *__restrict__ Ag, double *__restrict__ Vg, double *__restrict__ wg,
                    int order, bool absval, double *__restrict__ scratch, int *status, const EigDesc *desc) {
   extern __shared__ double sm[];
@@ -81,7 +89,7 @@ __global__ void __launch_bounds__(kEigThreads)
   int *qq = pp + np;
   int *flag = qq + np;
 
-  __shared__ double red[kEigThreads];
+  __shared__ double red[NT];
   double fr = 0.0;
   for (int e = tid; e < n * n; e += nt) {
     const int i = e / n, j = e - i * n;
@@ -104,7 +112,7 @@ __global__ void __launch_bounds__(kEigThreads)
 
   const int nblk = np * (np + 1) / 2;
   const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  constexpr int kMaxMine = (3240 + kEigThreads - 1) / kEigThreads;  // np <= 80: nblk <= 3240 (n <= 160)
+  constexpr int kMaxMine = eig_max_mine(NT);  // n <= 160, NT = 1024: np <= 80, nblk <= 3240
   short myI[kMaxMine], myJ[kMaxMine];
   int nmy = 0;
   for (int e = tid; e < nblk && nmy < kMaxMine; e += nt) {
@@ -936,10 +944,16 @@ void sym_eig_grouped(const EigDesc *desc, int count, int max_n, int order, bool 
   const size_t smem = eig_smem(max_n, true);
   if (smem > Runtime::get().smem_optin)
     fail(kErrUnsupported, "symmetric eigensolver: l = %d exceeds on-chip capacity", max_n);
-  CK(cudaFuncSetAttribute(sym_eig_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  sym_eig_kernel<true><<<count, kEigThreads, smem, st>>>(0, nullptr, nullptr, nullptr, order, absval, nullptr, status,
-                                                         desc);
-  KLAUNCHED();
+  // the smallest CTA that holds the largest matrix: small matrices leave room for many CTAs per SM
+  auto go = [&](auto kernel, int nt) {
+    CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kernel<<<count, nt, smem, st>>>(0, nullptr, nullptr, nullptr, order, absval, nullptr, status, desc);
+    KLAUNCHED();
+  };
+  if (max_n <= eig_max_n(128)) go(sym_eig_kernel<true, 128>, 128);
+  else if (max_n <= eig_max_n(256)) go(sym_eig_kernel<true, 256>, 256);
+  else if (max_n <= eig_max_n(512)) go(sym_eig_kernel<true, 512>, 512);
+  else go(sym_eig_kernel<true, kEigThreads>, kEigThreads);
 }
 
 void svd_jacobi_batched(int n, int batch, const double *B, double *U, double *s, double *V, int *status,

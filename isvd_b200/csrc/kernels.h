@@ -41,6 +41,29 @@ void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t
 // C = alpha * (sum of the `splits` partial products) + beta * C (partials: batch x splits x M x N).
 void splitk_reduce(const Gemm<double, double> &g, int splits, const double *partial, cudaStream_t st);
 
+// One product of a grouped launch over many independent products of their own shapes:
+// C = alpha A B + beta C (A M x K, B K x N, element strides as in Gemm).  Its output tiles are the
+// work items tile0 .. tile0 + ceil(M / BM) * tn - 1 of the launch (tn tiles along N).
+struct GroupedProd {
+  int M, N, K;
+  const void *A;
+  long long a_rs, a_cs;
+  const void *B;
+  long long b_rs, b_cs;
+  void *C;
+  long long c_rs, c_cs;
+  double alpha, beta;
+  int tile0, tn;
+};
+// FP64 grouped products on the FP64 tensor-core path (k_dmma.cu): one persistent launch walks the
+// `total` work items of prods[0 .. nprod) (device memory, tile0 ascending).  Every product has the
+// same operand orientation: a_kc (a_cs == 1, else a_rs == 1) and b_nc (b_cs == 1, else b_rs == 1).
+// Tile shapes: dmma_grouped_bm(shape) x dmma_grouped_bn(shape), shape < kDmmaGroupedShapes.
+constexpr int kDmmaGroupedShapes = 3;
+int dmma_grouped_bm(int shape);
+int dmma_grouped_bn(int shape);
+void dmma_grouped(const GroupedProd *prods, int nprod, int total, int shape, bool a_kc, bool b_nc, cudaStream_t st);
+
 // ------------------------------------------------------------------ elementwise
 // Omega(j, c) for j < rows, c < cols: standard normal values from Philox4x32-10 (key = seed)
 // with Box-Muller, rounded to bf16; value index = offset + j * cols + c.  Written at out[j*ld + c].
@@ -109,8 +132,11 @@ struct KnSeries {  // power-series coefficients of C(Z) and C(Z)^-1 (k_small.cu)
   double c[kSeriesLen], d[kSeriesLen];
 };
 void kn_step(const KnStep &a, cudaStream_t st);
-// count independent steps (steps in device memory, each with its own buffers; max_l >= every l)
-void kn_step_grouped(const KnStep *steps, int count, int max_l, cudaStream_t st);
+// count independent steps (steps in device memory, each with its own buffers; max_l >= every l),
+// one thread-block cluster of `cluster` CTAs per step (<= 0: eight; at most what the device
+// allows).  A step's 32 x 32 product tiles are spread over its cluster: ceil(l / 32)^2 CTAs keep
+// every CTA busy.
+void kn_step_grouped(const KnStep *steps, int count, int max_l, int cluster, cudaStream_t st);
 
 // ---------------------------------------------------------------- k_chol.cu
 enum CholMode { kCholFactor = 0, kCholInverse = 1 };
