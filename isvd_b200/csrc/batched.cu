@@ -1,14 +1,21 @@
 // Batched iSVD: many independent matrices of uneven sizes and ranks (GP / GR / KN / GR, one MPI
-// rank, products in the matrices' own type on CUDA cores, FP64 l x l steps).
+// rank, products in the matrices' own type, FP64 l x l steps).
 //
 // Every stage runs as grouped launches over all matrices instead of one launch per matrix:
 //   * products: one persistent GEMM kernel walks a list of (product, output tile) work items --
 //     the sketches, Gram matrices, applies, G = Qs'Qs products and Kolmogorov-Nagumo coefficient
-//     products of every matrix in one launch.  Its tile shape is chosen per product list by
-//     measurement on first use (every candidate computes the same result in the same order; the
-//     fastest is kept and remembered by a signature of the list);
-//   * small dense steps: the Jacobi eigensolver with one CTA per l x l matrix of its own size, and
-//     the Kolmogorov-Nagumo step with one thread-block cluster per matrix;
+//     products of every matrix in one launch; FP64 lists on the FP64 tensor cores (k_dmma.cu),
+//     the others on CUDA cores.  Its tile shape is chosen per product list by measurement on first
+//     use (the fastest candidate is kept and remembered by a signature of the list);
+//   * orthogonalization: block i of a matrix is Q_i = Y_i R_i^-1 with Y_i' Y_i = R_i' R_i (grouped
+//     Cholesky, one CTA per block), where the reference's Gramian orthogonalization takes the
+//     eigenbasis, Q_i = Y_i V_i S_i^-1.  The two bases span the same space and differ by an
+//     orthogonal l x l factor; the Kolmogorov-Nagumo iteration only sees the projectors Q_i Q_i'
+//     and the starting block Q_1 (whose rotation rotates every iterate alike, leaving the error
+//     norm, the iteration count and the postprocessed U, s, V unchanged), so the results are those
+//     of single solves to rounding, at a fraction of the eigensolves' cost;
+//   * small dense steps: the Jacobi eigensolver with one CTA per l x l matrix of its own size
+//     (postprocessing), and the Kolmogorov-Nagumo step with one thread-block cluster per matrix;
 //   * the Kolmogorov-Nagumo iterations of all matrices advance together; a matrix leaves the
 //     active set at its own convergence test, so its iteration count and error are those of a
 //     single solve.
@@ -378,7 +385,7 @@ struct Plan : BatchPlan {
   std::vector<int> m, n, k, l, Nl;
   struct Mat {  // workspace of one matrix
     DBuf<T> om, y, qs, wp, mt, qbar, z, wk, vk;
-    DBuf<double> wg, vg, lam, G, W, DD, C, Ci, F, Fs, work, wz, vz, lz;
+    DBuf<double> wg, xr, G, W, DD, C, Ci, F, Fs, work, wz, vz, lz;
   };
   std::vector<std::unique_ptr<Mat>> mats;
   DBuf<double> errs;
@@ -394,16 +401,36 @@ struct Plan : BatchPlan {
   GemmList<T, T> sketch, apply, qbar_l, proj, ul, vl;
   GemmList<T, double> gram, gfull, wzl;
   GemmList<double, double> l1, l2, l4;
-  MapList<double, T> m_scale, m_mt, m_s, m_wk, m_vk;
+  MapList<double, T> m_x, m_mt, m_s, m_wk, m_vk;
   MapList<double, double> m_init;
-  DevList<EigDesc> eig1, eig2;  // sorted by n, descending
-  std::vector<std::pair<int, int>> eig1_cls, eig2_cls;  // (first, largest n) of each size class
+  DevList<CholDesc> chol;        // the orthogonalization's block factors
+  DevList<EigDesc> eig2;         // the postprocessing's eigensolves, sorted by n, descending
+  std::vector<std::pair<int, int>> eig2_cls;  // (first, largest n) of each size class
   DevList<KnStep> steps;
   // graphs of the work before and after the iterations
   cudaGraphExec_t pre = nullptr, post = nullptr;
   unsigned long long pre_k = 0, post_k = 0;
 
-  ~Plan() override { drop_graphs(); }
+  // side streams on which the step launches of several size classes run beside each other
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+
+  ~Plan() override {
+    drop_graphs();
+    for (int i = 0; i < 2; ++i) {
+      if (side[i]) cudaStreamDestroy(side[i]);
+      if (join[i]) cudaEventDestroy(join[i]);
+    }
+    if (fork) cudaEventDestroy(fork);
+  }
+  void make_side_streams() {
+    if (fork) return;
+    CK(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    for (int i = 0; i < 2; ++i) {
+      CK(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
+    }
+  }
   void drop_graphs() {
     if (pre) cudaGraphExecDestroy(pre);
     if (post) cudaGraphExecDestroy(post);
@@ -416,8 +443,9 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
   const int B = P.count, N = P.N;
   P.sketch.clear(); P.apply.clear(); P.qbar_l.clear(); P.proj.clear(); P.ul.clear(); P.vl.clear();
   P.gram.clear(); P.gfull.clear(); P.wzl.clear();
-  P.m_scale.host.clear(); P.m_s.host.clear(); P.m_wk.host.clear(); P.m_vk.host.clear(); P.m_init.host.clear();
-  std::vector<EigDesc> e1, e2;
+  P.m_x.host.clear(); P.m_s.host.clear(); P.m_wk.host.clear(); P.m_vk.host.clear(); P.m_init.host.clear();
+  std::vector<CholDesc> c1;
+  std::vector<EigDesc> e2;
   for (int b = 0; b < B; ++b) {
     auto &M = *P.mats[b];
     const int m = P.m[b], n = P.n[b], k = P.k[b], l = P.l[b], Nl = P.Nl[b];
@@ -425,8 +453,8 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
     P.sketch.host.push_back(prod(m, Nl, n, P.a[b], P.lda[b], 1, M.om.p, Nl, 1, M.y.p, Nl, 1));
     for (int i = 0; i < N; ++i) {
       P.gram.host.push_back(prod(l, l, m, M.y.p + i * l, 1, Nl, M.y.p + i * l, Nl, 1, M.wg.p + i * ll, l, 1));
-      e1.push_back(EigDesc{l, M.wg.p + i * ll, M.vg.p + i * ll, M.lam.p + (size_t)i * l});
-      P.m_scale.host.push_back(gm(M.vg.p + i * ll, l, 1, M.wp.p + i * ll, l, 1, l, l, kMapInvSqrt, M.lam.p + i * l));
+      c1.push_back(CholDesc{l, M.wg.p + i * ll, M.xr.p + i * ll});
+      P.m_x.host.push_back(gm(M.xr.p + i * ll, l, 1, M.wp.p + i * ll, l, 1, l, l, kMapCopy));
       P.apply.host.push_back(prod(m, l, l, M.y.p + i * l, Nl, 1, M.wp.p + i * ll, l, 1, M.qs.p + i * l, Nl, 1));
     }
     P.gfull.host.push_back(prod(Nl, Nl, m, M.qs.p, 1, Nl, M.qs.p, Nl, 1, M.G.p, Nl, 1));
@@ -453,11 +481,10 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
     for (int i = 0; i < (int)e.size(); ++i)
       if (i == 0 || cl(e[i].n) != cl(e[i - 1].n)) cls.emplace_back(i, e[i].n);
   };
-  classes(e1, P.eig1_cls);
   classes(e2, P.eig2_cls);
-  P.eig1.upload(e1, st);
+  P.chol.upload(c1, st);
   P.eig2.upload(e2, st);
-  P.m_scale.prepare(st); P.m_s.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
+  P.m_x.prepare(st); P.m_s.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
 }
 
 // The grouped eigensolves of list d (classes cls: first index and largest n), one launch per class.
@@ -475,8 +502,8 @@ void run_pre(Plan<T> &P, cudaStream_t st, bool measure) {
     rng_gaussian<T>(P.mats[b]->om.p, P.n[b], P.Nl[b], P.Nl[b], P.seeds[b], 0, st);
   P.sketch.run(st, measure);
   P.gram.run(st, measure);
-  eig_classes(P.eig1, P.eig1_cls, P.status.p, st);
-  P.m_scale.launch(st);
+  chol_inv_grouped(P.chol.d.p, P.chol.count, P.max_l, P.status.p, st);
+  P.m_x.launch(st);
   P.apply.run(st, measure);
   P.gfull.run(st, measure);
   P.m_init.launch(st);
@@ -556,7 +583,7 @@ BatchPlan *batch_plan_create(int count, const int *m, const int *n, const int *k
     M->z.alloc((size_t)n[b] * l);
     M->wk.alloc((size_t)l * k[b]);
     M->vk.alloc((size_t)l * k[b]);
-    M->wg.alloc(N * ll); M->vg.alloc(N * ll); M->lam.alloc((size_t)N * l);
+    M->wg.alloc(N * ll); M->xr.alloc(N * ll);
     M->G.alloc((size_t)Nl * Nl);
     M->W.alloc(6 * nl);
     M->DD.alloc(2 * ll); M->C.alloc(ll); M->Ci.alloc(ll); M->F.alloc(ll); M->Fs.alloc(4 * ll);
@@ -635,13 +662,17 @@ void batch_solve(BatchPlan *plan, const T *const *a, const long long *lda, T *co
     P.l2.run(st, true);
     // the steps grouped by their number of 32 x 32 product tiles, nt = ceil(l / 32)^2, one launch
     // per group with the cluster size c that minimises waves x tiles per CTA,
-    // ceil(count c / SMs) ceil(nt / c) (one 1024-thread CTA per SM)
+    // ceil(count c / SMs) ceil(nt / c) (one 1024-thread CTA per SM); the groups (at most three for
+    // l <= 96) run side by side, the largest on the library stream, the others on side streams
     auto tiles_of = [](const KnStep &s) { return ((s.l + 31) / 32) * ((s.l + 31) / 32); };
     std::stable_sort(hsteps.begin(), hsteps.end(),
                      [&](const KnStep &x, const KnStep &y) { return tiles_of(x) > tiles_of(y); });
     P.steps.upload(hsteps, st);
+    P.make_side_streams();
+    CK(cudaEventRecord(P.fork, st));
+    int group = 0;
     const int sms = rt.num_sms;
-    for (size_t g0 = 0; g0 < hsteps.size();) {
+    for (size_t g0 = 0; g0 < hsteps.size(); ++group) {
       const int nt = tiles_of(hsteps[g0]);
       size_t g1 = g0;
       int lmax = 0;
@@ -653,7 +684,16 @@ void batch_solve(BatchPlan *plan, const T *const *a, const long long *lda, T *co
         const long long cost = ((cnt * c + sms - 1) / sms) * ((nt + c - 1) / c);
         if (best < 0 || cost < best) { best = cost; best_c = c; }
       }
-      kn_step_grouped(P.steps.d.p + g0, (int)cnt, lmax, best_c, st);
+      cudaStream_t gs = st;
+      if (group > 0 && group <= 2) {
+        gs = P.side[group - 1];
+        CK(cudaStreamWaitEvent(gs, P.fork, 0));
+      }
+      kn_step_grouped(P.steps.d.p + g0, (int)cnt, lmax, best_c, gs);
+      if (gs != st) {
+        CK(cudaEventRecord(P.join[group - 1], gs));
+        CK(cudaStreamWaitEvent(st, P.join[group - 1], 0));
+      }
       g0 = g1;
     }
     P.l4.run(st, true);

@@ -38,16 +38,20 @@ __device__ double block_sum(double v, double *red) {
 // only.  Each newly marked column adds 1 to *null_count.
 // perm (n ints per matrix): factor P A P' instead (row / column i of the factored matrix is
 // row / column perm[i] of A) and store X at the original positions, out[perm[i], perm[j]] = X[i, j].
+// desc (optional): matrix blockIdx.x is desc[blockIdx.x] (its own n, W and out) instead of the
+// batch entry of the uniform-size arguments.
 __global__ void __launch_bounds__(kCholThreads)
     chol_inv_kernel(int n, const double *__restrict__ W, double alpha, double shift_abs, double shift_rel,
                     double piv_rel, double *__restrict__ out, double out_scale, int mode, int *status,
-                    int *__restrict__ null_mask, int *__restrict__ null_count, const int *__restrict__ perm) {
+                    int *__restrict__ null_mask, int *__restrict__ null_count, const int *__restrict__ perm,
+                    const CholDesc *__restrict__ desc) {
   extern __shared__ double sm[];
   __shared__ double red[kCholThreads / 32];
+  if (desc) n = desc[blockIdx.x].n;
   const int ld = n + 1, tid = threadIdx.x, nt = blockDim.x;
   double *R = sm;                       // n x ld
   double *aux = sm + (size_t)n * ld;    // n: starting diagonal, then the column being inverted
-  const double *w = W + (size_t)blockIdx.x * n * n;
+  const double *w = desc ? desc[blockIdx.x].W : W + (size_t)blockIdx.x * n * n;
   const int *pm = perm ? perm + (size_t)blockIdx.x * n : nullptr;
   int *mask = null_mask ? null_mask + (size_t)blockIdx.x * n : nullptr;
   double tr = 0.0;
@@ -113,7 +117,7 @@ __global__ void __launch_bounds__(kCholThreads)
     if (tid == 0) R[j * ld + j] = inv;
     __syncthreads();
   }
-  double *o = out + (size_t)blockIdx.x * n * n;
+  double *o = desc ? desc[blockIdx.x].out : out + (size_t)blockIdx.x * n * n;
   if (mode == kCholFactor) {
     for (int e = tid; e < n * n; e += nt) {
       const int i = e / n, j = e - i * n;
@@ -303,7 +307,17 @@ void chol_inv_batched(int n, int batch, const double *W, double alpha, double sh
   if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "Cholesky: l = %d exceeds on-chip capacity", n);
   CK(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   chol_inv_kernel<<<batch, kCholThreads, smem, st>>>(n, W, alpha, shift_abs, shift_rel, piv_rel, out, out_scale,
-                                                     mode, status, null_mask, null_count, perm);
+                                                     mode, status, null_mask, null_count, perm, nullptr);
+  KLAUNCHED();
+}
+
+void chol_inv_grouped(const CholDesc *desc, int count, int max_n, int *status, cudaStream_t st) {
+  if (count <= 0 || max_n <= 0) return;
+  const size_t smem = chol_smem(max_n);
+  if (smem > Runtime::get().smem_optin) fail(kErrUnsupported, "Cholesky: l = %d exceeds on-chip capacity", max_n);
+  CK(cudaFuncSetAttribute(chol_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  chol_inv_kernel<<<count, kCholThreads, smem, st>>>(0, nullptr, 1.0, 0.0, 0.0, 0.0, nullptr, 1.0, kCholFactor, status,
+                                                     nullptr, nullptr, nullptr, desc);
   KLAUNCHED();
 }
 

@@ -153,6 +153,17 @@ constexpr int kStatusNotPD = 7;  // status word: a Cholesky pivot was not positi
 void chol_inv_batched(int n, int batch, const double *W, double alpha, double shift_abs, double shift_rel,
                       double piv_rel, double *out, double out_scale, int mode, int *status, cudaStream_t st,
                       int *null_mask = nullptr, int *null_count = nullptr, const int *perm = nullptr);
+// One matrix of a grouped factorization: n x n row-major W (upper triangle read) -> out = R^-1
+// (upper triangular, zeros below) for W = R' R.
+struct CholDesc {
+  int n;
+  const double *W;
+  double *out;
+};
+// chol_inv_batched in kCholFactor mode (alpha 1, no shift, piv_rel 0: a pivot that is not positive
+// and finite sets *status = kStatusNotPD) for count matrices of their own sizes (desc in device
+// memory, max_n >= every n).
+void chol_inv_grouped(const CholDesc *desc, int count, int max_n, int *status, cudaStream_t st);
 // Null columns of a TS factorization: y's columns c < cols with mask[c] set (cols = N l) are filled
 // with Philox4x32-10 uniform values in [-1/2, 1/2) keyed by (seed, row_offset + row, c); perm gets,
 // per block of l columns, the kept columns first and then the null ones, each in order.
