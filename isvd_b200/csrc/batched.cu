@@ -63,18 +63,40 @@ __device__ __forceinline__ void lds_vec(const T *p, T (&out)[V]) {
   }
 }
 
+// cp.async of one element (4 or 8 bytes) global -> shared, zero-filled when !valid.
+template <class T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(gmem), "r"(valid ? 8 : 0));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(d), "l"(gmem), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+constexpr int kGStages = 3, kGBK = 16;
+template <class T, int BM, int BN>
+constexpr int ggemm_smem() {  // bytes of the kGStages ring of A (BK x BM) and B (BK x BN) slices
+  return kGStages * kGBK * (BM + BN + 2 * (16 / (int)sizeof(T))) * (int)sizeof(T);
+}
+
 // Grouped products on CUDA cores: each CTA walks the work items blockIdx.x, blockIdx.x + gridDim.x,
-// ...; a work item is one BM x BN output tile of the product that owns it.  256 threads in a
-// 16 x 16 grid, each accumulating TM x TN outputs: rows ty * TM/2 + [0, TM/2) of both halves of
-// the tile (and columns likewise), so that a thread's operands of one k are two vector loads from
-// shared memory per operand.  Each output is one FMA chain in ascending k.
+// ...; a work item is one BM x BN output tile of the product that owns it.  K slices of 16 flow
+// through a kGStages-deep cp.async ring in shared memory (A stored k-major as As[k][m], B as
+// Bs[k][n]).  256 threads in a 16 x 16 grid, each accumulating TM x TN outputs: rows
+// ty * TM/2 + [0, TM/2) of both halves of the tile (and columns likewise), so that a thread's
+// operands of one k are two vector loads from shared memory per operand.  Each output is one FMA
+// chain in ascending k.
 template <class T, class Tout, int BM, int BN>
 __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restrict__ prods, int nprod, int total) {
-  constexpr int BK = 16, TM = BM / 16, TN = BN / 16, HM = TM / 2, HN = TN / 2;
+  constexpr int BK = kGBK, TM = BM / 16, TN = BN / 16, HM = TM / 2, HN = TN / 2;
   constexpr int LA = BM * BK / kGThreads, LB = BK * BN / kGThreads;
   constexpr int kPad = 16 / (int)sizeof(T);  // rows stay 16-byte aligned; transposing stores spread over banks
-  __shared__ __align__(16) T As[BK][BM + kPad];
-  __shared__ __align__(16) T Bs[BK][BN + kPad];
+  constexpr int ALD = BM + kPad, BLD = BN + kPad, STAGE = BK * (ALD + BLD);
+  extern __shared__ __align__(16) unsigned char gsm[];
+  T *ring = reinterpret_cast<T *>(gsm);
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   for (int t = blockIdx.x; t < total; t += gridDim.x) {
     int lo = 0, hi = nprod - 1;  // the product owning work item t
@@ -88,64 +110,60 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
     const T *__restrict__ A = static_cast<const T *>(g.A);
     const T *__restrict__ B = static_cast<const T *>(g.B);
     const bool akc = (g.a_cs == 1), bnc = (g.b_cs == 1);
+    const int nk = (g.K + BK - 1) / BK;
     T acc[TM][TN];
 #pragma unroll
     for (int i = 0; i < TM; ++i)
 #pragma unroll
       for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
-    T ra[LA], rb[LB];
-    auto load = [&](int k0) {
+    auto issue = [&](int kt) {  // K slice kt into stage kt % kGStages
+      T *As = ring + (kt % kGStages) * STAGE, *Bs = As + BK * ALD;
+      const int k0 = kt * BK;
 #pragma unroll
       for (int r = 0; r < LA; ++r) {
         const int e = tid + r * kGThreads;
         const int mm = akc ? e / BK : e % BM, kk = akc ? e % BK : e / BM;
         const int gm = m0 + mm, gk = k0 + kk;
-        ra[r] = (gm < g.M && gk < g.K) ? A[(long long)gm * g.a_rs + (long long)gk * g.a_cs] : T(0);
+        const bool ok = gm < g.M && gk < g.K;
+        cp_async_elem(As + kk * ALD + mm, ok ? A + (long long)gm * g.a_rs + (long long)gk * g.a_cs : A, ok);
       }
 #pragma unroll
       for (int r = 0; r < LB; ++r) {
         const int e = tid + r * kGThreads;
         const int nn = bnc ? e % BN : e / BK, kk = bnc ? e / BN : e % BK;
         const int gn = n0 + nn, gk = k0 + kk;
-        rb[r] = (gn < g.N && gk < g.K) ? B[(long long)gk * g.b_rs + (long long)gn * g.b_cs] : T(0);
+        const bool ok = gn < g.N && gk < g.K;
+        cp_async_elem(Bs + kk * BLD + nn, ok ? B + (long long)gk * g.b_rs + (long long)gn * g.b_cs : B, ok);
       }
     };
-    auto store = [&]() {
+    __syncthreads();  // the previous work item's reads of the ring are done before it is refilled
 #pragma unroll
-      for (int r = 0; r < LA; ++r) {
-        const int e = tid + r * kGThreads;
-        const int mm = akc ? e / BK : e % BM, kk = akc ? e % BK : e / BM;
-        As[kk][mm] = ra[r];
-      }
-#pragma unroll
-      for (int r = 0; r < LB; ++r) {
-        const int e = tid + r * kGThreads;
-        const int nn = bnc ? e % BN : e / BK, kk = bnc ? e / BN : e % BK;
-        Bs[kk][nn] = rb[r];
-      }
-    };
-    __syncthreads();  // the previous work item's reads of As / Bs are done
-    if (g.K > 0) load(0);
-    for (int k0 = 0; k0 < g.K; k0 += BK) {
-      store();
-      __syncthreads();
-      if (k0 + BK < g.K) load(k0 + BK);
+    for (int s0 = 0; s0 < kGStages - 1; ++s0) {
+      if (s0 < nk) issue(s0);
+      cp_async_commit_group();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+      cp_async_wait_group<kGStages - 2>();
+      __syncthreads();  // slice kt visible to all; slice kt - 1 no longer read (its stage is refilled)
+      if (kt + kGStages - 1 < nk) issue(kt + kGStages - 1);
+      cp_async_commit_group();
+      const T *As = ring + (kt % kGStages) * STAGE, *Bs = As + BK * ALD;
 #pragma unroll
       for (int kk = 0; kk < BK; ++kk) {
         T av[TM], bv[TN];
         T (&a0)[HM] = *reinterpret_cast<T(*)[HM]>(av), (&a1)[HM] = *reinterpret_cast<T(*)[HM]>(av + HM);
         T (&b0)[HN] = *reinterpret_cast<T(*)[HN]>(bv), (&b1)[HN] = *reinterpret_cast<T(*)[HN]>(bv + HN);
-        lds_vec<HM>(&As[kk][ty * HM], a0);
-        lds_vec<HM>(&As[kk][BM / 2 + ty * HM], a1);
-        lds_vec<HN>(&Bs[kk][tx * HN], b0);
-        lds_vec<HN>(&Bs[kk][BN / 2 + tx * HN], b1);
+        lds_vec<HM>(As + kk * ALD + ty * HM, a0);
+        lds_vec<HM>(As + kk * ALD + BM / 2 + ty * HM, a1);
+        lds_vec<HN>(Bs + kk * BLD + tx * HN, b0);
+        lds_vec<HN>(Bs + kk * BLD + BN / 2 + tx * HN, b1);
 #pragma unroll
         for (int i = 0; i < TM; ++i)
 #pragma unroll
           for (int j = 0; j < TN; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
       }
-      __syncthreads();
     }
+    cp_async_wait_group<0>();
     Tout *__restrict__ C = static_cast<Tout *>(g.C);
 #pragma unroll
     for (int i = 0; i < TM; ++i) {
@@ -162,6 +180,21 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
       }
     }
   }
+}
+
+template <class T, class Tout, int BM, int BN>
+void ggemm_launch(const GProd *prods, int nprod, int total, cudaStream_t st) {
+  auto *k = ggemm_kernel<T, Tout, BM, BN>;
+  constexpr int bytes = ggemm_smem<T, BM, BN>();
+  static int per_sm = 0;  // resident CTAs per SM, resolved on first use
+  if (per_sm == 0) {
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kGThreads, bytes));
+    per_sm = std::max(1, per_sm);
+  }
+  const int grid = std::max(1, std::min(total, per_sm * Runtime::get().num_sms));
+  k<<<grid, kGThreads, bytes, st>>>(prods, nprod, total);
+  KLAUNCHED();
 }
 
 // ---------------------------------------------------------------- grouped elementwise
@@ -279,13 +312,11 @@ struct GemmList {
       dmma_grouped(static_cast<const GroupedProd *>(dev.d.p), dev.count, total, cfg, a_kc, b_nc, st);
       return;
     }
-    const int grid = std::max(1, std::min(total, 4 * Runtime::get().num_sms));
     switch (cfg) {
-      case 0: ggemm_kernel<T, Tout, 64, 64><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
-      case 1: ggemm_kernel<T, Tout, 128, 64><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
-      default: ggemm_kernel<T, Tout, 128, 128><<<grid, kGThreads, 0, st>>>(dev.d.p, dev.count, total); break;
+      case 0: ggemm_launch<T, Tout, 64, 64>(dev.d.p, dev.count, total, st); break;
+      case 1: ggemm_launch<T, Tout, 128, 64>(dev.d.p, dev.count, total, st); break;
+      default: ggemm_launch<T, Tout, 128, 128>(dev.d.p, dev.count, total, st); break;
     }
-    KLAUNCHED();
   }
   // Choose the tile shape (measuring every candidate on first sight of the signature when all
   // products overwrite their outputs) and upload the work items.  May run the products.
@@ -312,6 +343,7 @@ struct GemmList {
         int bestc = 0;
         for (int cfg = 0; cfg < (dmma ? kDmmaGroupedShapes : kConfigs); ++cfg) {
           finalize(cfg, st);
+          launch(cfg, st);  // untimed: a kernel's first launch sets its attributes on the host
           CK(cudaEventRecord(e0, st));
           launch(cfg, st);
           CK(cudaEventRecord(e1, st));

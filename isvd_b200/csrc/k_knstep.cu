@@ -43,7 +43,19 @@ constexpr int kKsPer = (32 * kKsMaxL + kKsThreads - 1) / kKsThreads;
 struct Ks {
   int l, nr, cs, rank;
   double *As, *Bs, *part;
+  // one-CTA steps (cs == 1) with l <= kKsFullL: both operands of a product staged whole in shared
+  // memory (A: roundup(l, 32) rows of row stride ald, B: l4 rows of row stride bld), so that the
+  // CTA's nr^2 tiles read L2 once per product instead of once per tile
+  bool full;
+  int ald, bld;
 };
+constexpr int kKsFullL = 96;
+__host__ __device__ constexpr int ks_full_ld(int l) { return (l + 31) / 32 * 32 + 4; }  // 4 (mod 16) doubles
+// dynamic shared memory of the whole-operand layout: A, B and the two halves' 32 x 32 partial sums
+__host__ __device__ constexpr size_t ks_full_smem(int l) {
+  return ((size_t)((l + 31) / 32 * 32) * ks_full_ld(l) + (size_t)((l + 3) & ~3) * ks_full_ld(l) + 2 * 1024) *
+         sizeof(double);
+}
 
 // C = alpha A B + beta Cin + diag I on the 32 x 32 output tiles [tile_begin, tile_end) of a phase
 // (tiles numbered across the products of the phase); CTA r takes the tiles t = r mod cs.
@@ -60,6 +72,47 @@ __device__ void ks_mm(const Ks &k, int tile_begin, int tile_end, double alpha, c
   const int lane = tid & 31, half = ty >> 4, mt = ty & 15, ti = mt >> 2, tj = mt & 3;  // warp: 8 x 8 tile, half
   const int l4 = (l + 3) & ~3, kh = ((l4 >> 1) + 3) & ~3;
   const int kb = half * kh, ke = min(l4, kb + kh);
+  if (k.full) {  // cs == 1: every tile of [tile_begin, tile_end) in this CTA, operands staged once
+    const int lr = (l + 31) & ~31;
+    __syncthreads();  // the previous product's reads of the staged operands are done
+    for (int e = tid; e < lr * k.ald; e += kKsThreads) {  // A rows [0, lr) x columns [0, ald), zero outside l x l
+      const int r = e / k.ald, cc = e - r * k.ald;
+      k.As[e] = (r < l && cc < l) ? __ldcg(A + (size_t)r * l + cc) : 0.0;
+    }
+    for (int e = tid; e < l4 * k.bld; e += kKsThreads) {  // B rows [0, l4) x columns [0, bld)
+      const int r = e / k.bld, cc = e - r * k.bld;
+      k.Bs[e] = (r < l && cc < l) ? __ldcg(B + (size_t)r * l + cc) : 0.0;
+    }
+    __syncthreads();
+    for (int t = tile_begin; t < tile_end; ++t) {
+      const int tt = t - tile_begin;
+      const int i0 = (tt / k.nr) * 32, j0 = (tt % k.nr) * 32;
+      const int i = i0 + ty, j = j0 + tx;
+      const double cin = (beta != 0.0 && i < l && j < l) ? __ldcg(Cin + (size_t)i * l + j) : 0.0;
+      double d[2] = {0.0, 0.0};
+      const double *ap = k.As + (i0 + ti * 8 + (lane >> 2)) * k.ald + (lane & 3);
+      const double *bq = k.Bs + (lane & 3) * k.bld + j0 + tj * 8 + (lane >> 2);
+      for (int kk = kb; kk < ke; kk += 4)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                     : "+d"(d[0]), "+d"(d[1])
+                     : "d"(ap[kk]), "d"(bq[kk * k.bld]));
+      double *part = k.part + half * 1024;
+      const int orow = ti * 8 + (lane >> 2), ocol = tj * 8 + 2 * (lane & 3);
+      __syncthreads();  // the previous tile's epilogue reads of the partial sums are done
+      part[orow * 32 + ocol] = d[0];
+      part[orow * 32 + ocol + 1] = d[1];
+      __syncthreads();
+      const int o = ty * 32 + tx;
+      const double acc = k.part[o] + k.part[1024 + o];
+      if (i < l && j < l) {
+        const double v = alpha * acc + beta * cin + (i == j ? diag : 0.0);
+        C[(size_t)i * l + j] = v;
+        if (C2) C2[(size_t)i * l + j] = v;
+        if (C3) C3[(size_t)i * l + j] = v;
+      }
+    }
+    return;
+  }
   const int first = tile_begin + (((k.rank - tile_begin) % k.cs) + k.cs) % k.cs;
   for (int t = first; t < tile_end; t += k.cs) {
     const int tt = t - tile_begin;
@@ -189,7 +242,7 @@ __device__ int ks_block_size(int deg) {
   return sb;
 }
 
-__device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries &ser) {
+__device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries &ser, bool full = false) {
   extern __shared__ double sm[];
   __shared__ double red[kKsThreads / 32];
   __shared__ int plan[3];  // degree (-1: Newton-Schulz), block size, Newton-Schulz steps
@@ -197,7 +250,14 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
   const int l = a.l;
   const size_t ll = (size_t)l * l;
   Ks k{l, (l + 31) / 32, (int)cluster.num_blocks(), (int)cluster.block_rank(), sm, sm + 32 * kAld,
-         sm + 32 * kAld + (kKsMaxL + 4) * kBld};
+         sm + 32 * kAld + (kKsMaxL + 4) * kBld, false, kAld, kBld};
+  if (full) {  // the whole-operand layout (the launch sized the dynamic shared memory for it)
+    k.full = true;
+    k.ald = k.bld = ks_full_ld(l);
+    k.As = sm;
+    k.Bs = sm + (size_t)((l + 31) / 32 * 32) * k.ald;
+    k.part = k.Bs + (size_t)((l + 3) & ~3) * k.bld;
+  }
   const int nt = k.nr * k.nr;
   const int gtid = k.rank * kKsThreads + threadIdx.x, gstride = k.cs * kKsThreads;
   // work: Z | P_1..P_8 | accC x2 | accCi x2 | BC_0..BC_7 | BI_0..BI_7 (Newton-Schulz: P_1..P_5), then
@@ -332,9 +392,11 @@ __device__ __forceinline__ void kn_cluster_body(const KnStep &a, const KnSeries 
 __global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_kernel(KnStep a, KnSeries ser) { kn_cluster_body(a, ser); }
 
 // One cluster per step of steps[] (grid = count x cluster size): many independent problems.
-__global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_grouped_kernel(const KnStep *steps, KnSeries ser) {
+// full: one-CTA clusters with the whole-operand product layout (every l <= kKsFullL).
+__global__ void __launch_bounds__(kKsThreads, 1) kn_cluster_grouped_kernel(const KnStep *steps, KnSeries ser,
+                                                                         int full) {
   const KnStep a = steps[blockIdx.x / cg::this_cluster().num_blocks()];
-  kn_cluster_body(a, ser);
+  kn_cluster_body(a, ser, full != 0);
 }
 
 // Coefficients of g(z)^(1/2) and g(z)^(-1/2), g(z) = 1 - sum_{n>=1} Cat(n-1) z^n: for h = f^alpha
@@ -406,19 +468,21 @@ void kn_step_grouped(const KnStep *steps, int count, int max_l, int cluster, cud
   probe.l = max_l;
   int cs = choose_cluster_size(probe, st);
   if (cs == 0) fail(kErrUnsupported, "grouped Kolmogorov-Nagumo step: no thread-block cluster launch on this device");
+  const size_t smem_max = std::max(kKsSmem, ks_full_smem(kKsFullL));
   static bool attr = false;
   if (!attr) {
     CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kKsSmem));
+    CK(cudaFuncSetAttribute(kn_cluster_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
     attr = true;
   }
   // many clusters run side by side: `cluster` CTAs each (default eight)
   cs = std::min(cs, cluster > 0 ? cluster : 8);
+  const int full = (cs == 1 && max_l <= kKsFullL) ? 1 : 0;
   static const KnSeries series = make_series();
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(count * cs);
   cfg.blockDim = dim3(kKsThreads);
-  cfg.dynamicSmemBytes = kKsSmem;
+  cfg.dynamicSmemBytes = full ? std::max(kKsSmem, ks_full_smem(max_l)) : kKsSmem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -427,7 +491,7 @@ void kn_step_grouped(const KnStep *steps, int count, int max_l, int cluster, cud
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  CK(cudaLaunchKernelEx(&cfg, kn_cluster_grouped_kernel, steps, series));
+  CK(cudaLaunchKernelEx(&cfg, kn_cluster_grouped_kernel, steps, series, full));
   KLAUNCHED();
 }
 
