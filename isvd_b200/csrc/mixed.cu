@@ -214,7 +214,7 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
 
 template <class T>
 void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G,
-                     int np) {
+                     int np, bool all_pairs) {
   UmmaGemm g;
   g.M = Nl; g.N = Nl; g.K = m;
   PlaneBuf qt;
@@ -228,6 +228,11 @@ void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T
     g.A = qt.P; g.B = qt.P;
   }
   set_products(g, np, np);
+  if (all_pairs) {
+    g.nprod = 0;
+    for (int p = 0; p < np; ++p)
+      for (int q = 0; q < np; ++q) { g.pa[g.nprod] = p; g.pb[g.nprod] = q; ++g.nprod; }
+  }
   g.C = G; g.c_double = true; g.c_rs = Nl; g.c_cs = 1;
   g.upper = true;
   g.status = c.status;
@@ -346,7 +351,7 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, long long 
   template void mixed_block_apply<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
                                      const T *, T *, long long);                                           \
   template void mixed_gram_full<T>(const StageCtx &, const Planes &, int, int, const T *, long long,          \
-                                   double *, int);                                                              \
+                                   double *, int, bool);                                                        \
   template void mixed_apply_coeff<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
                                      const double *, T *, long long);                                      \
   template void mixed_project<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *,     \

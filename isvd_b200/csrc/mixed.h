@@ -66,9 +66,11 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
                        const T *Wp, T *out, long long ldo);
 
 // G = Qs' Qs (Nl x Nl, FP64 out; symmetric, computed on the upper triangle and mirrored).
+// all_pairs: every plane product (p, q < np), so that G is the Gram of the planes' sum itself (to
+// FP32 accumulation), instead of the products above the FP32 rounding level of the matrix.
 template <class T>
 void mixed_gram_full(const StageCtx &c, const Planes &qp, int m, int Nl, const T *qs, long long ldq, double *G,
-                     int np = 2);
+                     int np = 2, bool all_pairs = false);
 
 // Qbar = Qs M (M: Nl x l FP64, row-major) -> qt (m x l, ld ldqt).
 template <class T>

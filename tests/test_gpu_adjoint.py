@@ -91,12 +91,17 @@ def test_adjoint_matches_dense_svd_gradient(lib, ordera):
 
 
 @pytest.mark.parametrize("ordera", [b"R", b"C"])
-@pytest.mark.parametrize("precision", [0, 1], ids=["native", "mixed"])
-def test_adjoint_fp32_u_and_v_terms(lib, ordera, precision):
+@pytest.mark.parametrize("precision,operator", [(0, "a"), (1, "gram"), (1, "a")],
+                         ids=["native", "mixed-gram", "mixed-in-a"])
+def test_adjoint_fp32_u_and_v_terms(lib, monkeypatch, ordera, precision, operator):
     """FP32 adjoint with both complement systems (dU and dV), A row- and column-major, NATIVE and
-    MIXED (products by A on the tensor cores), against the FP64 dense gradient of
-    L = w's + ||U U' X||_F^2 + ||V V' Y||_F^2."""
+    MIXED (products on the tensor cores), against the FP64 dense gradient of
+    L = w's + ||U U' X||_F^2 + ||V V' Y||_F^2.  MIXED runs the complement systems in the
+    coordinates of B'B (the default for n <= m) and, with ISVD_GPU_ADJOINT_CG_A=1, with the
+    operator in A (both systems in one pass over A per product)."""
     torch = pytest.importorskip("torch")
+    if operator == "a":
+        monkeypatch.setenv("ISVD_GPU_ADJOINT_CG_A", "1")
     a, k, w, xx = slice_case(11)
     yy = np.random.default_rng(12).standard_normal((a.shape[1], 8))
     at = torch.tensor(a, dtype=torch.float64, requires_grad=True)
