@@ -107,6 +107,7 @@ __global__ void __launch_bounds__(kGThreads) ggemm_kernel(const GProd *__restric
     }
     const GProd g = prods[lo];
     const int tt = t - g.tile0, m0 = (tt / g.tn) * BM, n0 = (tt % g.tn) * BN;
+    if (g.upper && n0 + BN <= m0) continue;  // strictly below the diagonal (uniform in the CTA)
     const T *__restrict__ A = static_cast<const T *>(g.A);
     const T *__restrict__ B = static_cast<const T *>(g.B);
     const bool akc = (g.a_cs == 1), bnc = (g.b_cs == 1);
@@ -207,7 +208,8 @@ struct GMap {  // dst(r, c) = f(src(r, c), w[c]) over rows x cols
   const double *w;
   int mode;
 };
-enum { kMapCopy = 0, kMapInvSqrt = 1, kMapSqrt = 2, kMapIdentity = 3 };
+// kMapMirror: the strictly lower triangle from the upper one, dst(r, c) = src(c, r) for r > c
+enum { kMapCopy = 0, kMapInvSqrt = 1, kMapSqrt = 2, kMapIdentity = 3, kMapMirror = 4 };
 
 template <class Ts, class Td>
 __global__ void gmap_kernel(const GMap *__restrict__ maps) {
@@ -221,6 +223,9 @@ __global__ void gmap_kernel(const GMap *__restrict__ maps) {
     double v;
     if (g.mode == kMapIdentity) {
       v = (r == c) ? 1.0 : 0.0;
+    } else if (g.mode == kMapMirror) {
+      if (r <= c) continue;
+      v = (double)src[c * g.s_rs + r * g.s_cs];
     } else {
       const double x = (double)src[r * g.s_rs + c * g.s_cs];
       v = g.mode == kMapInvSqrt ? x / sqrt(g.w[c]) : g.mode == kMapSqrt ? sqrt(x) : x;
@@ -398,6 +403,7 @@ inline GProd prod(int M, int N, int K, const void *A, long long a_rs, long long 
   g.C = C; g.c_rs = c_rs; g.c_cs = c_cs;
   g.alpha = alpha; g.beta = 0.0;
   g.tile0 = 0; g.tn = 1;
+  g.upper = 0;
   return g;
 }
 
@@ -434,7 +440,7 @@ struct Plan : BatchPlan {
   GemmList<T, double> gram, gfull, wzl;
   GemmList<double, double> l1, l2, l4;
   MapList<double, T> m_x, m_mt, m_s, m_wk, m_vk;
-  MapList<double, double> m_init;
+  MapList<double, double> m_init, m_mirror;
   DevList<CholDesc> chol;        // the orthogonalization's block factors
   DevList<EigDesc> eig2;         // the postprocessing's eigensolves, sorted by n, descending
   std::vector<std::pair<int, int>> eig2_cls;  // (first, largest n) of each size class
@@ -475,7 +481,7 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
   const int B = P.count, N = P.N;
   P.sketch.clear(); P.apply.clear(); P.qbar_l.clear(); P.proj.clear(); P.ul.clear(); P.vl.clear();
   P.gram.clear(); P.gfull.clear(); P.wzl.clear();
-  P.m_x.host.clear(); P.m_s.host.clear(); P.m_wk.host.clear(); P.m_vk.host.clear(); P.m_init.host.clear();
+  P.m_x.host.clear(); P.m_s.host.clear(); P.m_mirror.host.clear(); P.m_wk.host.clear(); P.m_vk.host.clear(); P.m_init.host.clear();
   std::vector<CholDesc> c1;
   std::vector<EigDesc> e2;
   for (int b = 0; b < B; ++b) {
@@ -490,6 +496,8 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
       P.apply.host.push_back(prod(m, l, l, M.y.p + i * l, Nl, 1, M.wp.p + i * ll, l, 1, M.qs.p + i * l, Nl, 1));
     }
     P.gfull.host.push_back(prod(Nl, Nl, m, M.qs.p, 1, Nl, M.qs.p, Nl, 1, M.G.p, Nl, 1));
+    P.gfull.host.back().upper = 1;  // G = Qs'Qs symmetric: the upper triangle's tiles, then mirrored
+    P.m_mirror.host.push_back(gm(M.G.p, Nl, 1, M.G.p, Nl, 1, Nl, Nl, kMapMirror));
     // iterate [M | B | Bgc] in W[0]: Bc = G[:, 0:l], M = [I; 0]
     P.m_init.host.push_back(gm(M.G.p, Nl, 1, M.W.p + l, 3 * l, 1, Nl, l, kMapCopy));
     P.m_init.host.push_back(gm(nullptr, 0, 0, M.W.p, 3 * l, 1, Nl, l, kMapIdentity));
@@ -516,7 +524,7 @@ void build_lists(Plan<T> &P, cudaStream_t st) {
   classes(e2, P.eig2_cls);
   P.chol.upload(c1, st);
   P.eig2.upload(e2, st);
-  P.m_x.prepare(st); P.m_s.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
+  P.m_x.prepare(st); P.m_s.prepare(st); P.m_mirror.prepare(st); P.m_wk.prepare(st); P.m_vk.prepare(st); P.m_init.prepare(st);
 }
 
 // The grouped eigensolves of list d (classes cls: first index and largest n), one launch per class.
@@ -538,6 +546,7 @@ void run_pre(Plan<T> &P, cudaStream_t st, bool measure) {
   P.m_x.launch(st);
   P.apply.run(st, measure);
   P.gfull.run(st, measure);
+  P.m_mirror.launch(st);
   P.m_init.launch(st);
 }
 

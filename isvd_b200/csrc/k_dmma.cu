@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(WM * WN * 32)
     }
     const GroupedProd g = prods[lo];
     const int tt = t - g.tile0, m0 = (tt / g.tn) * BM, n0 = (tt % g.tn) * BN;
+    if (g.upper && n0 + BN <= m0) continue;  // strictly below the diagonal (uniform in the CTA)
     double acc[TM][TN][2];
 #pragma unroll
     for (int i = 0; i < TM; ++i)

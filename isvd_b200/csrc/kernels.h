@@ -54,6 +54,7 @@ struct GroupedProd {
   long long c_rs, c_cs;
   double alpha, beta;
   int tile0, tn;
+  int upper;  // C symmetric (A = B'): tiles entirely below the diagonal are skipped (mirrored by the caller)
 };
 // FP64 grouped products on the FP64 tensor-core path (k_dmma.cu): one persistent launch walks the
 // `total` work items of prods[0 .. nprod) (device memory, tile0 ascending).  Every product has the
