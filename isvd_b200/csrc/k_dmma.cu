@@ -298,8 +298,8 @@ void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t
     dmma_launch<128, 128, 2, 4>(g, a_kc, b_nc, st);
 }
 
-int dmma_grouped_bm(int shape) { return shape == 2 ? 128 : 64; }
-int dmma_grouped_bn(int shape) { return shape == 0 ? 32 : 64; }
+int dmma_grouped_bm(int shape) { return shape == 2 ? 128 : shape == 4 ? 32 : 64; }
+int dmma_grouped_bn(int shape) { return (shape == 0 || shape >= 3) ? 32 : 64; }
 
 void dmma_grouped(const GroupedProd *prods, int nprod, int total, int shape, bool a_kc, bool b_nc, cudaStream_t st) {
   if (nprod <= 0 || total <= 0) return;
@@ -308,10 +308,12 @@ void dmma_grouped(const GroupedProd *prods, int nprod, int total, int shape, boo
   else if (a_kc) dmma_grouped_launch<BM, BN, WM, WN, true, false>(prods, nprod, total, st);            \
   else if (b_nc) dmma_grouped_launch<BM, BN, WM, WN, false, true>(prods, nprod, total, st);            \
   else dmma_grouped_launch<BM, BN, WM, WN, false, false>(prods, nprod, total, st);
-  switch (shape) {  // warp tiles of 32 x 32 outputs (4 x 4 mma tiles)
+  switch (shape) {  // warp tiles of 32 x 32 outputs (4 x 4 mma tiles), or 32 x 16 (shape 3)
     case 0: ISVD_DMMA_GROUPED(64, 32, 2, 1) break;
     case 1: ISVD_DMMA_GROUPED(64, 64, 2, 2) break;
-    default: ISVD_DMMA_GROUPED(128, 64, 4, 2) break;
+    case 2: ISVD_DMMA_GROUPED(128, 64, 4, 2) break;
+    case 3: ISVD_DMMA_GROUPED(64, 32, 2, 2) break;
+    default: ISVD_DMMA_GROUPED(32, 32, 1, 1) break;
   }
 #undef ISVD_DMMA_GROUPED
 }

@@ -60,7 +60,7 @@ struct GroupedProd {
 // `total` work items of prods[0 .. nprod) (device memory, tile0 ascending).  Every product has the
 // same operand orientation: a_kc (a_cs == 1, else a_rs == 1) and b_nc (b_cs == 1, else b_rs == 1).
 // Tile shapes: dmma_grouped_bm(shape) x dmma_grouped_bn(shape), shape < kDmmaGroupedShapes.
-constexpr int kDmmaGroupedShapes = 3;
+constexpr int kDmmaGroupedShapes = 5;
 int dmma_grouped_bm(int shape);
 int dmma_grouped_bn(int shape);
 void dmma_grouped(const GroupedProd *prods, int nprod, int total, int shape, bool a_kc, bool b_nc, cudaStream_t st);
