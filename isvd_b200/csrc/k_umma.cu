@@ -1256,6 +1256,11 @@ static bool pair_mn_ok(const UmmaGemm &g) {
   const long long tiles = (long long)((g.N + 255) / 256) * ((g.M + 255) / 256);
   return tiles >= Runtime::get().num_sms / 2 && g.K >= 1024 && g.A.np + g.B.np <= 4;
 }
+// ISVD_UMMA_WIDE_MN=0: MN-major B products keep 128-wide tiles (for comparison)
+static bool wide_mn_off() {
+  const char *e = getenv("ISVD_UMMA_WIDE_MN");
+  return e && atoi(e) == 0;
+}
 static bool smalln_bk64() {
   const char *e = getenv("ISVD_UMMA_SMALLN_BK");
   return e && atoi(e) == 64;
@@ -1286,7 +1291,10 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   } else if (amn) {
     fail(kErrUnsupported, "tcgen05 GEMM: MN-major A needs MN-major B");
   } else if (bmn) {
-    launch_t<128, 64, false, true>(g, st, status);
+    // wide MN-major B against at most 128 rows of A (the projection Z' = Qbar' A, n columns): 256-wide
+    // tiles read the A operand half as often from L2 (32-deep k-blocks keep four pipeline stages)
+    if (g.M <= BM && g.N >= 2048 && !g.upper && !wide_mn_off()) launch_t<256, 32, false, true>(g, st, status);
+    else launch_t<128, 64, false, true>(g, st, status);
   } else if (g.N <= 64) {
     // narrow outputs (N <= 64, e.g. products with k or l columns): 64-wide tiles, no half-empty MMAs
     launch_t<64, 64, false, false>(g, st, status);
