@@ -589,6 +589,20 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   // Omega passed in: all n rows; column blocks use the rows of their own columns
   if (omega) Om.bind(omega + (colblk ? (size_t)p.colidxbegin * ldomega : 0), Nl, acols, ldomega, true, st);
   DBuf<T> Y((size_t)ml * Nl), Q((size_t)ml * l);
+  // MIXED GP / GR / (KN | WY) on one process: the sketch and the Gramian apply hand their outputs
+  // to the next stage as bf16 planes (what that stage would split them into), so Y and Qs are never
+  // written as values nor split again (ISVD_GPU_PLANE_HANDOFF=0 keeps the values)
+  PlaneHandoff hand;
+  struct HandoffScope {
+    StageCtx &sc;
+    ~HandoffScope() { sc.handoff = nullptr; }
+  } hand_scope{c.sc};
+  {
+    const char *e = getenv("ISVD_GPU_PLANE_HANDOFF");
+    if (mixed && !multi && bo == "GR" && (bi == "KN" || bi == "WY") && l % 64 == 0 && handoff_shape_ok(Nl) &&
+        !(e && atoi(e) == 0))
+      c.sc.handoff = &hand;
+  }
   if (colblk) {  // Y = sum over the ranks of A_j Omega_j, then this rank's rows (reference
     DBuf<T> Yf((size_t)m * Nl);  // MPI_Reduce_scatter_block, @x@_sketch.h:82)
     sketch_dev<T>(c.sc, m, acols, Nl, ordera_, a_use, lda, omega ? Om.d : nullptr, ldomega, (uint64_t)(uint32_t)seed,
@@ -650,6 +664,7 @@ void driver(const isvd_Param &p, const char *alg_s, const char *alg_o, const cha
   } else {
     integrate_hr_dev<T>(c.sc, ml, l, N, Y.p, Nl, Q.p, l);
   }
+  c.sc.handoff = nullptr;
   tm.mark(3, st);
   sync();
   done();

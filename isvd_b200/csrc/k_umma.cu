@@ -52,9 +52,39 @@ struct KParams {
   int stage_out;  // epilogue stages its rows through shared memory (C rows contiguous)
   int bloop;      // one CTA runs every batch of its tile in turn (grid z = 1, no split-K)
   int vec_out;    // direct epilogue stores as 16-byte vectors (C rows contiguous and aligned)
+  __nv_bfloat16 *pl;  // optional bf16 planes of the output (UmmaGemm::planes)
+  long long pl_ld, pl_ps;
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// The three bf16 planes of an output value v = alpha acc, split as split_planes splits the stored
+// value: FP32 pieces of the FP32-rounded value, or FP64 pieces of the FP64 value.
+__device__ __forceinline__ void out_pieces(double v, int c_double, __nv_bfloat16 *o) {
+  if (c_double) {
+    double r = v;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const __nv_bfloat16 h = __double2bfloat16(r);
+      o[q] = h;
+      r -= (double)__bfloat162float(h);
+    }
+  } else {
+    const float x = (float)v;
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(h0);
+    const __nv_bfloat16 h1 = __float2bfloat16_rn(r1);
+    o[0] = h0;
+    o[1] = h1;
+    o[2] = __float2bfloat16_rn(r1 - __bfloat162float(h1));
+  }
+}
+__device__ __forceinline__ void store_pieces(const KParams &p, long long off, double v) {
+  __nv_bfloat16 o[3];
+  out_pieces(v, p.c_double, o);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) p.pl[q * p.pl_ps + off] = o[q];
+}
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(bar)), "r"(count));
@@ -388,6 +418,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (gn >= p.N || (p.upper && gn < gr)) continue;
           const float v = stg[r * SROW + t * 32 + lane];
           if (p.splits == 1) {
+            if (p.pl) store_pieces(p, (long long)b * p.c_step + (long long)gr * p.pl_ld + gn, p.alpha * (double)v);
+            if (!p.C) continue;
             const long long off = (long long)b * p.c_step + (long long)gr * p.c_rs + (long long)gn * p.c_cs;
             if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)v;
             else ((float *)p.C)[off] = (float)(p.alpha * (double)v);
@@ -400,9 +432,28 @@ __global__ void __launch_bounds__(kThreads, 1)
       // this thread's row: 16-byte stores of 4 (FP32) or 2 (FP64) consecutive columns
       const int gn0 = n0 + h * C::HALF;
       const long long off0 = (long long)b * p.c_step + (long long)gm * p.c_rs + gn0;
+      if (p.pl) {  // eight consecutive columns: one 16-byte store per plane (N, ld, steps multiples of 8)
+        const long long po0 = (long long)b * p.c_step + (long long)gm * p.pl_ld + gn0;
+#pragma unroll
+        for (int j = 0; j < C::HALF; j += 8) {
+          if (gn0 + j >= p.N) break;
+          __nv_bfloat16 o[8][3];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) out_pieces(p.alpha * (double)acc[j + u], p.c_double, o[u]);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            uint4 w;
+            w.x = (uint32_t)__bfloat16_as_ushort(o[0][q]) | ((uint32_t)__bfloat16_as_ushort(o[1][q]) << 16);
+            w.y = (uint32_t)__bfloat16_as_ushort(o[2][q]) | ((uint32_t)__bfloat16_as_ushort(o[3][q]) << 16);
+            w.z = (uint32_t)__bfloat16_as_ushort(o[4][q]) | ((uint32_t)__bfloat16_as_ushort(o[5][q]) << 16);
+            w.w = (uint32_t)__bfloat16_as_ushort(o[6][q]) | ((uint32_t)__bfloat16_as_ushort(o[7][q]) << 16);
+            *(uint4 *)(p.pl + q * p.pl_ps + po0 + j) = w;
+          }
+        }
+      }
 #pragma unroll
       for (int j = 0; j < C::HALF; j += 4) {
-        if (gn0 + j >= p.N) break;  // N % 4 == 0: a group is either whole or outside
+        if (!p.C || gn0 + j >= p.N) break;  // N % 4 == 0: a group is either whole or outside
         if (p.c_double) {
           double2 *o = (double2 *)((double *)p.C + off0 + j);
           o[0] = make_double2(p.alpha * (double)acc[j], p.alpha * (double)acc[j + 1]);
@@ -421,6 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (gn >= p.N) break;
         if (upper_tile && gn < gm) continue;
         if (p.splits == 1) {
+          if (p.pl) store_pieces(p, (long long)b * p.c_step + (long long)gm * p.pl_ld + gn, p.alpha * (double)acc[j]);
+          if (!p.C) continue;
           const long long off = (long long)b * p.c_step + (long long)gm * p.c_rs + (long long)gn * p.c_cs;
           if (p.c_double) ((double *)p.C)[off] = p.alpha * (double)acc[j];
           else ((float *)p.C)[off] = (float)(p.alpha * (double)acc[j]);
@@ -1017,6 +1070,8 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   if ((AMN && g.a_mn_step % 8) || (BMN && g.b_mn_step % 8))
     fail(kErrArgument, "tcgen05 GEMM: MN-major operand batch steps must be multiples of 8 elements");
   p.C = g.C; p.c_double = g.c_double;
+  p.pl = g.planes; p.pl_ld = g.p_ld; p.pl_ps = g.p_ps;
+  if (g.planes && (g.c_cs != 1 || g.upper)) fail(kErrArgument, "tcgen05 GEMM: plane output needs unit column stride");
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;
@@ -1050,6 +1105,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
         break;
       }
   }
+  if (g.planes) splits = 1;  // the planes are written by the epilogue: no split-K partials
   splits = std::max(1, std::min(splits, p.total_kb));
   p.kbps = (p.total_kb + splits - 1) / splits;
   p.splits = (p.total_kb + p.kbps - 1) / p.kbps;
@@ -1071,7 +1127,9 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   // each one accumulation segment, instead of one CTA per (tile, batch) that would mostly set up
   p.bloop = (BN <= 128 && g.batch > 1 && p.splits == 1 && p.total_kb <= 16) ? 1 : 0;
   p.stage_out = (!p.bloop && (p.splits > 1 || g.c_cs == 1) && stages * stage_bytes >= 8 * 32 * (C::HALF + 1) * 4) ? 1 : 0;
+  if (g.planes_in_place && !p.bloop) fail(kErrUnsupported, "tcgen05 GEMM: in-place plane output needs the batch loop");
   p.vec_out = (BN <= 128 && g.c_cs == 1 && !g.upper && g.N % 4 == 0 && g.c_rs % 4 == 0 && g.c_step % 4 == 0 &&
+               (!g.planes || (g.N % 8 == 0 && g.p_ld % 8 == 0 && g.c_step % 8 == 0 && ((uintptr_t)g.planes % 16) == 0)) &&
                ((uintptr_t)g.C % 16) == 0) ? 1 : 0;
   if (stages < 2) fail(kErrUnsupported, "tcgen05 GEMM: %d planes do not fit in shared memory", g.A.np + g.B.np);
   const size_t smem = (size_t)stages * stage_bytes + 1024 + 256;
@@ -1117,6 +1175,7 @@ void launch_pair(const UmmaGemm &g, cudaStream_t st, int *status) {
   for (int i = 0; i < g.nprod; ++i) { p.pa[i] = g.pa[i]; p.pb[i] = g.pb[i]; }
   p.batch = 1; p.splits = 1;
   p.C = g.C; p.c_double = g.c_double;
+  if (g.planes) fail(kErrUnsupported, "tcgen05 CTA-pair GEMM: no plane output");
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;
@@ -1286,7 +1345,7 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
   const int stage64 = g.A.np * BM * 64 * 2 + g.B.np * 256 * 64 * 2;
   const bool small_n = g.N <= 128;
   if (amn && bmn) {
-    if (g.batch == 1 && g.splits <= 0 && pair_mn_ok(g)) launch_pair<64, true>(g, st, status);
+    if (g.batch == 1 && g.splits <= 0 && !g.planes && pair_mn_ok(g)) launch_pair<64, true>(g, st, status);
     else launch_t<128, 64, true, true>(g, st, status);
   } else if (amn) {
     fail(kErrUnsupported, "tcgen05 GEMM: MN-major A needs MN-major B");
@@ -1307,7 +1366,7 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
     const bool few_tiles = tiles128 < Runtime::get().num_sms;
     if (g.A.np + g.B.np >= 5 && !smalln_bk64() && !few_tiles) launch_t<128, 32, false, false>(g, st, status);
     else launch_t<128, 64, false, false>(g, st, status);
-  } else if (g.batch == 1 && g.splits <= 0 && !g.upper && pair_ok(g)) {
+  } else if (g.batch == 1 && g.splits <= 0 && !g.upper && !g.planes && pair_ok(g)) {
     if (pair_bk() == 32) launch_pair<32, false>(g, st, status);
     else launch_pair<64, false>(g, st, status);
   } else if (3 * stage64 <= (int)rt.smem_optin - 2048 && !bk32_forced()) {

@@ -86,7 +86,9 @@ int sketch_planes() {
 // only one panel's planes exist at a time and none are kept; the projection streams A again.
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
-                  long long ldom, uint64_t seed, T *y, long long ldy) {
+                  long long ldom, uint64_t seed, T *y, long long ldy, PlaneHandoff *hand) {
+  if (hand && !handoff_shape_ok(Nl)) hand = nullptr;
+  if (hand) hand->prepare(y, ldy, m, Nl, c.st);
   const bool a_dev = is_device_pointer(a);
   const bool ooc = !a_dev && c.a_panel_rows > 0;
   const long long P = ooc ? c.a_panel_rows : panel_rows(m, n, sizeof(T));
@@ -125,6 +127,7 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
   g.status = c.status;
   g.chunk_k = 512;  // 5e-7 relative tensor-core chain error per chunk, below the 2^-17 split level
   g.tag = "sketch";
+  if (hand) { g.p_ld = hand->pb.P.ld; g.p_ps = hand->pb.P.plane_stride; }
   if (a_dev) {
     // A on the device: split every row, then one launch over all m rows (no per-panel wave tail)
     for (long long r0 = 0; r0 < m; r0 += P) {
@@ -135,7 +138,8 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
     }
     g.M = m;
     g.A = all;
-    g.C = y;
+    g.C = hand ? nullptr : y;
+    if (hand) g.planes = hand->pb.buf.p;
     umma_gemm(g, c.st);
   } else {
     // A in host memory: panel p + 1 is copied while panel p is split and multiplied
@@ -149,7 +153,8 @@ void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T 
       pp.rows = rows;
       g.M = (int)rows;
       g.A = pp;
-      g.C = y + r0 * ldy;
+      g.C = hand ? nullptr : y + r0 * ldy;
+      if (hand) g.planes = hand->pb.buf.p + (size_t)r0 * hand->pb.P.ld;
       umma_gemm(g, c.st);
     });
   }
@@ -189,7 +194,8 @@ void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, 
 
 template <class T>
 void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
-                       const T *Wp, T *out, long long ldo) {
+                       const T *Wp, T *out, long long ldo, PlaneHandoff *hand) {
+  if (hand && l % 64 != 0) fail(kErrUnsupported, "plane hand-off of the block applies needs l %% 64 == 0");
   if (l % 64 == 0) {
     PlaneBuf wt;
     make_planes<T>(wt, Wp, l, (long long)N * l, l, 3, true, c.st);  // [Wp_0' .. Wp_N-1'] (l x Nl)
@@ -200,7 +206,16 @@ void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N,
     g.batch = N; g.a_k_step = l; g.b_k_step = l; g.c_step = l;
     g.C = out; g.c_double = is_double<T>(); g.c_rs = ldo; g.c_cs = 1;
     g.status = c.status;
-  g.tag = "block_apply";
+    g.tag = "block_apply";
+    if (hand) {
+      const bool in_place = hand->of && yp.ptr == hand->pb.buf.p;
+      if (!in_place) hand->prepare(out, ldo, m, (long long)N * l, c.st);
+      g.C = nullptr;
+      g.planes = hand->pb.buf.p; g.p_ld = hand->pb.P.ld; g.p_ps = hand->pb.P.plane_stride;
+      g.planes_in_place = in_place;
+      hand->of = out;
+      hand->ld_of = ldo;
+    }
     umma_gemm(g, c.st);
     return;
   }
@@ -343,13 +358,27 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, long long 
   umma_gemm(gg, c.st);
 }
 
+void PlaneHandoff::prepare(const void *p, long long ld, long long rows, long long cols, cudaStream_t st) {
+  const long long pld = plane_ld(cols), rp = plane_rows(rows), ps = rp * pld;
+  pb.buf.ensure((size_t)3 * ps);
+  for (int q = 0; q < 3; ++q) {  // padding rows and columns: zero (TMA boxes of the last tiles read them)
+    __nv_bfloat16 *pl = pb.buf.p + (size_t)q * ps;
+    if (rp > rows) CK(cudaMemsetAsync(pl + (size_t)rows * pld, 0, (size_t)(rp - rows) * pld * 2, st));
+    if (pld > cols) CK(cudaMemset2DAsync(pl + cols, pld * 2, 0, (pld - cols) * 2, rows, st));
+  }
+  pb.P.ptr = pb.buf.p; pb.P.np = 3; pb.P.rows = rows; pb.P.cols = cols; pb.P.ld = pld; pb.P.plane_stride = ps;
+  pb.P.mn_major = false;
+  of = p;
+  ld_of = ld;
+}
+
 #define ISVD_INST(T)                                                                                        \
   template void mixed_sketch<T>(const StageCtx &, int, int, int, char, const T *, long long, const T *,      \
-                                long long, uint64_t, T *, long long);                                      \
+                                long long, uint64_t, T *, long long, PlaneHandoff *);                      \
   template void mixed_block_gram<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,    \
                                     double *);                                                             \
   template void mixed_block_apply<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \
-                                     const T *, T *, long long);                                           \
+                                     const T *, T *, long long, PlaneHandoff *);                           \
   template void mixed_gram_full<T>(const StageCtx &, const Planes &, int, int, const T *, long long,          \
                                    double *, int, bool);                                                        \
   template void mixed_apply_coeff<T>(const StageCtx &, const Planes &, int, int, int, const T *, long long,   \

@@ -17,6 +17,20 @@ struct PlaneBuf {
   Planes P;
 };
 
+// The three bf16 planes (rows x cols, ld = cols, padding rows zero) that stand for the matrix at
+// `of` (row stride ld_of) between two stages: its values there are not written.  `of` null: empty.
+struct PlaneHandoff {
+  PlaneBuf pb;
+  const void *of = nullptr;
+  long long ld_of = 0;
+  bool holds(const void *p, long long ld) const { return of && of == p && ld_of == ld; }
+  // the planes of a rows x cols matrix at p (row stride ld), to be written: allocated, padding zeroed
+  void prepare(const void *p, long long ld, long long rows, long long cols, cudaStream_t st);
+};
+// Whether a stage of this shape can hand its output over as planes: cols a multiple of 64 (no
+// padding columns), so that plane_ld(cols) == cols.
+inline bool handoff_shape_ok(long long cols) { return cols > 0 && cols % 64 == 0; }
+
 // Planes of the rows x cols matrix src (element (r, c) at src[r * s_rs + c]), optionally transposed.
 template <class T>
 void make_planes(PlaneBuf &pb, const T *src, long long s_rs, long long rows, long long cols, int np, bool transpose,
@@ -47,9 +61,11 @@ struct MixedCache {
 // bf16 planes of A the MIXED sketch keeps per element (2; 3 with ISVD_GPU_SKETCH_PLANES=3).
 int sketch_planes();
 
+// Y = A Omega (m x Nl, row stride ldy).  hand (Nl a multiple of 64): Y's three bf16 planes are
+// written into it instead of Y's values.
 template <class T>
 void mixed_sketch(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
-                  long long ldom, uint64_t seed, T *y, long long ldy);
+                  long long ldom, uint64_t seed, T *y, long long ldy, PlaneHandoff *hand = nullptr);
 
 // The next four take bf16 planes `yp` of an m x Nl row-major matrix (split without transpose,
 // make_planes(.., false)) and the matrix itself (`y`, used when the block width rules out the
@@ -60,10 +76,12 @@ template <class T>
 void mixed_block_gram(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
                       double *W);
 
-// Q_i = Y_i Wp_i (Wp: N x l x l in T) -> out (m x Nl, ld ldo).
+// Q_i = Y_i Wp_i (Wp: N x l x l in T) -> out (m x Nl, ld ldo).  hand (l a multiple of 64): the
+// output's three bf16 planes go into it instead of its values -- over yp in place when yp are the
+// hand-off's own planes.
 template <class T>
 void mixed_block_apply(const StageCtx &c, const Planes &yp, int m, int l, int N, const T *y, long long ldy,
-                       const T *Wp, T *out, long long ldo);
+                       const T *Wp, T *out, long long ldo, PlaneHandoff *hand = nullptr);
 
 // G = Qs' Qs (Nl x Nl, FP64 out; symmetric, computed on the upper triangle and mirrored).
 // all_pairs: every plane product (p, q < np), so that G is the Gram of the planes' sum itself (to

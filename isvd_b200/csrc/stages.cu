@@ -45,7 +45,7 @@ template <class T>
 void sketch_dev(const StageCtx &c, int m, int n, int Nl, char ordera, const T *a, long long lda, const T *omega,
                 long long ldom, uint64_t seed, T *y, long long ldy) {
   if (c.precision == kMixed) {
-    mixed_sketch<T>(c, m, n, Nl, ordera, a, lda, omega, ldom, seed, y, ldy);
+    mixed_sketch<T>(c, m, n, Nl, ordera, a, lda, omega, ldom, seed, y, ldy, c.handoff);
     read_status(c, "Gaussian projection sketching");
     return;
   }
@@ -75,13 +75,17 @@ namespace {
 // One Gramian pass on the N column blocks of y (in place):  Q_i = Y_i F(W_i),  W_i = Y_i' Y_i,
 //   polar = false:  F = V S^-1           (reference :80-98: gesvd('O') vectors over sqrt(values))
 //   polar = true:   F = V S^-1 V'        (re-orthogonalization that keeps Q's columns in place)
+// emit (MIXED, l % 64 == 0, with c.handoff): Q goes to the hand-off as bf16 planes, y is not
+// written.  Y's planes come from the hand-off when it holds them (the sketch's), else from y.
 template <class T>
-void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, bool polar) {
+void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, bool polar, bool emit) {
   const int Nl = N * l;
   const size_t ll = (size_t)l * l;
   DBuf<double> W(N * ll), V(N * ll), w((size_t)N * l);
   PlaneBuf yp;  // MIXED: bf16 planes of Y, shared by the Gram and the apply
-  if (c.precision == kMixed) make_planes<T>(yp, y, ldy, m, Nl, 3, false, c.st);
+  const bool from_hand = c.precision == kMixed && c.handoff && c.handoff->holds(y, ldy);
+  if (from_hand) yp.P = c.handoff->pb.P;
+  else if (c.precision == kMixed) make_planes<T>(yp, y, ldy, m, Nl, 3, false, c.st);
   // W_i = Y_i' Y_i   (reference :82-84)
   if (c.precision == kMixed) {
     mixed_block_gram<T>(c, yp.P, m, l, N, y, ldy, W.p);
@@ -131,9 +135,12 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
   // Q_i = Y_i F_i  (:95-98).  MIXED with planes: the product reads only the planes, so it writes
   // y in place; otherwise it goes to a temporary that is copied back.
   if (c.precision == kMixed && l % 64 == 0) {
-    mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, y, ldy);
+    const bool out_planes = emit && c.handoff;
+    mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, y, ldy, out_planes ? c.handoff : nullptr);
+    if (!out_planes && c.handoff && c.handoff->holds(y, ldy)) c.handoff->of = nullptr;  // y's values changed
     return;
   }
+  if (from_hand) fail(kErrUnsupported, "plane hand-off into the Gramian orthogonalization needs l %% 64 == 0");
   DBuf<T> tmp((size_t)m * Nl);
   if (c.precision == kMixed) {
     mixed_block_apply<T>(c, yp.P, m, l, N, y, ldy, Wp.p, tmp.p, Nl);
@@ -157,8 +164,9 @@ void gramian_pass(const StageCtx &c, int m, int l, int N, T *y, long long ldy, b
 // place of the Cholesky factor) restores orthonormality to FP32 level without moving the span.
 template <class T>
 void orth_gramian_dev(const StageCtx &c, int m, int l, int N, T *y, long long ldy) {
-  gramian_pass<T>(c, m, l, N, y, ldy, false);
-  if (c.precision == kMixed && !c.deferred_orth) gramian_pass<T>(c, m, l, N, y, ldy, true);
+  const bool two = c.precision == kMixed && !c.deferred_orth;
+  gramian_pass<T>(c, m, l, N, y, ldy, false, !two);
+  if (two) gramian_pass<T>(c, m, l, N, y, ldy, true, true);
   read_status(c, "Gramian orthogonalization");
 }
 
@@ -214,7 +222,8 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   const long long lw = 3LL * l;  // row stride of the iterate [M | B | Bgc]
   DBuf<double> G((size_t)Nl * Nl);
   PlaneBuf qp;  // MIXED: bf16 planes of Qs, shared by G and the final Qbar = Qs M
-  if (c.precision == kMixed) make_planes<T>(qp, qs, ldq, m, Nl, 3, false, c.st);
+  if (c.precision == kMixed && c.handoff && c.handoff->holds(qs, ldq)) qp.P = c.handoff->pb.P;  // the apply's
+  else if (c.precision == kMixed) make_planes<T>(qp, qs, ldq, m, Nl, 3, false, c.st);
   if (c.precision == kMixed) {
     mixed_gram_full<T>(c, qp.P, m, Nl, qs, ldq, G.p);
   } else {

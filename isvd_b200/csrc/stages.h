@@ -8,7 +8,8 @@
 
 namespace isvdb {
 
-struct MixedCache;  // bf16 planes of A kept between the sketch and the postprocess (mixed.h)
+struct MixedCache;    // bf16 planes of A kept between the sketch and the postprocess (mixed.h)
+struct PlaneHandoff;  // bf16 planes of one stage's output handed to the next stage (mixed.h)
 
 struct StageCtx {
   cudaStream_t st;
@@ -36,6 +37,9 @@ struct StageCtx {
   // out-of-core A: a host A is streamed through the device in row panels of this many rows by the
   // sketch and the projection (0: A is on the device, or copied there whole)
   long long a_panel_rows = 0;
+  // MIXED driver, GP / GR / (KN or WY): the sketch and the Gramian apply write the bf16 planes of
+  // their output here instead of its values, and the next stage reads them instead of splitting
+  PlaneHandoff *handoff = nullptr;
 };
 
 struct IterResult {

@@ -205,7 +205,8 @@ IterResult integrate_wy_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   DBuf<double> G((size_t)Nl * Nl);
   PlaneBuf qp;  // MIXED: bf16 planes of Qs, shared by G and the final Qbar = Qs M
   if (mixed) {
-    make_planes<T>(qp, qs, ldq, m, Nl, 3, false, st);
+    if (c.handoff && c.handoff->holds(qs, ldq)) qp.P = c.handoff->pb.P;  // the Gramian apply's planes
+    else make_planes<T>(qp, qs, ldq, m, Nl, 3, false, st);
     mixed_gram_full<T>(c, qp.P, m, Nl, qs, ldq, G.p);
   } else {
     Gemm<T, double> g;
