@@ -409,7 +409,26 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
       for (int j = 0; j < C::HALF; ++j) stg[lane * SROW + j] = acc[j];
       __syncwarp();
-      for (int r = 0; r < 32; ++r) {
+      // plane output (no value output): two consecutive columns per lane, one 4-byte store per plane
+      const bool pairs = p.pl && !p.C && p.splits == 1 && !p.upper && (p.N & 1) == 0 && (C::HALF % 64) == 0;
+      for (int r = 0; pairs && r < 32; ++r) {
+        const int gr = m0 + q * 32 + r;
+        if (gr >= p.M) break;
+#pragma unroll
+        for (int t = 0; t < C::HALF / 64; ++t) {
+          const int gn = n0 + h * C::HALF + t * 64 + 2 * lane;
+          if (gn >= p.N) continue;
+          __nv_bfloat16 o0[3], o1[3];
+          out_pieces(p.alpha * (double)stg[r * SROW + t * 64 + 2 * lane], p.c_double, o0);
+          out_pieces(p.alpha * (double)stg[r * SROW + t * 64 + 2 * lane + 1], p.c_double, o1);
+          const long long po = (long long)b * p.c_step + (long long)gr * p.pl_ld + gn;
+#pragma unroll
+          for (int qq = 0; qq < 3; ++qq)
+            *(uint32_t *)(p.pl + qq * p.pl_ps + po) =
+                (uint32_t)__bfloat16_as_ushort(o0[qq]) | ((uint32_t)__bfloat16_as_ushort(o1[qq]) << 16);
+        }
+      }
+      for (int r = 0; !pairs && r < 32; ++r) {
         const int gr = m0 + q * 32 + r;
         if (gr >= p.M) break;
 #pragma unroll
