@@ -852,6 +852,8 @@ __global__ void umma_reduce_kernel(const KParams p) {
       const int c = c0 + j;
       if (c >= p.N || (p.upper && c < (int)r)) continue;
       const double sum = ((acc[0][j] + acc[1][j]) + (acc[2][j] + acc[3][j])) + ((acc[4][j] + acc[5][j]) + (acc[6][j] + acc[7][j]));
+      if (p.pl) store_pieces(p, (long long)b * p.c_step + (long long)r * p.pl_ld + c, p.alpha * sum);
+      if (!p.C) continue;
       const long long off = (long long)b * p.c_step + (long long)r * p.c_rs + (long long)c * p.c_cs;
       if (p.c_double) ((double *)p.C)[off] = p.alpha * sum;
       else ((float *)p.C)[off] = (float)(p.alpha * sum);
@@ -1124,7 +1126,6 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
         break;
       }
   }
-  if (g.planes) splits = 1;  // the planes are written by the epilogue: no split-K partials
   splits = std::max(1, std::min(splits, p.total_kb));
   p.kbps = (p.total_kb + splits - 1) / splits;
   p.splits = (p.total_kb + p.kbps - 1) / p.kbps;

@@ -46,7 +46,7 @@ struct UmmaGemm {
   int *status = nullptr;     // device status word: set, the call returns without a host synchronisation
   // Optional output as three bf16 planes: element (i, j) of batch b, in the output type (FP32, or
   // FP64 with c_double), split as split_planes splits it, at planes + q p_ps + i p_ld + b c_step + j.
-  // Needs c_cs == 1; C may then be null (no value output); no split-K.  planes_in_place: the planes
+  // Needs c_cs == 1; C may then be null (no value output).  planes_in_place: the planes
   // overwrite the A operand's own planes (block applies: every CTA runs its batches in order, so a
   // batch's output columns are written after the last read of them); the call fails otherwise.
   __nv_bfloat16 *planes = nullptr;

@@ -216,6 +216,35 @@ def test_mixed_driver_vs_fp64(lib, oracle, x):
     assert oracle.max_principal_angle(v1[:, :k], v0[:, :k]) < 1e-4
 
 
+@pytest.mark.parametrize("integ", ["KN", "WY"])
+@pytest.mark.parametrize("where", ["host", "device"])
+def test_mixed_plane_handoff_bitwise(lib, monkeypatch, where, integ):
+    """The MIXED driver hands Y (sketch -> Gramian orthogonalization) and Qs (-> integration) over
+    as the bf16 planes the next stage would split them into: with the hand-off and without it
+    (ISVD_GPU_PLANE_HANDOFF=0) the results are bitwise the same, with A on the device (one sketch
+    launch) and in host memory (one launch per streamed panel)."""
+    torch = pytest.importorskip("torch")
+    m, n, k, p, Nn = 2000, 1200, 40, 24, 4  # l = 64, N l = 256
+    l = k + p
+    a = np.ascontiguousarray(lowrank(m, n, 300, 10 ** (-3 / 300), 1e-6, 31).astype(np.float32))
+    aa = torch.from_numpy(a).cuda() if where == "device" else a
+    if where == "host":
+        monkeypatch.setenv("ISVD_GPU_PANEL_ROWS", "512")
+    prm = lib.create_param(m, n, k, p, Nn)
+    argv = [None, None, [256, 1e-4] if integ == "KN" else [256, 1e-3], None]
+    out = []
+    for off in ("1", "0"):
+        monkeypatch.setenv("ISVD_GPU_PLANE_HANDOFF", off)
+        s = np.zeros(l, np.float32); u = np.zeros((m, l), np.float32); v = np.zeros((n, l), np.float32)
+        retv, _, st = lib.isvd("s", prm, ("GP", "GR", integ, "GR"), aa, n, s, u, l, v, l, seed=7, argv=argv,
+                               retc=(0, 0, 2, 0), precision=1)
+        assert st == 0, lib.last_error()
+        out.append((s, u, v, int(retv[2][0])))
+    (s1, u1, v1, i1), (s0, u0, v0, i0) = out
+    assert i1 == i0
+    assert np.array_equal(s1, s0) and np.array_equal(u1, u0) and np.array_equal(v1, v0)
+
+
 @pytest.mark.parametrize("where", ["host", "device"])
 def test_mixed_driver_wide_blocks(lib, oracle, where):
     """l = 64 (device A: one sketch launch; host A: one per streamed 512-row panel): the Gramian
