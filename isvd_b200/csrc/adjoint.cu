@@ -612,9 +612,11 @@ int svd_adjoint_dev(const StageCtx &c, int m, int n, int k, char ordera, const T
   if (!du) CK(cudaMemsetAsync(lam.p, 0, mk * sizeof(T), st));
   if (!dv) CK(cudaMemsetAsync(gam.p, 0, nk * sizeof(T), st));
   // MIXED, n <= m: the systems in the n-dimensional coordinates of B'B (ISVD_GPU_ADJOINT_CG_A=1 keeps
-  // the operator in A, for comparison)
+  // the operator in A, for comparison).  Forming A'A costs m n^2, about as much as 2 n / k CG
+  // iterations with the operator in A (2 m n k each): the form pays when n <= 128 k (64 iterations).
   const char *in_a = getenv("ISVD_GPU_ADJOINT_CG_A");
-  const bool gram = A.mixed && n <= m && n % 8 == 0 && cg_iters > 0 && (du || dv) && !(in_a && atoi(in_a) != 0);
+  const bool gram = A.mixed && n <= m && n % 8 == 0 && (long long)n <= 128LL * k && cg_iters > 0 && (du || dv) &&
+                    !(in_a && atoi(in_a) != 0);
   const int iters = gram ? complement_gram_cg<T>(c, A, k, u, ldu, v, ldv, s, du ? ru.p : nullptr, lam.p,
                                                  dv ? rv.p : nullptr, gam.p, cg_iters, tol)
                          : complement_cg<T>(c, A, k, u, ldu, v, ldv, s, du ? ru.p : nullptr, lam.p,
