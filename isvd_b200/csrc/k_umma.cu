@@ -410,7 +410,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int j = 0; j < C::HALF; ++j) stg[lane * SROW + j] = acc[j];
       __syncwarp();
       // plane output (no value output): two consecutive columns per lane, one 4-byte store per plane
-      const bool pairs = p.pl && !p.C && p.splits == 1 && !p.upper && (p.N & 1) == 0 && (C::HALF % 64) == 0;
+      const bool pairs = p.pl && !p.C && p.splits == 1 && !p.upper && (p.N & 1) == 0 && (C::HALF % 64) == 0 &&
+                         ((p.c_step | p.pl_ld) & 1) == 0 && ((uintptr_t)p.pl & 3) == 0;
       for (int r = 0; pairs && r < 32; ++r) {
         const int gr = m0 + q * 32 + r;
         if (gr >= p.M) break;
