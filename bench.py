@@ -63,7 +63,9 @@ SKETCH_LAUNCH_TRAFFIC = 86.989471744e9 + 3.400887296e9
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks / throttle reasons sampled every 50 ms during the timed region: entering
+    waits (up to 5 s) for nvidia-smi's first line and drops it, so that the samples kept start with
+    the region."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -77,10 +79,13 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.first = threading.Event()
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            self.first.wait(5.0)
+            self.lines.clear()
         except OSError:
             self.proc = None
         return self
@@ -88,6 +93,8 @@ class ClockSampler:
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
+            self.first.set()
+        self.first.set()
 
     def __exit__(self, *a):
         if self.proc:
