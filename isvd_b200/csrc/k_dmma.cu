@@ -14,6 +14,7 @@
 #include <cstdlib>
 
 #include "kernels.h"
+#include "planes.cuh"
 #include "runtime.h"
 
 namespace isvdb {
@@ -152,10 +153,46 @@ __global__ void __launch_bounds__(WM * WN * 32)
           double v = g.alpha * acc[i][j][h];
           if (g.beta != 0.0) v += g.beta * *c;
           *c = v;
+          acc[i][j][h] = v;  // the stored value, for the plane output below
         } else {
           C[(long long)gm * g.N + gn] = acc[i][j][h];
         }
       }
+  }
+  using L = DmmaLayout<BM, BN, A_KC, B_NC>;
+  if constexpr (BN * (BM + 1) <= kStages * L::stage) {
+    if (direct && g.pl_t && b == g.pl_batch) {
+      // bf16 planes of this tile's transpose: the values go through the (now idle) cp.async ring
+      // as a BN x BM tile, then each thread splits 8 consecutive rows of one output column and
+      // stores 16 bytes per plane (plane row gn, columns gm .. gm + 7)
+      constexpr int TLD = BM + 1;
+      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+            smem[(wn0 + 8 * j + 2 * fc + h) * TLD + (wm0 + 8 * i + fr)] = acc[i][j][h];
+      __syncthreads();
+      constexpr int NT = WM * WN * 32;
+      for (int t = tid; t < BN * (BM / 8); t += NT) {
+        const int cl = t / (BM / 8), seg = t - cl * (BM / 8);
+        const int gn = n0 + cl;
+        if (gn >= g.N) continue;
+        __nv_bfloat16 o[3][8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          __nv_bfloat16 pc[3];
+          split3<double>(smem[cl * TLD + 8 * seg + e], pc, 3);
+#pragma unroll
+          for (int q = 0; q < 3; ++q) o[q][e] = pc[q];
+        }
+        const long long po = (long long)gn * g.pl_ld + m0 + 8 * seg;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) *(uint4 *)(g.pl_t + q * g.pl_ps + po) = pack8(o[q]);
+      }
+    }
   }
 }
 
@@ -292,7 +329,12 @@ void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t
   const long long tiles128 = (long long)((g.M + 127) / 128) * ((g.N + 127) / 128) * g.batch;
   const int sms = Runtime::get().num_sms;
   const bool long_k = g.splits <= 0 && (long long)g.K >= 2048 && tiles128 * (g.K / 1024) >= 2LL * sms;
-  if (g.M <= 64 || g.N <= 64 || (tiles128 < 2LL * sms && !long_k))
+  if (g.pl_t && (g.splits != 1 || g.M % 64 || g.pl_ld % 8 || ((uintptr_t)g.pl_t & 15) || g.pl_ps % 8 ||
+                 g.pl_batch < 0 || g.pl_batch >= g.batch))
+    fail(kErrArgument, "dmma_gemm: plane output needs splits = 1, M %% 64 == 0 and 16-byte aligned plane rows");
+  // plane output: 64 x 64 tiles (their epilogue stages a tile's transpose through the cp.async
+  // ring; without split-K the tile shape does not change the results)
+  if (g.pl_t || g.M <= 64 || g.N <= 64 || (tiles128 < 2LL * sms && !long_k))
     dmma_launch<64, 64, 2, 2>(g, a_kc, b_nc, st);
   else
     dmma_launch<128, 128, 2, 4>(g, a_kc, b_nc, st);

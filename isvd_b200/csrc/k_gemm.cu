@@ -275,6 +275,7 @@ void gemm(const Gemm<T, Tout> &g, cudaStream_t st) {
       return;
     }
   }
+  if (g.pl_t) fail(kErrArgument, "gemm: plane output only on the FP64 tensor-core path");
   // 128 x 128 tiles when they fill the GPU, or when a long inner dimension lets split-K fill it
   // (8 x 8 register blocks: half the shared-memory reads per FMA of 64 x 64 tiles); otherwise
   // 64 x 64 tiles (4x more CTAs)

@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 
+#include "planes.cuh"
 #include "runtime.h"
 #include "umma.h"
 
@@ -54,6 +55,8 @@ struct KParams {
   int vec_out;    // direct epilogue stores as 16-byte vectors (C rows contiguous and aligned)
   __nv_bfloat16 *pl;  // optional bf16 planes of the output (UmmaGemm::planes)
   long long pl_ld, pl_ps;
+  int n_group;  // N tiles per column group of the tile order (0: row-major tile order)
+  int l2_hint;  // B loads evict-last, A loads evict-first
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -133,6 +136,26 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
           "r"(su32(dst)),
       "l"((uint64_t)map), "r"(su32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
+}
+// The same load with an L2 cache policy (createpolicy): evict-first for streamed operands,
+// evict-last for the operand that the other resident CTAs read again.
+__device__ __forceinline__ void tma_load_3d_pol(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z,
+                                                uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%3, "
+      "%4, %5}], [%2], %6;" ::"r"(su32(dst)),
+      "l"((uint64_t)map), "r"(su32(bar)), "r"(x), "r"(y), "r"(z), "l"(pol)
+      : "memory");
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
 }
 
 // Shared-memory matrix descriptor (sm100 layout: start>>4 [0,14), LBO>>4 [16,30), SBO>>4 [32,46),
@@ -218,7 +241,16 @@ __global__ void __launch_bounds__(kThreads, 1)
   volatile int *abort_flag = (volatile int *)(tslot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nt = blockIdx.x, mt = blockIdx.y;
+  int nt = blockIdx.x, mt = blockIdx.y;
+  if (p.n_group > 0 && p.n_group < (int)gridDim.x) {
+    // column-grouped tile order: the linear block index walks group g's n_group N tiles (fastest)
+    // for every M tile, then group g + 1; the last group may be narrower
+    const unsigned L = blockIdx.y * gridDim.x + blockIdx.x, span = (unsigned)p.n_group * gridDim.y;
+    const unsigned g = L / span, r = L - g * span;
+    const unsigned w = min((unsigned)p.n_group, gridDim.x - g * (unsigned)p.n_group);
+    mt = (int)(r / w);
+    nt = (int)(g * (unsigned)p.n_group + r % w);
+  }
   // segments: the batches this CTA accumulates one after the other (bloop), else its one batch
   // (batch loops and vector stores serve the skinny N <= 128 shapes; the 256-wide sketch tiles keep
   // their registers for the 128-column accumulators)
@@ -256,6 +288,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // ---------------------------------------------------------------- TMA producer
     int issued = 0, s = 0;
     uint32_t ph = 1;  // parity of the empty phase to wait for (first pass: none)
+    const bool hint = p.l2_hint != 0;
+    const uint64_t pol_a = hint ? l2_policy_evict_first() : 0, pol_b = hint ? l2_policy_evict_last() : 0;
     for (int seg = 0; seg < nseg && !*abort_flag; ++seg) {
     const int b = bloop ? seg : bz;
     const int a_row = (int)(b * p.a_mn_step) + m0;
@@ -271,7 +305,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       const int ka = k0 + (int)(b * p.a_k_step), kbb = k0 + (int)(b * p.b_k_step);
       for (int q = 0; q < p.na; ++q) {
         if (!AMN) {
-          tma_load_3d(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q);
+          if (hint) tma_load_3d_pol(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q, pol_a);
+          else tma_load_3d(st + q * C::A_TILE, &mapA, &full[s], ka, a_row, q);
         } else {
 #pragma unroll
           for (int j = 0; j < BM / 64; ++j)
@@ -281,7 +316,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint8_t *bt = st + p.na * C::A_TILE;
       for (int q = 0; q < p.nb; ++q) {
         if (!BMN) {
-          tma_load_3d(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q);
+          if (hint) tma_load_3d_pol(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q, pol_b);
+          else tma_load_3d(bt + q * C::B_TILE, &mapB, &full[s], kbb, b_row, q);
         } else {
 #pragma unroll
           for (int j = 0; j < BN / 64; ++j)
@@ -874,27 +910,6 @@ __global__ void mirror_upper_kernel(T *C, long long n, long long ld) {
 }
 
 // ------------------------------------------------------------------------------ splits
-// Piece q of x: x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1) (round to nearest).
-template <class T>
-__device__ __forceinline__ void split3(T x, __nv_bfloat16 *o, int np) {
-  double r = (double)x;
-#pragma unroll
-  for (int q = 0; q < 3; ++q) {
-    if (q >= np) break;
-    const __nv_bfloat16 h = __double2bfloat16(r);
-    o[q] = h;
-    r -= (double)__bfloat162float(h);
-  }
-}
-
-__device__ __forceinline__ uint4 pack8(const __nv_bfloat16 *v) {
-  uint4 u;
-  u.x = (uint32_t)__bfloat16_as_ushort(v[0]) | ((uint32_t)__bfloat16_as_ushort(v[1]) << 16);
-  u.y = (uint32_t)__bfloat16_as_ushort(v[2]) | ((uint32_t)__bfloat16_as_ushort(v[3]) << 16);
-  u.z = (uint32_t)__bfloat16_as_ushort(v[4]) | ((uint32_t)__bfloat16_as_ushort(v[5]) << 16);
-  u.w = (uint32_t)__bfloat16_as_ushort(v[6]) | ((uint32_t)__bfloat16_as_ushort(v[7]) << 16);
-  return u;
-}
 
 // Pieces of an FP32 value in FP32 arithmetic: x - bf16(x) is exact in FP32 (the rounding error of
 // an 8-bit rounding of a 24-bit significand), and so is the next remainder.
@@ -1094,6 +1109,8 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.C = g.C; p.c_double = g.c_double;
   p.pl = g.planes; p.pl_ld = g.p_ld; p.pl_ps = g.p_ps;
   if (g.planes && (g.c_cs != 1 || g.upper)) fail(kErrArgument, "tcgen05 GEMM: plane output needs unit column stride");
+  p.n_group = std::max(0, g.n_group);
+  p.l2_hint = g.l2_hint ? 1 : 0;
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;

@@ -1,6 +1,7 @@
 // Launchers of the device kernels of libisvd_gpu_b200 (all enqueue on the library stream).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -28,6 +29,12 @@ struct Gemm {
   // C symmetric (M == N, A = B'): tiles entirely below the diagonal are not computed; the caller
   // completes C with mirror_upper
   bool upper = false;
+  // FP64 tensor-core path without split-K only (dmma_gemm, splits == 1, M % 64 == 0): batch
+  // pl_batch's output C(i, j) is also written as three bf16 planes of its transpose, piece q at
+  // pl_t[q pl_ps + j pl_ld + i] (as split_planes(.., transpose = true) splits it)
+  __nv_bfloat16 *pl_t = nullptr;
+  long long pl_ld = 0, pl_ps = 0;
+  int pl_batch = 0;
 };
 
 template <class T, class Tout>
@@ -40,7 +47,6 @@ bool dmma_enabled();
 void dmma_gemm(const Gemm<double, double> &g, bool a_kc, bool b_nc, cudaStream_t st);
 // C = alpha * (sum of the `splits` partial products) + beta * C (partials: batch x splits x M x N).
 void splitk_reduce(const Gemm<double, double> &g, int splits, const double *partial, cudaStream_t st);
-
 // One product of a grouped launch over many independent products of their own shapes:
 // C = alpha A B + beta C (A M x K, B K x N, element strides as in Gemm).  Its output tiles are the
 // work items tile0 .. tile0 + ceil(M / BM) * tn - 1 of the launch (tn tiles along N).

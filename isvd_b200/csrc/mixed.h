@@ -42,8 +42,10 @@ struct MixedGProduct {
   PlaneBuf g, b;
   int Nl = 0;
   void prepare(const StageCtx &c, int Nl_, const double *G);
-  // Bgc = alpha G Bc (Nl x l, row strides ldb and ldo)
-  void apply(const StageCtx &c, int l, const double *Bc, long long ldb, double alpha, double *Bgc, long long ldo);
+  // Bgc = alpha G Bc (Nl x l, row strides ldb and ldo).  split == false: Bc's planes (b) were
+  // written by the producer of Bc (the previous iteration's update), Bc itself is not read.
+  void apply(const StageCtx &c, int l, const double *Bc, long long ldb, double alpha, double *Bgc, long long ldo,
+             bool split = true);
 };
 
 // A's bf16 planes (m x n, K-major along n), made by the sketch and reused by the postprocess.

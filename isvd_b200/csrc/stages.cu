@@ -255,13 +255,21 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
   const double invN = 1.0 / N;
   MixedGProduct gprod;  // MIXED: G's bf16 planes, reused by every iteration
   if (c.precision == kMixed) gprod.prepare(c, Nl, G.p);
+  // MIXED, Nl % 64 == 0: the update writes the bf16 planes of B+ (the next Bc) from its epilogue,
+  // so that the G product reads them without a split launch (ISVD_GPU_KN_UPDATE_PLANES=0: split)
+  const bool update_planes = c.precision == kMixed && dmma_enabled() && Nl % 64 == 0 && [] {
+    const char *e = getenv("ISVD_GPU_KN_UPDATE_PLANES");
+    return !(e && atoi(e) == 0);
+  }();
+  bool split_bc = true;  // the first iteration's Bc = G[:, 0:l] is split by the G product
   // One iteration: W(next) from W(cur).  After two eager iterations (which size every buffer and
   // set every kernel attribute) the iteration is captured as one CUDA graph per parity of the
   // ping-pong buffers, so that an iteration costs one graph launch plus the host read of err.
   auto iteration = [&](double *Wcur, double *Wnext, double *errp) {
     double *Bc = Wcur + l, *Bgc = Wcur + 2 * l;
     if (c.precision == kMixed) {  // Bgc = G Bc / N   (:174-177)
-      gprod.apply(c, l, Bc, lw, invN, Bgc, lw);
+      gprod.apply(c, l, Bc, lw, invN, Bgc, lw, split_bc || !update_planes);
+      split_bc = false;
     } else {
       Gemm<double, double> g = gm<double>(Nl, l, Nl);
       g.alpha = invN;
@@ -293,6 +301,9 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
       g.B = Fs.p; g.b_rs = l; g.b_cs = 1; g.b_bs = 2 * (long long)ll;
       g.C = Wnext; g.c_rs = lw; g.c_cs = 1; g.c_bs = l;
       g.splits = 1;  // 2 N l / 64^2 tiles already fill the GPU: no split-K partials to add up
+      if (update_planes) {  // batch 1 is B+: its transpose's planes feed the next G product
+        g.pl_t = gprod.b.buf.p; g.pl_ld = gprod.b.P.ld; g.pl_ps = gprod.b.P.plane_stride; g.pl_batch = 1;
+      }
       gemm(g, c.st);
     }
   };

@@ -52,6 +52,12 @@ struct UmmaGemm {
   __nv_bfloat16 *planes = nullptr;
   long long p_ld = 0, p_ps = 0;
   bool planes_in_place = false;
+  // Tile order (long-K products whose B operand is larger than L2, e.g. the sketch's Omega'):
+  // n_group > 0 runs the output tiles in column groups of n_group N tiles, every M tile of a group
+  // before the next group, so that the CTAs resident at one time read one group's B rows;
+  // l2_hint loads B with the L2 evict-last policy and A with evict-first.
+  int n_group = 0;
+  bool l2_hint = false;
 };
 
 // Geometry of a plane buffer for a rows x cols matrix: ld = cols rounded up to 64, rows padded to

@@ -73,6 +73,30 @@ def test_mixed_sketch_cta_pair(lib, monkeypatch, bk):
     assert np.abs(y2 - ref).max() < 1e-5 * scale
 
 
+@pytest.mark.parametrize("order", [("3", "0"), ("3", "1"), ("16", "1"), ("0", "1")])
+def test_mixed_sketch_tile_order_bitwise(lib, monkeypatch, order):
+    """The sketch's column-grouped tile order (ISVD_GPU_SKETCH_NGROUP: 3 N tiles per group over 16,
+    so the last group is one tile wide; 16: one group) and its L2 cache policies
+    (ISVD_GPU_SKETCH_L2HINT) change which CTA runs a tile and when, not the tile's arithmetic:
+    bitwise the row-major order's Y."""
+    m, n, nl = 1100, 900, 4096
+    rng = np.random.default_rng(21)
+    a = rng.standard_normal((m, n)).astype(np.float32)
+    om = rng.standard_normal((n, nl)).astype(np.float32)
+    prm = lib.create_param(m, n, nl, 0, 1)
+    monkeypatch.setenv("ISVD_GPU_SKETCH_NGROUP", "0")
+    monkeypatch.setenv("ISVD_GPU_SKETCH_L2HINT", "0")
+    y0 = np.zeros((m, nl), np.float32)
+    lib.sketch_omega("s", prm, a, n, om, nl, y0, nl)
+    monkeypatch.setenv("ISVD_GPU_SKETCH_NGROUP", order[0])
+    monkeypatch.setenv("ISVD_GPU_SKETCH_L2HINT", order[1])
+    y1 = np.zeros((m, nl), np.float32)
+    lib.sketch_omega("s", prm, a, n, om, nl, y1, nl)
+    assert np.array_equal(y0, y1)
+    ref = a.astype(np.float64) @ om.astype(np.float64)
+    assert np.abs(y1 - ref).max() < 1e-5 * np.abs(ref).max()
+
+
 def test_mixed_kn_gram_cta_pair(lib, monkeypatch):
     """KN at N l = 4096 (the Gram matrix Qs'Qs has 136 upper 256 x 256 tiles): with the Gram on
     the MN-major CTA-pair kernel (the default), the same iteration count and Qbar as with the
@@ -100,6 +124,33 @@ def test_mixed_kn_gram_cta_pair(lib, monkeypatch):
     it1, q1 = run()
     assert it2 == it1
     assert (q2 - q1).abs().max().item() < 1e-5
+
+
+def test_kn_update_planes_bitwise(lib, monkeypatch):
+    """The next Bc's bf16 planes written by the [M | B] update's epilogue (the default when N l is a
+    multiple of 64) give bitwise the iteration count and Qbar of the separate transposed split
+    (ISVD_GPU_KN_UPDATE_PLANES=0)."""
+    torch = pytest.importorskip("torch")
+    m, l, Nn = 3000, 128, 16
+    g = torch.Generator(device="cuda").manual_seed(5)
+    base = torch.linalg.qr(torch.randn(m, l, device="cuda", dtype=torch.float64, generator=g))[0]
+    qs = torch.cat([torch.linalg.qr(base + 0.05 * torch.randn(m, l, device="cuda", dtype=torch.float64,
+                                                               generator=g))[0] for _ in range(Nn)], dim=1)
+    qs = qs.float().contiguous()
+    prm = lib.create_param(m, m, l, 0, Nn)
+
+    def run():
+        qt = torch.zeros((m, l), device="cuda", dtype=qs.dtype)
+        torch.cuda.synchronize()
+        r = lib.integrate("s", "KN", prm, qs, l * Nn, qt, l, argv=[256, 1e-4])
+        return int(r[0]), qt.cpu().numpy()
+
+    monkeypatch.setenv("ISVD_GPU_KN_UPDATE_PLANES", "1")
+    it1, q1 = run()
+    monkeypatch.setenv("ISVD_GPU_KN_UPDATE_PLANES", "0")
+    it0, q0 = run()
+    assert it1 == it0 and it1 > 3
+    assert np.array_equal(q1, q0)
 
 
 def test_mixed_sketch_internal_omega_matches_native(lib):
