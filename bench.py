@@ -57,9 +57,9 @@ def peaks():
 
 
 # DRAM bytes (read + write) of the sketch kernel's one launch over the 200000 x 20000 matrix
-# (N l = 4096), from a one-pass ncu capture of a full solve (dram__bytes_read.sum +
-# dram__bytes_write.sum, graphs off, `bench.py --single`)
-SKETCH_LAUNCH_TRAFFIC = 86.989471744e9 + 3.400887296e9
+# (N l = 4096, tiles in two column groups, Y written as bf16 planes), from a one-pass ncu capture
+# of a full solve (dram__bytes_read.sum + dram__bytes_write.sum, `bench.py --single`)
+SKETCH_LAUNCH_TRAFFIC = 69.929373696e9 + 4.996154112e9
 
 
 class ClockSampler:
