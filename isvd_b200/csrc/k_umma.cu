@@ -56,7 +56,7 @@ struct KParams {
   __nv_bfloat16 *pl;  // optional bf16 planes of the output (UmmaGemm::planes)
   long long pl_ld, pl_ps;
   int n_group;  // N tiles per column group of the tile order (0: row-major tile order)
-  int l2_hint;  // B loads evict-last, A loads evict-first
+  int l2_hint;  // bit 0: B loads evict-last, A loads evict-first; bit 1: A loads evict-last
 };
 
 __device__ __forceinline__ uint32_t su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -150,6 +150,11 @@ __device__ __forceinline__ void tma_load_3d_pol(void *dst, const CUtensorMap *ma
 __device__ __forceinline__ uint64_t l2_policy_evict_first() {
   uint64_t pol;
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_normal() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
   return pol;
 }
 __device__ __forceinline__ uint64_t l2_policy_evict_last() {
@@ -289,7 +294,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     int issued = 0, s = 0;
     uint32_t ph = 1;  // parity of the empty phase to wait for (first pass: none)
     const bool hint = p.l2_hint != 0;
-    const uint64_t pol_a = hint ? l2_policy_evict_first() : 0, pol_b = hint ? l2_policy_evict_last() : 0;
+    const uint64_t pol_a = (p.l2_hint & 2) ? l2_policy_evict_last() : (p.l2_hint & 1) ? l2_policy_evict_first() : 0;
+    const uint64_t pol_b = (p.l2_hint & 1) ? l2_policy_evict_last() : l2_policy_evict_normal();
     for (int seg = 0; seg < nseg && !*abort_flag; ++seg) {
     const int b = bloop ? seg : bz;
     const int a_row = (int)(b * p.a_mn_step) + m0;
@@ -1110,7 +1116,7 @@ void launch_t(const UmmaGemm &g, cudaStream_t st, int *status) {
   p.pl = g.planes; p.pl_ld = g.p_ld; p.pl_ps = g.p_ps;
   if (g.planes && (g.c_cs != 1 || g.upper)) fail(kErrArgument, "tcgen05 GEMM: plane output needs unit column stride");
   p.n_group = std::max(0, g.n_group);
-  p.l2_hint = g.l2_hint ? 1 : 0;
+  p.l2_hint = (g.l2_hint ? 1 : 0) | (g.a_keep ? 2 : 0);
   p.c_rs = g.c_rs; p.c_cs = g.c_cs;
   p.alpha = g.alpha;
   p.upper = g.upper ? 1 : 0;

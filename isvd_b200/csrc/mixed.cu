@@ -382,6 +382,18 @@ void MixedGProduct::apply(const StageCtx &c, int l, const double *Bc, long long 
   gg.alpha = alpha;
   gg.status = c.status;
   gg.tag = "kn_product";
+  // G's planes (3 Nl^2 bf16) are read again by every iteration: evict-last keeps them in L2 when
+  // they fit (ISVD_GPU_KN_L2KEEP=0: default policy)
+  static const long long l2 = [] {
+    int dev = 0, v = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&v, cudaDevAttrL2CacheSize, dev));
+    return (long long)v;
+  }();
+  gg.a_keep = 3LL * Nl * Nl * 2 <= l2 * 85 / 100 && [] {
+    const char *e = getenv("ISVD_GPU_KN_L2KEEP");
+    return !(e && atoi(e) == 0);
+  }();
   umma_gemm(gg, c.st);
 }
 

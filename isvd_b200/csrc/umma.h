@@ -58,6 +58,9 @@ struct UmmaGemm {
   // l2_hint loads B with the L2 evict-last policy and A with evict-first.
   int n_group = 0;
   bool l2_hint = false;
+  // A loads with the L2 evict-last policy (B unchanged): an A operand that later launches read
+  // again and that fits in L2 (the Kolmogorov-Nagumo G planes, read once per iteration)
+  bool a_keep = false;
 };
 
 // Geometry of a plane buffer for a rows x cols matrix: ld = cols rounded up to 64, rows padded to
