@@ -1364,9 +1364,11 @@ static bool wide_mn_off() {
   const char *e = getenv("ISVD_UMMA_WIDE_MN");
   return e && atoi(e) == 0;
 }
-static bool smalln_bk64() {
+// ISVD_UMMA_SMALLN_BK=64 / 32: the k-block depth of the N <= 128 products with five or more planes
+// (0: by the tile count, below)
+static int smalln_bk() {
   const char *e = getenv("ISVD_UMMA_SMALLN_BK");
-  return e && atoi(e) == 64;
+  return e ? atoi(e) : 0;
 }
 static bool bk32_forced() {
   const char *e = getenv("ISVD_UMMA_BK");
@@ -1408,7 +1410,8 @@ void umma_gemm(const UmmaGemm &g, cudaStream_t st) {
     // for 107 iterations)
     const long long tiles128 = (long long)((g.N + 127) / 128) * ((g.M + BM - 1) / BM) * g.batch;
     const bool few_tiles = tiles128 < Runtime::get().num_sms;
-    if (g.A.np + g.B.np >= 5 && !smalln_bk64() && !few_tiles) launch_t<128, 32, false, false>(g, st, status);
+    const int sbk = smalln_bk();
+    if (g.A.np + g.B.np >= 5 && (sbk == 32 || (sbk != 64 && !few_tiles))) launch_t<128, 32, false, false>(g, st, status);
     else launch_t<128, 64, false, false>(g, st, status);
   } else if (g.batch == 1 && g.splits <= 0 && !g.upper && !g.planes && pair_ok(g)) {
     if (pair_bk() == 32) launch_pair<32, false>(g, st, status);
