@@ -207,11 +207,17 @@ void coeff_unorthonormalize(const StageCtx &c, int Nl, int l, int N, const doubl
   (void)Nl;
 }
 
-// K depth per CTA of the split-K [Dc, Dgc] product of long Kolmogorov-Nagumo loops.
+// K depth per CTA of the split-K [Dc, Dgc] product of long Kolmogorov-Nagumo loops (0: the
+// generic split-K model).
 static int kn_dd_kchunk() {
   const char *e = getenv("ISVD_GPU_KN_DD_KCHUNK");
   const int v = e ? atoi(e) : 128;
-  return v >= 16 ? v : 128;
+  return v == 0 ? 0 : (v >= 16 ? v : 128);
+}
+// N l from which the loop uses kn_dd_kchunk (ISVD_GPU_KN_DD_FROM overrides 2048)
+static int kn_dd_from() {
+  const char *e = getenv("ISVD_GPU_KN_DD_FROM");
+  return e ? atoi(e) : 2048;
 }
 
 //
@@ -291,7 +297,7 @@ IterResult integrate_kn_dev(const StageCtx &c, int m, int l, int N, const T *qs,
       // long K (N l >= 2048): 128-deep K chunks per CTA, more splits than the generic split-K
       // model picks (measured at N l = 4096: 32 splits 157.7 us per iteration against 161.2 with
       // the model's 18; 24: 161.8, 12: 167.6, 6: 187.5); ISVD_GPU_KN_DD_KCHUNK overrides the depth
-      if (Nl >= 2048) g.splits = std::max(1, Nl / kn_dd_kchunk());
+      if (Nl >= kn_dd_from() && kn_dd_kchunk() > 0) g.splits = std::max(1, Nl / kn_dd_kchunk());
       g.alpha = invN;
       g.A = Bc; g.a_rs = 1; g.a_cs = lw; g.a_bs = 0;
       g.B = Bc; g.b_rs = lw; g.b_cs = 1; g.b_bs = l;
